@@ -1,0 +1,254 @@
+"""Host-side mirror of the reference's operator API for the vertex-patch
+Schwarz MG path, over the C ABI of include/tps.h.
+
+Reference classes mirrored here (same names, argument meaning and error
+behaviour -- errors raise, nothing is swallowed):
+
+* ``LaplaceOperator``  -- include/laplace_operator.cuh:80-201 (vmult/Tvmult)
+* ``PatchSmoother``    -- include/patch_smoother.cuh:91-351 (vmult/step)
+* ``MGTransferCUDA``   -- include/cuda_mg_transfer.cuh:57-213
+  (prolongate, prolongate_and_add, restrict_and_add)
+* ``MultigridSolvers`` -- include/solver.cuh:1541-2210 (vmult, solve_gmres,
+  plus the MG-preconditioned CG driver)
+
+Vectors are torch CUDA tensors (float64 or float32, contiguous, one entry per
+DoF of the level, lexicographic x-fastest numbering).  torch only provides
+device memory and the current stream; every operation runs in libtps.so.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import torch
+
+from . import _lib as L
+
+_DTYPES = {torch.float64: L.TPS_F64, torch.float32: L.TPS_F32}
+_PRECISIONS = {"fp64": L.VCYCLE_F64, "fp32": L.VCYCLE_F32, "fp64_rounded": L.VCYCLE_F64_ROUNDED}
+
+
+def split_cells(n_cells: int) -> tuple[int, int]:
+    """n_cells = n_coarse * 2^(n_levels-1) with the smallest n_coarse >= 2."""
+    if n_cells < 2:
+        raise ValueError("at least 2 cells per direction are required")
+    n, levels = n_cells, 1
+    while n % 2 == 0 and n // 2 >= 2:
+        n //= 2
+        levels += 1
+    return n, levels
+
+
+def _stream() -> ctypes.c_void_p:
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class PoissonProblem:
+    """Uniform Q_k discretisation of -div(grad u) = f on the unit square/cube
+    with homogeneous Dirichlet data and its geometric MG hierarchy (replaces
+    the Triangulation/DoFHandler set-up of apps/poisson.cu:152-181 and the
+    level set-up of MultigridSolvers, include/solver.cuh:1545-1744)."""
+
+    def __init__(self, dim: int, degree: int, n_cells: int, relaxation: float = 1.0,
+                 n_coarse: int | None = None, device: int | None = None):
+        if n_coarse is None:
+            n_coarse, n_levels = split_cells(n_cells)
+        else:
+            q, n_levels = n_cells // n_coarse, 1
+            if q * n_coarse != n_cells or q & (q - 1):
+                raise ValueError("n_cells must be n_coarse * 2^l")
+            while q > 1:
+                q //= 2
+                n_levels += 1
+        self.dim, self.degree, self.n_cells = dim, degree, n_cells
+        self.n_coarse, self.n_levels = n_coarse, n_levels
+        self.device = torch.cuda.current_device() if device is None else device
+        pb = L.TpsProblem(dim, degree, n_coarse, n_levels, relaxation, None, self.device)
+        h = ctypes.c_void_p()
+        L.check(L.lib().tps_create(ctypes.byref(pb), ctypes.byref(h)), None)
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().tps_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        if not self._h:
+            raise RuntimeError("problem has been closed")
+        return self._h
+
+    def n_dofs(self, level: int | None = None) -> int:
+        lvl = self.n_levels - 1 if level is None else level
+        n = ctypes.c_int64()
+        c = ctypes.c_int()
+        L.check(L.lib().tps_level_info(self.handle, lvl, ctypes.byref(n), ctypes.byref(c)),
+                self.handle)
+        return n.value
+
+    def cells(self, level: int | None = None) -> int:
+        lvl = self.n_levels - 1 if level is None else level
+        return self.n_coarse << lvl
+
+    def new_vector(self, level: int | None = None, dtype=torch.float64) -> torch.Tensor:
+        """LaplaceOperator::initialize_dof_vector equivalent."""
+        return torch.zeros(self.n_dofs(level), dtype=dtype, device=f"cuda:{self.device}")
+
+    def _check_vec(self, v: torch.Tensor, level: int, dtype=None) -> int:
+        if not isinstance(v, torch.Tensor) or not v.is_cuda:
+            raise TypeError("vectors must be CUDA tensors")
+        if not v.is_contiguous():
+            raise ValueError("vectors must be contiguous")
+        if v.numel() != self.n_dofs(level):
+            raise ValueError(f"vector has {v.numel()} entries, level {level} has {self.n_dofs(level)}")
+        if v.dtype not in _DTYPES or (dtype is not None and v.dtype != dtype):
+            raise TypeError(f"unsupported dtype {v.dtype}")
+        return _DTYPES[v.dtype]
+
+
+class LaplaceOperator:
+    """LaplaceOperator<dim, k, Number>::vmult on one level: dst = A src on the
+    interior rows, dst = src on the Dirichlet rows."""
+
+    def __init__(self, problem: PoissonProblem, level: int | None = None):
+        self.problem = problem
+        self.level = problem.n_levels - 1 if level is None else level
+
+    def vmult(self, dst: torch.Tensor, src: torch.Tensor) -> None:
+        p = self.problem
+        dt = p._check_vec(dst, self.level)
+        p._check_vec(src, self.level, dst.dtype)
+        L.check(L.lib().tps_laplace_vmult(p.handle, self.level, dt, dst.data_ptr(), src.data_ptr(),
+                                          _stream()), p.handle)
+
+    Tvmult = vmult
+
+    def initialize_dof_vector(self, dtype=torch.float64) -> torch.Tensor:
+        return self.problem.new_vector(self.level, dtype)
+
+
+class PatchSmoother:
+    """PatchSmoother (PreconditionRelaxation over the coloured vertex-patch
+    sweep): vmult zeroes dst and sweeps once, step sweeps once in place."""
+
+    def __init__(self, problem: PoissonProblem, level: int | None = None):
+        self.problem = problem
+        self.level = problem.n_levels - 1 if level is None else level
+
+    def _sweep(self, dst, src, zero_init: bool, reverse: bool):
+        p = self.problem
+        dt = p._check_vec(dst, self.level)
+        p._check_vec(src, self.level, dst.dtype)
+        L.check(L.lib().tps_smoother_step(p.handle, self.level, dt, dst.data_ptr(), src.data_ptr(),
+                                          int(zero_init), int(reverse), _stream()), p.handle)
+
+    def vmult(self, dst: torch.Tensor, src: torch.Tensor, reverse: bool = False) -> None:
+        self._sweep(dst, src, True, reverse)
+
+    def step(self, dst: torch.Tensor, src: torch.Tensor, reverse: bool = False) -> None:
+        self._sweep(dst, src, False, reverse)
+
+    def Tvmult(self, dst, src):  # include/patch_smoother.cuh:55-67: no-op in the reference
+        pass
+
+    def Tstep(self, dst, src):
+        pass
+
+
+class MGTransferCUDA:
+    """Geometric transfer between consecutive levels (to_level / from_level is
+    the finer one)."""
+
+    def __init__(self, problem: PoissonProblem):
+        self.problem = problem
+
+    def prolongate(self, to_level: int, dst: torch.Tensor, src: torch.Tensor) -> None:
+        dst.zero_()
+        self.prolongate_and_add(to_level, dst, src)
+
+    def prolongate_and_add(self, to_level: int, dst: torch.Tensor, src: torch.Tensor) -> None:
+        p = self.problem
+        dt = p._check_vec(dst, to_level)
+        p._check_vec(src, to_level - 1, dst.dtype)
+        L.check(L.lib().tps_prolongate_add(p.handle, to_level, dt, dst.data_ptr(), src.data_ptr(),
+                                           _stream()), p.handle)
+
+    def restrict_and_add(self, from_level: int, dst: torch.Tensor, src: torch.Tensor) -> None:
+        p = self.problem
+        dt = p._check_vec(dst, from_level - 1)
+        p._check_vec(src, from_level, dst.dtype)
+        L.check(L.lib().tps_restrict_add(p.handle, from_level, dt, dst.data_ptr(), src.data_ptr(),
+                                         _stream()), p.handle)
+
+
+@dataclass
+class SolveReport:
+    iterations: int
+    converged: bool
+    initial_residual: float
+    final_residual: float
+    history: list = field(default_factory=list)
+    time_ms: float = 0.0
+
+
+def _report(r: L.TpsReport) -> SolveReport:
+    n = min(r.iterations + 1, L.MAX_HISTORY)
+    return SolveReport(r.iterations, bool(r.converged), r.initial_residual, r.final_residual,
+                       [r.history[i] for i in range(n)], r.time_ms)
+
+
+class MultigridSolvers:
+    """MG-preconditioned Krylov solves on the finest level (FP64 outer
+    iteration, V-cycle in FP64, FP32, or FP64 with FP32-rounded input)."""
+
+    def __init__(self, problem: PoissonProblem):
+        self.problem = problem
+
+    def vmult(self, dst: torch.Tensor, src: torch.Tensor, precision: str = "fp32",
+              symmetric: bool = False) -> None:
+        """One V-cycle applied to src (MultigridSolvers::vmult)."""
+        p = self.problem
+        lvl = p.n_levels - 1
+        p._check_vec(dst, lvl, torch.float64)
+        p._check_vec(src, lvl, torch.float64)
+        L.check(L.lib().tps_vcycle(p.handle, _PRECISIONS[precision], int(symmetric), dst.data_ptr(),
+                                   src.data_ptr(), _stream()), p.handle)
+
+    def _solve(self, driver, b, x, precision, symmetric, max_iter, rel_tol, abs_tol, use_graph,
+               raise_on_fail):
+        p = self.problem
+        lvl = p.n_levels - 1
+        p._check_vec(b, lvl, torch.float64)
+        if x is None:
+            x = torch.zeros_like(b)
+        p._check_vec(x, lvl, torch.float64)
+        o = L.TpsSolveOpts(driver, _PRECISIONS[precision], int(symmetric), max_iter, rel_tol,
+                           abs_tol, int(use_graph))
+        rep = L.TpsReport()
+        st = L.lib().tps_solve(p.handle, ctypes.byref(o), b.data_ptr(), x.data_ptr(),
+                               ctypes.byref(rep), _stream())
+        if st != L.TPS_OK and (raise_on_fail or st != 4):
+            L.check(st, p.handle)
+        return x, _report(rep)
+
+    def solve_cg(self, b: torch.Tensor, x: torch.Tensor | None = None, precision: str = "fp32",
+                 symmetric: bool = True, max_iter: int = 100, rel_tol: float = 1e-10,
+                 use_graph: bool = True, raise_on_fail: bool = True):
+        """Flexible CG, FP64 outer iteration, to ||b - A x|| <= rel_tol ||b||."""
+        return self._solve(L.DRIVER_CG, b, x, precision, symmetric, max_iter, rel_tol, 1e-300,
+                           use_graph, raise_on_fail)
+
+    def solve_gmres(self, b: torch.Tensor, x: torch.Tensor | None = None,
+                    precision: str = "fp64_rounded", max_iter: int = 20, reduce: float = 1e-9,
+                    abs_tol: float = 1e-16, raise_on_fail: bool = False):
+        """deal.II-SolverGMRES-semantics solve as in MultigridSolvers::solve_gmres
+        (non-convergence is reported, not raised, like the reference)."""
+        return self._solve(L.DRIVER_GMRES, b, x, precision, False, max_iter, reduce, abs_tol,
+                           False, raise_on_fail)

@@ -1,0 +1,288 @@
+// Host 1D finite-element data and the FP64 generalized eigensolver.
+//
+// Restates, without deal.II, what the reference obtains from FE_DGQ<1>/FE_Q<1>
+// + QGauss<1>(k+1) (include/patch_base.template.cuh:713-762,
+// include/tensor_product.h:112-189) and from
+// TensorProductMatrixSymmetricSum::reinit (include/tensor_product.h:208-210).
+// The eigendecomposition runs in FP64 on the host (the reference runs it in
+// the V-cycle precision, include/patch_base.template.cuh:791-806) and splits
+// the centro-symmetric interior problem into its even and odd halves so the
+// eigenvectors are exactly symmetric / antisymmetric, which the kernels use
+// to halve the fast-diagonalization work.
+#include "fe_data.h"
+
+#include <algorithm>
+#include <cmath>
+#include <stdexcept>
+
+namespace tps {
+namespace {
+
+// Legendre polynomial value and first two derivatives on [-1,1].
+void legendre_eval(int n, double t, double &p, double &dp)
+{
+  double pm1 = 1.0, pn = t;
+  if (n == 0) {
+    p = 1.0;
+    dp = 0.0;
+    return;
+  }
+  for (int j = 2; j <= n; ++j) {
+    const double pj = ((2.0 * j - 1.0) * t * pn - (j - 1.0) * pm1) / j;
+    pm1 = pn;
+    pn = pj;
+  }
+  p = pn;
+  dp = n * (pm1 - t * pn) / (1.0 - t * t);
+}
+
+std::vector<double> gauss_lobatto(int k)
+{
+  std::vector<double> x(k + 1);
+  x[0] = 0.0;
+  x[k] = 1.0;
+  for (int i = 1; i < k; ++i) {
+    double t = -std::cos(M_PI * i / k);
+    for (int it = 0; it < 200; ++it) {
+      double p, dp;
+      legendre_eval(k, t, p, dp);
+      const double d2p = (2.0 * t * dp - k * (k + 1.0) * p) / (1.0 - t * t);
+      const double step = dp / d2p;
+      t -= step;
+      if (std::fabs(step) < 1e-17) break;
+    }
+    x[i] = 0.5 * (1.0 + t);
+  }
+  return x;
+}
+
+void gauss_legendre(int n, std::vector<double> &x, std::vector<double> &w)
+{
+  x.assign(n, 0.0);
+  w.assign(n, 0.0);
+  for (int i = 0; i < n; ++i) {
+    double t = -std::cos(M_PI * (i + 0.75) / (n + 0.5));
+    for (int it = 0; it < 200; ++it) {
+      double p, dp;
+      legendre_eval(n, t, p, dp);
+      const double step = p / dp;
+      t -= step;
+      if (std::fabs(step) < 1e-17) break;
+    }
+    double p, dp;
+    legendre_eval(n, t, p, dp);
+    x[i] = 0.5 * (1.0 + t);
+    w[i] = 1.0 / ((1.0 - t * t) * dp * dp);
+  }
+}
+
+// Lagrange basis on `nodes`: value and derivative of basis i at x.
+void lagrange(const std::vector<double> &nodes, int i, double x, double &v, double &d)
+{
+  const int np = static_cast<int>(nodes.size());
+  v = 1.0;
+  d = 0.0;
+  for (int m = 0; m < np; ++m) {
+    if (m == i) continue;
+    const double inv = 1.0 / (nodes[i] - nodes[m]);
+    d = d * (x - nodes[m]) * inv + v * inv;  // product rule, accumulated
+    v *= (x - nodes[m]) * inv;
+  }
+}
+
+void cholesky_lower(int m, std::vector<double> &C, const double *B)
+{
+  C.assign(m * m, 0.0);
+  for (int j = 0; j < m; ++j) {
+    double s = B[j * m + j];
+    for (int p = 0; p < j; ++p) s -= C[j * m + p] * C[j * m + p];
+    if (!(s > 0)) throw std::runtime_error("mass matrix not positive definite");
+    C[j * m + j] = std::sqrt(s);
+    for (int i = j + 1; i < m; ++i) {
+      double t = B[i * m + j];
+      for (int p = 0; p < j; ++p) t -= C[i * m + p] * C[j * m + p];
+      C[i * m + j] = t / C[j * m + j];
+    }
+  }
+}
+
+// Symmetric Jacobi; A destroyed, Q eigenvectors as columns.
+void jacobi(int m, std::vector<double> &A, std::vector<double> &Q, std::vector<double> &d)
+{
+  Q.assign(m * m, 0.0);
+  for (int i = 0; i < m; ++i) Q[i * m + i] = 1.0;
+  for (int sweep = 0; sweep < 64; ++sweep) {
+    double off = 0.0, diag = 0.0;
+    for (int i = 0; i < m; ++i)
+      for (int j = 0; j < m; ++j) (i == j ? diag : off) += A[i * m + j] * A[i * m + j];
+    if (off <= 1e-34 * (diag + off)) break;
+    for (int p = 0; p < m; ++p)
+      for (int q = p + 1; q < m; ++q) {
+        const double apq = A[p * m + q];
+        if (apq == 0.0) continue;
+        const double tau = (A[q * m + q] - A[p * m + p]) / (2.0 * apq);
+        const double t = std::copysign(1.0, tau) / (std::fabs(tau) + std::hypot(1.0, tau));
+        const double c = 1.0 / std::hypot(1.0, t), s = t * c;
+        for (int r = 0; r < m; ++r) {
+          const double a = A[r * m + p], b = A[r * m + q];
+          A[r * m + p] = c * a - s * b;
+          A[r * m + q] = s * a + c * b;
+        }
+        for (int r = 0; r < m; ++r) {
+          const double a = A[p * m + r], b = A[q * m + r];
+          A[p * m + r] = c * a - s * b;
+          A[q * m + r] = s * a + c * b;
+        }
+        for (int r = 0; r < m; ++r) {
+          const double a = Q[r * m + p], b = Q[r * m + q];
+          Q[r * m + p] = c * a - s * b;
+          Q[r * m + q] = s * a + c * b;
+        }
+      }
+  }
+  d.resize(m);
+  for (int i = 0; i < m; ++i) d[i] = A[i * m + i];
+}
+
+}  // namespace
+
+void generalized_eigen(int m, const double *A, const double *B, double *V, double *lambda)
+{
+  std::vector<double> C, W(m * m), K(m * m), Q, d;
+  cholesky_lower(m, C, B);
+  // W = C^{-1} A
+  for (int col = 0; col < m; ++col)
+    for (int i = 0; i < m; ++i) {
+      double t = A[i * m + col];
+      for (int p = 0; p < i; ++p) t -= C[i * m + p] * W[p * m + col];
+      W[i * m + col] = t / C[i * m + i];
+    }
+  // K = W C^{-T}: row r of K solves C k_r = w_r (W symmetric-congruent)
+  for (int r = 0; r < m; ++r)
+    for (int i = 0; i < m; ++i) {
+      double t = W[r * m + i];
+      for (int p = 0; p < i; ++p) t -= C[i * m + p] * K[r * m + p];
+      K[r * m + i] = t / C[i * m + i];
+    }
+  for (int i = 0; i < m; ++i)
+    for (int j = i + 1; j < m; ++j) K[i * m + j] = K[j * m + i] = 0.5 * (K[i * m + j] + K[j * m + i]);
+  jacobi(m, K, Q, d);
+  // V = C^{-T} Q
+  std::vector<double> Vt(m * m);
+  for (int col = 0; col < m; ++col)
+    for (int i = m - 1; i >= 0; --i) {
+      double t = Q[i * m + col];
+      for (int p = i + 1; p < m; ++p) t -= C[p * m + i] * Vt[p * m + col];
+      Vt[i * m + col] = t / C[i * m + i];
+    }
+  std::vector<int> order(m);
+  for (int i = 0; i < m; ++i) order[i] = i;
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return d[a] < d[b]; });
+  for (int j = 0; j < m; ++j) {
+    lambda[j] = d[order[j]];
+    for (int i = 0; i < m; ++i) V[i * m + j] = Vt[i * m + order[j]];
+  }
+}
+
+DegreeData make_degree_data(int k)
+{
+  if (k < 1 || k > kMaxDegree) throw std::runtime_error("degree out of range");
+  DegreeData D;
+  D.k = k;
+  const int np = k + 1, n1 = 2 * k + 1, m = 2 * k - 1;
+  D.nodes = gauss_lobatto(k);
+  std::vector<double> xq, wq;
+  gauss_legendre(k + 1, xq, wq);
+  D.cmass.assign(np * np, 0.0);
+  D.clap.assign(np * np, 0.0);
+  for (int q = 0; q < k + 1; ++q) {
+    std::vector<double> v(np), dv(np);
+    for (int i = 0; i < np; ++i) lagrange(D.nodes, i, xq[q], v[i], dv[i]);
+    for (int i = 0; i < np; ++i)
+      for (int j = 0; j < np; ++j) {
+        D.cmass[i * np + j] += wq[q] * v[i] * v[j];
+        D.clap[i * np + j] += wq[q] * dv[i] * dv[j];
+      }
+  }
+  D.pmass.assign(n1 * n1, 0.0);
+  D.plap.assign(n1 * n1, 0.0);
+  for (int cell = 0; cell < 2; ++cell)
+    for (int i = 0; i < np; ++i)
+      for (int j = 0; j < np; ++j) {
+        D.pmass[(i + cell * k) * n1 + j + cell * k] += D.cmass[i * np + j];
+        D.plap[(i + cell * k) * n1 + j + cell * k] += D.clap[i * np + j];
+      }
+  // interior blocks, then even/odd split around the centre DoF c = k-1
+  std::vector<double> MI(m * m), LI(m * m);
+  for (int i = 0; i < m; ++i)
+    for (int j = 0; j < m; ++j) {
+      MI[i * m + j] = D.pmass[(i + 1) * n1 + j + 1];
+      LI[i * m + j] = D.plap[(i + 1) * n1 + j + 1];
+    }
+  const int c = k - 1;  // centre index of the interior
+  const double r2 = std::sqrt(0.5);
+  // even basis: (e_i + e_{m-1-i})/sqrt2 for i < c, and e_c ; odd: (e_i - e_{m-1-i})/sqrt2
+  const int ne = c + 1, no = c;
+  std::vector<double> Qe(m * ne, 0.0), Qo(m * std::max(no, 1), 0.0);
+  for (int i = 0; i < c; ++i) {
+    Qe[i * ne + i] = r2;
+    Qe[(m - 1 - i) * ne + i] = r2;
+    Qo[i * no + i] = r2;
+    Qo[(m - 1 - i) * no + i] = -r2;
+  }
+  Qe[c * ne + c] = 1.0;
+  auto project = [&](const std::vector<double> &Qx, int nx, const std::vector<double> &A) {
+    std::vector<double> R(nx * nx, 0.0);
+    for (int a = 0; a < nx; ++a)
+      for (int b = 0; b < nx; ++b) {
+        double s = 0.0;
+        for (int i = 0; i < m; ++i)
+          for (int j = 0; j < m; ++j) s += Qx[i * nx + a] * A[i * m + j] * Qx[j * nx + b];
+        R[a * nx + b] = s;
+      }
+    return R;
+  };
+  // Mode order: the C+1 reflection-even eigenvectors first (ascending), then
+  // the C odd ones (ascending).  The kernels rely on this order to apply S and
+  // S^T on folded half-lines with compile-time parity.
+  D.evec.assign(m * m, 0.0);
+  D.eval.assign(m, 0.0);
+  int col = 0;
+  for (int part = 0; part < 2; ++part) {
+    const int nx = part == 0 ? ne : no;
+    if (nx == 0) continue;
+    const std::vector<double> &Qx = part == 0 ? Qe : Qo;
+    std::vector<double> Ms = project(Qx, nx, MI), Ls = project(Qx, nx, LI);
+    std::vector<double> W(nx * nx), lam(nx);
+    generalized_eigen(nx, Ls.data(), Ms.data(), W.data(), lam.data());
+    for (int j = 0; j < nx; ++j, ++col) {
+      std::vector<double> v(m, 0.0);
+      for (int i = 0; i < m; ++i)
+        for (int a = 0; a < nx; ++a) v[i] += Qx[i * nx + a] * W[a * nx + j];
+      // make the reflection symmetry exact
+      for (int i = 0; i < c; ++i) {
+        const double s = part == 0 ? 0.5 * (v[i] + v[m - 1 - i]) : 0.5 * (v[i] - v[m - 1 - i]);
+        v[i] = s;
+        v[m - 1 - i] = part == 0 ? s : -s;
+      }
+      if (part == 1) v[c] = 0.0;
+      D.eval[col] = lam[j];
+      for (int i = 0; i < m; ++i) D.evec[i * m + col] = v[i];
+    }
+  }
+  // 1D prolongation: coarse basis evaluated at the child nodes
+  D.prol.assign(n1 * np, 0.0);
+  for (int f = 0; f < n1; ++f) {
+    const double x = f <= k ? 0.5 * D.nodes[f] : 0.5 + 0.5 * D.nodes[f - k];
+    for (int cc = 0; cc < np; ++cc) {
+      double v, d;
+      lagrange(D.nodes, cc, x, v, d);
+      if (std::fabs(v) < 1e-14) v = 0.0;
+      if (std::fabs(v - 1.0) < 1e-14) v = 1.0;
+      D.prol[f * np + cc] = v;
+    }
+  }
+  return D;
+}
+
+}  // namespace tps

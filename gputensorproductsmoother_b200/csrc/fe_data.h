@@ -1,0 +1,38 @@
+// Host-side 1D finite-element data of degree k on the reference cell [0,1]
+// (FP64), the vertex-patch matrices and their interior generalized
+// eigendecomposition.  Replaces LevelVertexPatch::reinit_tensor_product
+// (include/patch_base.template.cuh:709-1205) and TensorProductData
+// (include/tensor_product.h:60-284) of the reference, without deal.II.
+#pragma once
+
+#include <vector>
+
+namespace tps {
+
+constexpr int kMaxDegree = 7;
+
+struct DegreeData {
+  int k = 0;                  // polynomial degree
+  std::vector<double> nodes;  // k+1 Gauss-Lobatto support points on [0,1]
+  std::vector<double> cmass;  // (k+1)^2 cell mass on [0,1], QGauss(k+1)
+  std::vector<double> clap;   // (k+1)^2 cell stiffness on [0,1]
+  std::vector<double> pmass;  // (2k+1)^2 vertex-patch mass (two reference cells)
+  std::vector<double> plap;   // (2k+1)^2 vertex-patch stiffness
+  // Interior generalized eigenpairs of the patch on REFERENCE cells:
+  // plap_I v = mu pmass_I v, V^T pmass_I V = I, eigenvectors as columns
+  // (evec[i*m + j] = v_j[i]), exactly even/odd under reflection.  Columns
+  // 0..k-1 hold the k even modes, columns k..2k-2 the k-1 odd modes, each
+  // group in ascending eigenvalue order.
+  std::vector<double> evec;   // m^2, m = 2k-1
+  std::vector<double> eval;   // m, ordered like the columns of evec
+  std::vector<double> prol;   // (2k+1) x (k+1): coarse basis at child nodes
+};
+
+// Builds every table above for degree k (1 <= k <= kMaxDegree).
+DegreeData make_degree_data(int k);
+
+// Symmetric-definite generalized eigenproblem A v = lambda B v (FP64,
+// Cholesky + cyclic Jacobi); V column-major-as-rows like DegreeData::evec.
+void generalized_eigen(int m, const double *A, const double *B, double *V, double *lambda);
+
+}  // namespace tps

@@ -1,0 +1,865 @@
+// C-ABI implementation: problem set-up, level operators, the V-cycle and the
+// FP64 Krylov drivers (host C++, CUDA runtime only; no torch, no deal.II).
+//
+// Reference counterparts:
+//   tps_create        MultigridSolvers ctor (include/solver.cuh:1545-1744),
+//                     LevelVertexPatch::reinit (include/patch_base.template.cuh:194-307),
+//                     MGTransferCUDA::build (include/cuda_mg_transfer.template.cuh:453-559)
+//   tps_laplace_vmult LaplaceOperator::vmult (include/laplace_operator.cuh:86-101)
+//   tps_smoother_step PatchSmootherImpl::vmult/step (include/patch_smoother.cuh:155-292)
+//   tps_prolongate_add / tps_restrict_add
+//                     MGTransferCUDA (include/cuda_mg_transfer.template.cuh:575-671)
+//   tps_vcycle        MultigridSolvers::vmult + v_cycle (include/solver.cuh:1915-2001)
+//   tps_solve         MultigridSolvers::solve_gmres (include/solver.cuh:1865-1910) and the
+//                     MG-preconditioned flexible CG driver (no reference counterpart)
+#include "../../include/tps.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "blas.cuh"
+#include "fe_data.h"
+#include "kernel_table.h"
+
+namespace tps {
+
+const KernelTable *kernel_table(int degree)
+{
+  switch (degree) {
+    case 1: return &kernel_table_k1;
+    case 2: return &kernel_table_k2;
+    case 3: return &kernel_table_k3;
+    case 4: return &kernel_table_k4;
+    case 5: return &kernel_table_k5;
+    case 6: return &kernel_table_k6;
+    case 7: return &kernel_table_k7;
+    default: return nullptr;
+  }
+}
+
+// coarse dense solve kernels (FP64 inverse rounded to the V-cycle precision)
+cudaError_t launch_coarse_dense(const void *inv, const int *idx, int n_int, void *su,
+                                const void *d, int elem_bytes, cudaStream_t s);
+
+}  // namespace tps
+
+using namespace tps;
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct ApiError : std::runtime_error {
+  int code;
+  ApiError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+#define TPS_CUDA(call)                                                                       \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess)                                                                   \
+      throw ApiError(e_ == cudaErrorMemoryAllocation ? TPS_ERR_ALLOC : TPS_ERR_CUDA,         \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+  } while (0)
+
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  void release()
+  {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  void alloc(size_t b)
+  {
+    release();
+    if (b == 0) return;
+    cudaError_t e = cudaMalloc(&p, b);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      throw ApiError(TPS_ERR_ALLOC, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    bytes = b;
+    TPS_CUDA(cudaMemset(p, 0, b));
+  }
+  template <typename T>
+  T *as() const { return static_cast<T *>(p); }
+};
+
+// V-cycle work vectors of one precision
+struct VcycleVectors {
+  bool ready = false;
+  std::vector<std::unique_ptr<DevBuf>> d, su, t, tmp;  // per level
+  DevBuf coarse_inv;                                   // dense coarse inverse
+};
+
+}  // namespace
+
+struct tps_handle {
+  int dim = 0, k = 0, n_coarse = 0, n_levels = 0, device = 0;
+  double omega = 1.0;
+  std::vector<LevelGeomH> lv;
+  const KernelTable *kt = nullptr;
+  DegreeData D;
+  std::string err;
+  // coarse level: single vertex patch (n_coarse == 2) or dense solve
+  bool dense_coarse = false;
+  int n_int_coarse = 0;
+  std::vector<double> coarse_inv_host;  // n_int^2, FP64
+  DevBuf coarse_idx;
+  VcycleVectors vc[2];  // [0] FP64, [1] FP32
+  // Krylov work vectors (fine level, FP64)
+  DevBuf r, p, q, partial, scalars;
+  std::vector<std::unique_ptr<DevBuf>> gmres_v;
+  // CUDA graph of one CG iteration
+  cudaGraphExec_t graph = nullptr;
+  int graph_key = -1;
+  cudaStream_t graph_stream = nullptr;
+  const double *graph_x = nullptr;  // the captured graph updates this solution vector
+  cudaStream_t own_stream = nullptr;  // used by tps_solve_host
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+  ~tps_handle()
+  {
+    if (graph) cudaGraphExecDestroy(graph);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (own_stream) cudaStreamDestroy(own_stream);
+  }
+  const LevelGeomH &fine() const { return lv.back(); }
+};
+
+namespace {
+
+int dt_index(int dtype)
+{
+  if (dtype != TPS_F64 && dtype != TPS_F32) throw ApiError(TPS_ERR_INVALID, "dtype must be TPS_F64 or TPS_F32");
+  return dtype;
+}
+
+void check_level(const tps_handle *h, int level, int min_level = 0)
+{
+  if (level < min_level || level >= h->n_levels)
+    throw ApiError(TPS_ERR_INVALID, "level " + std::to_string(level) + " out of range");
+}
+
+template <typename F>
+int guarded(tps_handle *h, F &&f)
+{
+  if (!h) {
+    g_create_error = "null handle";
+    return TPS_ERR_INVALID;
+  }
+  try {
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) throw ApiError(TPS_ERR_CUDA, cudaGetErrorString(e));
+    f();
+    h->err.clear();
+    return TPS_OK;
+  } catch (const ApiError &e) {
+    h->err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    h->err = "host allocation failed";
+    return TPS_ERR_ALLOC;
+  } catch (const std::exception &e) {
+    h->err = e.what();
+    return TPS_ERR_INVALID;
+  }
+}
+
+// dense interior operator of the coarse level, assembled on the host in FP64
+// as the Kronecker sum of the global 1D matrices, and its inverse
+void build_dense_coarse(tps_handle *h)
+{
+  const int k = h->k, n = h->n_coarse, N1 = n * k + 1, dim = h->dim;
+  const double hh = 1.0 / n, s = stiffness_scale(dim, hh);
+  const int np = k + 1;
+  std::vector<double> M1(N1 * N1, 0.0), L1(N1 * N1, 0.0);
+  for (int c = 0; c < n; ++c)
+    for (int a = 0; a < np; ++a)
+      for (int b = 0; b < np; ++b) {
+        M1[(c * k + a) * N1 + c * k + b] += h->D.cmass[a * np + b];
+        L1[(c * k + a) * N1 + c * k + b] += h->D.clap[a * np + b];
+      }
+  std::vector<int> idx1;
+  for (int i = 1; i < N1 - 1; ++i) idx1.push_back(i);
+  const int m1 = static_cast<int>(idx1.size());
+  const int ni = dim == 3 ? m1 * m1 * m1 : m1 * m1;
+  h->n_int_coarse = ni;
+  std::vector<double> A(static_cast<size_t>(ni) * ni, 0.0);
+  auto coord = [&](int i, int &x, int &y, int &z) {
+    x = idx1[i % m1];
+    y = idx1[(i / m1) % m1];
+    z = dim == 3 ? idx1[i / (m1 * m1)] : 0;
+  };
+  for (int i = 0; i < ni; ++i) {
+    int xi, yi, zi;
+    coord(i, xi, yi, zi);
+    for (int j = 0; j < ni; ++j) {
+      int xj, yj, zj;
+      coord(j, xj, yj, zj);
+      const double mx = M1[xi * N1 + xj], my = M1[yi * N1 + yj];
+      const double lx = L1[xi * N1 + xj], ly = L1[yi * N1 + yj];
+      double v;
+      if (dim == 2) {
+        v = ly * mx + my * lx;
+      } else {
+        const double mz = M1[zi * N1 + zj], lz = L1[zi * N1 + zj];
+        v = lz * my * mx + mz * ly * mx + mz * my * lx;
+      }
+      A[static_cast<size_t>(i) * ni + j] = s * v;
+    }
+  }
+  // Cholesky and explicit inverse (coarse systems hold at most a few thousand DoFs)
+  std::vector<double> &L = A;
+  for (int j = 0; j < ni; ++j) {
+    double d = L[static_cast<size_t>(j) * ni + j];
+    for (int p = 0; p < j; ++p) d -= L[static_cast<size_t>(j) * ni + p] * L[static_cast<size_t>(j) * ni + p];
+    if (!(d > 0)) throw ApiError(TPS_ERR_INVALID, "coarse operator not positive definite");
+    d = std::sqrt(d);
+    L[static_cast<size_t>(j) * ni + j] = d;
+    for (int i = j + 1; i < ni; ++i) {
+      double t = L[static_cast<size_t>(i) * ni + j];
+      for (int p = 0; p < j; ++p) t -= L[static_cast<size_t>(i) * ni + p] * L[static_cast<size_t>(j) * ni + p];
+      L[static_cast<size_t>(i) * ni + j] = t / d;
+    }
+  }
+  std::vector<double> inv(static_cast<size_t>(ni) * ni, 0.0), col(ni);
+  for (int c = 0; c < ni; ++c) {
+    for (int i = 0; i < ni; ++i) {
+      double t = i == c ? 1.0 : 0.0;
+      for (int p = 0; p < i; ++p) t -= L[static_cast<size_t>(i) * ni + p] * col[p];
+      col[i] = t / L[static_cast<size_t>(i) * ni + i];
+    }
+    for (int i = ni - 1; i >= 0; --i) {
+      double t = col[i];
+      for (int p = i + 1; p < ni; ++p) t -= L[static_cast<size_t>(p) * ni + i] * col[p];
+      col[i] = t / L[static_cast<size_t>(i) * ni + i];
+    }
+    for (int i = 0; i < ni; ++i) inv[static_cast<size_t>(i) * ni + c] = col[i];
+  }
+  h->coarse_inv_host = std::move(inv);
+  std::vector<int> gidx(ni);
+  for (int i = 0; i < ni; ++i) {
+    int x, y, z;
+    coord(i, x, y, z);
+    gidx[i] = x + y * N1 + (dim == 3 ? z * N1 * N1 : 0);
+  }
+  h->coarse_idx.alloc(sizeof(int) * ni);
+  TPS_CUDA(cudaMemcpy(h->coarse_idx.p, gidx.data(), sizeof(int) * ni, cudaMemcpyHostToDevice));
+}
+
+VcycleVectors &vcycle_vectors(tps_handle *h, int p)
+{
+  VcycleVectors &V = h->vc[p];
+  if (V.ready) return V;
+  const size_t es = p == 0 ? sizeof(double) : sizeof(float);
+  V.d.clear();
+  V.su.clear();
+  V.t.clear();
+  V.tmp.clear();
+  for (int l = 0; l < h->n_levels; ++l) {
+    const LevelGeomH &g = h->lv[l];
+    V.d.emplace_back(new DevBuf);
+    V.su.emplace_back(new DevBuf);
+    V.t.emplace_back(new DevBuf);
+    V.tmp.emplace_back(new DevBuf);
+    V.d[l]->alloc(es * g.N);
+    V.su[l]->alloc(es * g.N);
+    V.t[l]->alloc(es * g.N);
+    if (l > 0 && h->dim == 3) {
+      // transfer scratch: fine z x coarse y x coarse x
+      const int64_t N1c = h->lv[l - 1].N1;
+      V.tmp[l]->alloc(es * static_cast<size_t>(g.N1) * N1c * N1c);
+    }
+  }
+  if (h->dense_coarse) {
+    const size_t n2 = h->coarse_inv_host.size();
+    V.coarse_inv.alloc(es * n2);
+    if (p == 0) {
+      TPS_CUDA(cudaMemcpy(V.coarse_inv.p, h->coarse_inv_host.data(), es * n2, cudaMemcpyHostToDevice));
+    } else {
+      std::vector<float> f(n2);
+      for (size_t i = 0; i < n2; ++i) f[i] = static_cast<float>(h->coarse_inv_host[i]);
+      TPS_CUDA(cudaMemcpy(V.coarse_inv.p, f.data(), es * n2, cudaMemcpyHostToDevice));
+    }
+  }
+  V.ready = true;
+  return V;
+}
+
+void smoother_sweep(tps_handle *h, int level, int p, void *x, const void *b, bool reverse,
+                    cudaStream_t s)
+{
+  const int nc = 1 << h->dim;
+  for (int i = 0; i < nc; ++i) {
+    const int c = reverse ? nc - 1 - i : i;
+    TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], x, b, c, h->omega, s));
+  }
+}
+
+void coarse_solve(tps_handle *h, int p, cudaStream_t s)
+{
+  VcycleVectors &V = h->vc[p];
+  const size_t es = p == 0 ? sizeof(double) : sizeof(float);
+  TPS_CUDA(cudaMemsetAsync(V.su[0]->p, 0, es * h->lv[0].N, s));
+  if (!h->dense_coarse) {
+    // one vertex patch covers every interior DoF: the smoother is an exact solve
+    smoother_sweep(h, 0, p, V.su[0]->p, V.d[0]->p, false, s);
+  } else {
+    TPS_CUDA(launch_coarse_dense(V.coarse_inv.p, h->coarse_idx.as<int>(), h->n_int_coarse,
+                                 V.su[0]->p, V.d[0]->p, static_cast<int>(es), s));
+  }
+}
+
+// MultigridSolvers::v_cycle (include/solver.cuh:1952-2001) on precision p:
+// input d[level], output su[level]
+void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s)
+{
+  VcycleVectors &V = h->vc[p];
+  if (level == 0) {
+    coarse_solve(h, p, s);
+    return;
+  }
+  const size_t es = p == 0 ? sizeof(double) : sizeof(float);
+  const LevelGeomH &g = h->lv[level];
+  const int di = h->dim - 2;
+  TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, es * g.N, s));
+  smoother_sweep(h, level, p, V.su[level]->p, V.d[level]->p, false, s);
+  TPS_CUDA(h->kt->laplace[di][p](g, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s));
+  TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], V.d[level - 1]->p, V.t[level]->p,
+                                   V.tmp[level]->p, 0, s));
+  vcycle_rec(h, level - 1, p, symmetric, s);
+  TPS_CUDA(h->kt->prolong[di][p](h->lv[level - 1], V.su[level]->p, V.su[level - 1]->p,
+                                 V.tmp[level]->p, s));
+  smoother_sweep(h, level, p, V.su[level]->p, V.d[level]->p, symmetric, s);
+}
+
+int vprec_index(int precision)
+{
+  if (precision < 0 || precision > 2) throw ApiError(TPS_ERR_INVALID, "bad V-cycle precision");
+  return precision == TPS_VCYCLE_F32 ? 1 : 0;
+}
+int input_kind(int precision) { return precision; }  // 0 f64, 1 f32, 2 f64-rounded
+
+void fine_vmult64(tps_handle *h, double *dst, const double *src, cudaStream_t s)
+{
+  const LevelGeomH &g = h->fine();
+  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, dst, src, nullptr, 0, s));
+  TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, 8, s));
+}
+
+void ensure_krylov(tps_handle *h)
+{
+  const int64_t N = h->fine().N;
+  if (!h->r.p) {
+    h->r.alloc(sizeof(double) * N);
+    h->p.alloc(sizeof(double) * N);
+    h->q.alloc(sizeof(double) * N);
+    h->partial.alloc(sizeof(double) * kRedBlocks * 4);
+    h->scalars.alloc(sizeof(CGScalars) + 64);
+  }
+  if (!h->ev0) {
+    TPS_CUDA(cudaEventCreate(&h->ev0));
+    TPS_CUDA(cudaEventCreate(&h->ev1));
+  }
+}
+
+// the part of a CG iteration that follows the convergence check:
+// z = V(d); beta; p = z + beta p; q = A p; alpha; x, r update; rr
+void cg_iteration_body(tps_handle *h, int prec, bool symmetric, double *x, cudaStream_t s)
+{
+  const int p = vprec_index(prec);
+  const int L = h->n_levels - 1;
+  const int64_t N = h->fine().N;
+  VcycleVectors &V = h->vc[p];
+  CGScalars *sc = h->scalars.as<CGScalars>();
+  double *part = h->partial.as<double>();
+  const int zk = p == 1 ? 1 : 0;
+  vcycle_rec(h, L, p, symmetric, s);
+  TPS_CUDA(launch_cg_beta(V.su[L]->p, zk, h->q.as<double>(), h->r.as<double>(), N, part, sc, s));
+  TPS_CUDA(launch_cg_update_p(h->p.as<double>(), V.su[L]->p, zk, N, sc, s));
+  TPS_CUDA(h->kt->laplace[h->dim - 2][0](h->fine(), h->q.p, h->p.p, nullptr, 0, s));
+  TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
+  TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
+                               V.d[L]->p, input_kind(prec), N, part, sc, s));
+  TPS_CUDA(launch_cg_finalize_rr(part, sc, s));
+}
+
+void read_scalars(tps_handle *h, CGScalars &out, cudaStream_t s)
+{
+  TPS_CUDA(cudaMemcpyAsync(&out, h->scalars.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, s));
+  TPS_CUDA(cudaStreamSynchronize(s));
+}
+
+int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x, tps_report *rep,
+             cudaStream_t s)
+{
+  const int p = vprec_index(o.precision);
+  vcycle_vectors(h, p);
+  ensure_krylov(h);
+  const int L = h->n_levels - 1;
+  const LevelGeomH &g = h->fine();
+  const int64_t N = g.N;
+  VcycleVectors &V = h->vc[p];
+  CGScalars *sc = h->scalars.as<CGScalars>();
+  double *part = h->partial.as<double>();
+  const int zk = p == 1 ? 1 : 0;
+  const bool sym = o.symmetric != 0;
+  TPS_CUDA(cudaEventRecord(h->ev0, s));
+  // Dirichlet rows: x_b = b_b, so r_b = 0 and the iteration lives on the interior
+  TPS_CUDA(launch_copy_boundary(x, b, h->dim, g.N1, 8, s));
+  TPS_CUDA(cudaMemsetAsync(h->r.p, 0, sizeof(double) * N, s));
+  TPS_CUDA(cudaMemsetAsync(h->q.p, 0, sizeof(double) * N, s));
+  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, h->r.p, x, b, 1, s));
+  TPS_CUDA(launch_cg_init(h->r.as<double>(), b, V.d[L]->p, input_kind(o.precision), N, part, s));
+  TPS_CUDA(launch_cg_finalize_init(part, sc, s));
+  CGScalars hs{};
+  read_scalars(h, hs, s);
+  const double bnorm = std::sqrt(hs.bb) > 0 ? std::sqrt(hs.bb) : 1.0;
+  double res = std::sqrt(hs.rr) / bnorm;
+  rep->initial_residual = std::sqrt(hs.rr);
+  rep->history[0] = res;
+  int it = 0;
+  int status = TPS_OK;
+  if (hs.breakdown) status = TPS_ERR_NONFINITE;
+  bool converged = res <= o.rel_tol;
+  if (!converged && status == TPS_OK) {
+    // first direction: z = V(r), p = z, rz; then q, alpha, x/r update
+    vcycle_rec(h, L, p, sym, s);
+    TPS_CUDA(launch_cg_first_direction(h->p.as<double>(), V.su[L]->p, zk, h->r.as<double>(), N, part, s));
+    TPS_CUDA(launch_cg_finalize_rz(part, sc, s));
+    TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, h->q.p, h->p.p, nullptr, 0, s));
+    TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
+    TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
+                                 V.d[L]->p, input_kind(o.precision), N, part, sc, s));
+    TPS_CUDA(launch_cg_finalize_rr(part, sc, s));
+    it = 1;
+    const int key = (o.precision << 1) | (sym ? 1 : 0);
+    // the graph bakes in x, so it is only reused for the same x pointer
+    cudaGraphExec_t exec = nullptr;
+    // stream capture is not available on the legacy default stream
+    bool use_graph = o.use_graph != 0 && s != nullptr;
+    for (;;) {
+      read_scalars(h, hs, s);
+      res = std::sqrt(hs.rr) / bnorm;
+      if (it < TPS_MAX_HISTORY) rep->history[it] = res;
+      if (hs.breakdown) {
+        status = hs.breakdown == 2 ? TPS_ERR_NONFINITE : TPS_ERR_BREAKDOWN;
+        break;
+      }
+      if (res <= o.rel_tol) {
+        converged = true;
+        break;
+      }
+      if (it >= o.max_iter) break;
+      if (use_graph) {
+        if (!exec) {
+          if (h->graph && h->graph_key == key && h->graph_stream == s && h->graph_x == x) {
+            exec = h->graph;
+          } else {
+            if (h->graph) {
+              cudaGraphExecDestroy(h->graph);
+              h->graph = nullptr;
+            }
+            cudaGraph_t graph;
+            TPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+            try {
+              cg_iteration_body(h, o.precision, sym, x, s);
+            } catch (...) {
+              cudaStreamEndCapture(s, &graph);
+              throw;
+            }
+            TPS_CUDA(cudaStreamEndCapture(s, &graph));
+            cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            TPS_CUDA(e);
+            h->graph = exec;
+            h->graph_key = key;
+            h->graph_stream = s;
+            h->graph_x = x;
+          }
+        }
+        TPS_CUDA(cudaGraphLaunch(exec, s));
+      } else {
+        cg_iteration_body(h, o.precision, sym, x, s);
+      }
+      ++it;
+    }
+  }
+  TPS_CUDA(cudaEventRecord(h->ev1, s));
+  TPS_CUDA(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  rep->time_ms = ms;
+  rep->iterations = it;
+  rep->final_residual = res;
+  rep->converged = converged ? 1 : 0;
+  if (status == TPS_OK && !converged) status = TPS_ERR_NOT_CONVERGED;
+  return status;
+}
+
+double dev_dot(tps_handle *h, const double *a, const double *b, cudaStream_t s)
+{
+  double *part = h->partial.as<double>();
+  TPS_CUDA(launch_dot_f64(a, b, h->fine().N, part, s));
+  TPS_CUDA(launch_reduce(part, 1, part + 2 * kRedBlocks, s));
+  double v = 0;
+  TPS_CUDA(cudaMemcpyAsync(&v, part + 2 * kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, s));
+  TPS_CUDA(cudaStreamSynchronize(s));
+  return v;
+}
+
+// preconditioner application dst = V(src), FP64 in/out
+void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, const double *src,
+                    cudaStream_t s)
+{
+  const int p = vprec_index(precision);
+  VcycleVectors &V = vcycle_vectors(h, p);
+  const int L = h->n_levels - 1;
+  const int64_t N = h->fine().N;
+  TPS_CUDA(launch_to_vcycle(V.d[L]->p, input_kind(precision), src, N, s));
+  vcycle_rec(h, L, p, symmetric, s);
+  TPS_CUDA(launch_from_vcycle(dst, V.su[L]->p, p == 1 ? 1 : 0, N, s));
+}
+
+// deal.II SolverGMRES semantics (left preconditioning, MGS, Givens) as used by
+// MultigridSolvers::solve_gmres (include/solver.cuh:1865-1910)
+int solve_gmres(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
+                tps_report *rep, cudaStream_t s)
+{
+  ensure_krylov(h);
+  vcycle_vectors(h, vprec_index(o.precision));
+  const LevelGeomH &g = h->fine();
+  const int64_t N = g.N;
+  const int basis = 28;  // max_n_tmp_vectors - 2 with deal.II's default of 30
+  const int nvec = std::min(basis, std::max(o.max_iter, 1)) + 1;
+  while (static_cast<int>(h->gmres_v.size()) < nvec) {
+    h->gmres_v.emplace_back(new DevBuf);
+    h->gmres_v.back()->alloc(sizeof(double) * N);
+  }
+  auto Vp = [&](int i) { return h->gmres_v[i]->as<double>(); };
+  double *pv = h->p.as<double>();
+  TPS_CUDA(cudaEventRecord(h->ev0, s));
+  TPS_CUDA(launch_copy_boundary(x, b, h->dim, g.N1, 8, s));
+  std::vector<double> H((basis + 1) * basis, 0.0), hv(basis + 1), gam(basis + 1), ci(basis + 1),
+      si(basis + 1);
+  int acc = 0, state = 0;  // 0 iterate, 1 success, 2 failure
+  double tol = o.abs_tol, rho0 = 0.0, last = 0.0;
+  int status = TPS_OK;
+  do {
+    fine_vmult64(h, pv, x, s);
+    TPS_CUDA(launch_sub_f64(pv, b, pv, N, s));
+    apply_vcycle64(h, o.precision, false, Vp(0), pv, s);
+    double rho = std::sqrt(dev_dot(h, Vp(0), Vp(0), s));
+    if (!std::isfinite(rho)) {
+      status = TPS_ERR_NONFINITE;
+      break;
+    }
+    if (acc == 0) {
+      rho0 = rho;
+      tol = std::max(o.abs_tol, o.rel_tol * rho);
+      rep->initial_residual = rho;
+    }
+    last = rho;
+    if (acc < TPS_MAX_HISTORY) rep->history[acc] = rho0 > 0 ? rho / rho0 : 0.0;
+    if (rho <= tol) { state = 1; break; }
+    if (acc >= o.max_iter) { state = 2; break; }
+    gam.assign(basis + 1, 0.0);
+    gam[0] = rho;
+    TPS_CUDA(launch_scale_f64(Vp(0), 1.0 / rho, N, s));
+    int dimk = 0;
+    for (int inner = 0; inner < basis && state == 0 && inner + 1 < nvec; ++inner) {
+      ++acc;
+      fine_vmult64(h, pv, Vp(inner), s);
+      apply_vcycle64(h, o.precision, false, Vp(inner + 1), pv, s);
+      dimk = inner + 1;
+      for (int i = 0; i < dimk; ++i) {
+        hv[i] = dev_dot(h, Vp(inner + 1), Vp(i), s);
+        TPS_CUDA(launch_axpy_f64(Vp(inner + 1), -hv[i], Vp(i), N, s));
+      }
+      const double sn = std::sqrt(dev_dot(h, Vp(inner + 1), Vp(inner + 1), s));
+      hv[inner + 1] = sn;
+      if (sn != 0.0) TPS_CUDA(launch_scale_f64(Vp(inner + 1), 1.0 / sn, N, s));
+      for (int i = 0; i < inner; ++i) {
+        const double c = ci[i], sv = si[i], d0 = hv[i];
+        hv[i] = c * d0 + sv * hv[i + 1];
+        hv[i + 1] = -sv * d0 + c * hv[i + 1];
+      }
+      const double r = 1.0 / std::sqrt(hv[inner] * hv[inner] + hv[inner + 1] * hv[inner + 1]);
+      si[inner] = hv[inner + 1] * r;
+      ci[inner] = hv[inner] * r;
+      hv[inner] = ci[inner] * hv[inner] + si[inner] * hv[inner + 1];
+      gam[inner + 1] = -si[inner] * gam[inner];
+      gam[inner] *= ci[inner];
+      for (int i = 0; i < dimk; ++i) H[i * basis + inner] = hv[i];
+      rho = std::fabs(gam[dimk]);
+      last = rho;
+      if (acc < TPS_MAX_HISTORY) rep->history[acc] = rho0 > 0 ? rho / rho0 : 0.0;
+      if (!std::isfinite(rho)) {
+        status = TPS_ERR_NONFINITE;
+        state = 2;
+      } else if (rho <= tol) {
+        state = 1;
+      } else if (acc >= o.max_iter) {
+        state = 2;
+      }
+    }
+    std::vector<double> y(dimk, 0.0);
+    for (int i = dimk - 1; i >= 0; --i) {
+      double t = gam[i];
+      for (int j = i + 1; j < dimk; ++j) t -= H[i * basis + j] * y[j];
+      y[i] = t / H[i * basis + i];
+    }
+    for (int i = 0; i < dimk; ++i) TPS_CUDA(launch_axpy_f64(x, y[i], Vp(i), N, s));
+  } while (state == 0 && status == TPS_OK);
+  TPS_CUDA(cudaEventRecord(h->ev1, s));
+  TPS_CUDA(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  rep->time_ms = ms;
+  rep->iterations = acc;
+  rep->final_residual = rho0 > 0 ? last / rho0 : 0.0;
+  rep->converged = state == 1 ? 1 : 0;
+  if (status == TPS_OK && state != 1) status = TPS_ERR_NOT_CONVERGED;
+  return status;
+}
+
+}  // namespace
+
+extern "C" {
+
+void tps_solve_opts_default(tps_solve_opts *o)
+{
+  if (!o) return;
+  o->driver = TPS_DRIVER_CG;
+  o->precision = TPS_VCYCLE_F32;
+  o->symmetric = 1;
+  o->max_iter = 100;
+  o->rel_tol = 1e-10;
+  o->abs_tol = 1e-16;
+  o->use_graph = 1;
+}
+
+int tps_create(const tps_problem *pb, tps_handle **out)
+{
+  g_create_error.clear();
+  if (!pb || !out) {
+    g_create_error = "null argument";
+    return TPS_ERR_INVALID;
+  }
+  *out = nullptr;
+  std::unique_ptr<tps_handle> h;
+  try {
+    if (pb->dim != 2 && pb->dim != 3) throw ApiError(TPS_ERR_INVALID, "dim must be 2 or 3");
+    if (pb->degree < 1 || pb->degree > kMaxDegree)
+      throw ApiError(TPS_ERR_UNSUPPORTED, "degree must be in 1..7");
+    if (pb->n_coarse < 2) throw ApiError(TPS_ERR_INVALID, "n_coarse must be >= 2");
+    if (pb->n_levels < 1 || pb->n_levels > 12) throw ApiError(TPS_ERR_INVALID, "n_levels must be in 1..12");
+    if (pb->kappa) throw ApiError(TPS_ERR_UNSUPPORTED, "variable coefficients are not supported by this build");
+    if (!(pb->relaxation > 0.0)) throw ApiError(TPS_ERR_INVALID, "relaxation must be positive");
+    const int64_t nf = static_cast<int64_t>(pb->n_coarse) << (pb->n_levels - 1);
+    const int64_t N1f = nf * pb->degree + 1;
+    const int64_t Nf = pb->dim == 3 ? N1f * N1f * N1f : N1f * N1f;
+    if (Nf >= (int64_t(1) << 31)) throw ApiError(TPS_ERR_INVALID, "finest level exceeds 2^31 DoFs");
+    h.reset(new tps_handle);
+    h->dim = pb->dim;
+    h->k = pb->degree;
+    h->n_coarse = pb->n_coarse;
+    h->n_levels = pb->n_levels;
+    h->omega = pb->relaxation;
+    h->device = pb->device;
+    TPS_CUDA(cudaSetDevice(pb->device));
+    for (int l = 0; l < pb->n_levels; ++l) {
+      LevelGeomH g;
+      g.n = pb->n_coarse << l;
+      g.N1 = g.n * pb->degree + 1;
+      g.N = pb->dim == 3 ? int64_t(g.N1) * g.N1 * g.N1 : int64_t(g.N1) * g.N1;
+      g.h = 1.0 / g.n;
+      h->lv.push_back(g);
+    }
+    h->kt = kernel_table(pb->degree);
+    if (!h->kt) throw ApiError(TPS_ERR_UNSUPPORTED, "degree not compiled in");
+    h->D = make_degree_data(pb->degree);
+    TPS_CUDA(h->kt->upload(h->D));
+    h->dense_coarse = pb->n_coarse != 2;
+    if (h->dense_coarse) {
+      const int64_t m1 = int64_t(pb->n_coarse) * pb->degree - 1;
+      const int64_t ni = pb->dim == 3 ? m1 * m1 * m1 : m1 * m1;
+      if (ni > 4096) throw ApiError(TPS_ERR_INVALID, "coarse level too large for the dense coarse solve");
+      build_dense_coarse(h.get());
+    }
+  } catch (const ApiError &e) {
+    g_create_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    g_create_error = "host allocation failed";
+    return TPS_ERR_ALLOC;
+  } catch (const std::exception &e) {
+    g_create_error = e.what();
+    return TPS_ERR_INVALID;
+  }
+  *out = h.release();
+  return TPS_OK;
+}
+
+int tps_destroy(tps_handle *h)
+{
+  if (!h) return TPS_ERR_INVALID;
+  cudaSetDevice(h->device);
+  delete h;
+  return TPS_OK;
+}
+
+const char *tps_last_error(const tps_handle *h)
+{
+  if (!h) return g_create_error.c_str();
+  return h->err.c_str();
+}
+
+int tps_level_info(const tps_handle *h, int level, int64_t *n_dofs, int *cells_per_dim)
+{
+  if (!h) return TPS_ERR_INVALID;
+  if (level < 0 || level >= h->n_levels) return TPS_ERR_INVALID;
+  if (n_dofs) *n_dofs = h->lv[level].N;
+  if (cells_per_dim) *cells_per_dim = h->lv[level].n;
+  return TPS_OK;
+}
+
+int tps_laplace_vmult(tps_handle *h, int level, int dtype, void *dst, const void *src, void *stream)
+{
+  return guarded(h, [&] {
+    check_level(h, level);
+    const int p = dt_index(dtype);
+    if (!dst || !src) throw ApiError(TPS_ERR_INVALID, "null vector");
+    if (dst == src) throw ApiError(TPS_ERR_INVALID, "dst and src must not alias");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const LevelGeomH &g = h->lv[level];
+    TPS_CUDA(h->kt->laplace[h->dim - 2][p](g, dst, src, nullptr, 0, s));
+    TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, p == 0 ? 8 : 4, s));
+  });
+}
+
+int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *b, int zero_init,
+                      int reverse, void *stream)
+{
+  return guarded(h, [&] {
+    check_level(h, level);
+    const int p = dt_index(dtype);
+    if (!x || !b) throw ApiError(TPS_ERR_INVALID, "null vector");
+    if (x == b) throw ApiError(TPS_ERR_INVALID, "x and b must not alias");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const LevelGeomH &g = h->lv[level];
+    if (zero_init) TPS_CUDA(cudaMemsetAsync(x, 0, (p == 0 ? 8 : 4) * g.N, s));
+    smoother_sweep(h, level, p, x, b, reverse != 0, s);
+  });
+}
+
+int tps_prolongate_add(tps_handle *h, int to_level, int dtype, void *fine, const void *coarse,
+                       void *stream)
+{
+  return guarded(h, [&] {
+    check_level(h, to_level, 1);
+    const int p = dt_index(dtype);
+    if (!fine || !coarse) throw ApiError(TPS_ERR_INVALID, "null vector");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    VcycleVectors &V = vcycle_vectors(h, p);
+    TPS_CUDA(h->kt->prolong[h->dim - 2][p](h->lv[to_level - 1], fine, coarse,
+                                           V.tmp[to_level]->p, s));
+  });
+}
+
+int tps_restrict_add(tps_handle *h, int from_level, int dtype, void *coarse, const void *fine,
+                     void *stream)
+{
+  return guarded(h, [&] {
+    check_level(h, from_level, 1);
+    const int p = dt_index(dtype);
+    if (!fine || !coarse) throw ApiError(TPS_ERR_INVALID, "null vector");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    VcycleVectors &V = vcycle_vectors(h, p);
+    TPS_CUDA(h->kt->restrict_[h->dim - 2][p](h->lv[from_level - 1], coarse, fine,
+                                             V.tmp[from_level]->p, 1, s));
+  });
+}
+
+int tps_vcycle(tps_handle *h, int precision, int symmetric, double *dst, const double *src,
+               void *stream)
+{
+  return guarded(h, [&] {
+    if (!dst || !src) throw ApiError(TPS_ERR_INVALID, "null vector");
+    apply_vcycle64(h, precision, symmetric != 0, dst, src, static_cast<cudaStream_t>(stream));
+  });
+}
+
+int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double *x,
+              tps_report *report, void *stream)
+{
+  int status = TPS_OK;
+  int rc = guarded(h, [&] {
+    if (!opts || !b || !x || !report) throw ApiError(TPS_ERR_INVALID, "null argument");
+    if (opts->max_iter < 1) throw ApiError(TPS_ERR_INVALID, "max_iter must be >= 1");
+    std::memset(report, 0, sizeof(*report));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (opts->driver == TPS_DRIVER_CG)
+      status = solve_cg(h, *opts, b, x, report, s);
+    else if (opts->driver == TPS_DRIVER_GMRES)
+      status = solve_gmres(h, *opts, b, x, report, s);
+    else
+      throw ApiError(TPS_ERR_INVALID, "unknown driver");
+  });
+  if (rc != TPS_OK) return rc;
+  if (status == TPS_ERR_NOT_CONVERGED) h->err = "solver did not converge within max_iter";
+  if (status == TPS_ERR_BREAKDOWN) h->err = "Krylov breakdown (p^T A p <= 0)";
+  if (status == TPS_ERR_NONFINITE) h->err = "non-finite residual";
+  return status;
+}
+
+int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host, double *x_host,
+                   tps_report *report)
+{
+  if (!h) return TPS_ERR_INVALID;
+  if (!b_host || !x_host) {
+    h->err = "null host buffer";
+    return TPS_ERR_INVALID;
+  }
+  int status = TPS_OK;
+  int rc = guarded(h, [&] {
+    const int64_t N = h->fine().N;
+    if (!h->own_stream) TPS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    cudaStream_t s = h->own_stream;
+    DevBuf db, dx;
+    db.alloc(sizeof(double) * N);
+    dx.alloc(sizeof(double) * N);
+    TPS_CUDA(cudaMemcpyAsync(db.p, b_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    TPS_CUDA(cudaMemcpyAsync(dx.p, x_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    status = tps_solve(h, opts, db.as<double>(), dx.as<double>(), report, s);
+    if (status == TPS_OK || status == TPS_ERR_NOT_CONVERGED) {
+      TPS_CUDA(cudaMemcpyAsync(x_host, dx.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+      TPS_CUDA(cudaStreamSynchronize(s));
+    }
+    // the cached graph refers to dx, which is freed on return
+    if (h->graph_x == dx.as<double>()) {
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+      h->graph_x = nullptr;
+    }
+  });
+  return rc != TPS_OK ? rc : status;
+}
+
+}  // extern "C"

@@ -1,0 +1,47 @@
+// Shared device-side definitions: per-degree 1D tables in __constant__
+// memory, level geometry, and launch helpers.
+//
+// Design note (B200): every 1D table is level-independent (mesh-size factors
+// are applied as scalars), so one copy per (degree, precision) lives in
+// constant memory.  Contraction loops are fully unrolled over compile-time
+// degrees, so each coefficient becomes an immediate constant-bank operand of
+// the FMA: no shared-memory or register traffic for the matrices.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace tps {
+
+template <int K>
+struct Dims {
+  static constexpr int NP = K + 1;      // DoFs per cell and direction
+  static constexpr int N1 = 2 * K + 1;  // DoFs per patch and direction
+  static constexpr int M = 2 * K - 1;   // interior DoFs per patch and direction
+};
+
+template <int K, typename T>
+struct DegreeTables {
+  T pmass[Dims<K>::N1 * Dims<K>::N1];   // patch mass (reference cells)
+  T plap[Dims<K>::N1 * Dims<K>::N1];    // patch stiffness (reference cells)
+  T cmass[Dims<K>::NP * Dims<K>::NP];   // cell mass
+  T clap[Dims<K>::NP * Dims<K>::NP];    // cell stiffness
+  T evec[Dims<K>::M * Dims<K>::M];      // interior eigenvectors (columns)
+  T eval[Dims<K>::M];                   // interior eigenvalues (reference scaling)
+  T prol[Dims<K>::N1 * Dims<K>::NP];    // 1D prolongation (child node x coarse basis)
+};
+
+template <int K, typename T>
+__constant__ DegreeTables<K, T> c_tables;
+
+// Geometry of one level: n cells per direction, N1 = n*k+1 DoFs per direction.
+struct LevelGeom {
+  int n;       // cells per direction
+  int N1;      // DoFs per direction
+  int64_t N;   // total DoFs
+  double h;    // cell size 1/n
+};
+
+inline unsigned ceil_div(int64_t a, int64_t b) { return static_cast<unsigned>((a + b - 1) / b); }
+
+}  // namespace tps

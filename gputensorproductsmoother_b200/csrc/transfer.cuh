@@ -1,0 +1,250 @@
+// Geometric MG transfer between a level with n_c cells per direction and its
+// uniform refinement (2 n_c cells), sm_100a.
+//
+// Reference behaviour: MGTransferCUDA::prolongate_and_add / restrict_and_add
+// (include/cuda_mg_transfer.template.cuh:575-671) with mg_kernel
+// (:21-369): per coarse cell, embed the (k+1)^d coarse values into the
+// (2k+1)^d child DoFs with the 1D prolongation, weight by 1/valence (0 on the
+// Dirichlet boundary), atomicAdd; restriction is the transpose.  Coarse
+// Dirichlet DoFs are zeroed before prolongation and after restriction.
+//
+// B200 design: the weighted per-cell scatter equals exact nodal interpolation
+// P = P1 (x) P1 (x) P1 restricted to interior DoFs, so both directions are
+// written as gathers (no atomics, deterministic):
+//   fine(i)   = sum_j P1(i_z,j_z) P1(i_y,j_y) P1(i_x,j_x) coarse(j)
+//   coarse(j) = sum_i P1(i_z,j_z) P1(i_y,j_y) P1(i_x,j_x) fine(i)
+// A 3D transfer is one 1D pass along z plus one 2D pass per xy-plane; the
+// intermediate (fine z x coarse y x coarse x, a quarter of the fine level)
+// lives in a per-level scratch buffer.
+#pragma once
+
+#include "tps_common.cuh"
+
+namespace tps {
+
+enum class XYOut { AddInterior = 0, SetInterior = 1, SetAll = 2 };
+
+template <int K>
+struct XYTile {
+  static constexpr int C = K <= 4 ? 4 : 2;  // coarse cells per CTA and direction
+  static constexpr int NT = 256;
+};
+
+// 1D prolongation of one coarse cell: v[0..k] coarse nodes -> out[0..2k-1]
+// fine nodes 2k*c + f (the node 2k*(c+1) belongs to the next cell).
+template <int K, typename T>
+__device__ __forceinline__ void prol_cell(const T (&v)[K + 1], T (&out)[2 * K])
+{
+  const DegreeTables<K, T> &tb = c_tables<K, T>;
+#pragma unroll
+  for (int f = 0; f < 2 * K; ++f) {
+    T s = T(0);
+#pragma unroll
+    for (int b = 0; b <= K; ++b) s += tb.prol[f * (K + 1) + b] * v[b];
+    out[f] = s;
+  }
+}
+
+// 1D restriction to the k coarse nodes c*k+b, b < k, from the fine nodes
+// v[0..4k] = 2k(c-1) .. 2k(c+1).
+template <int K, typename T>
+__device__ __forceinline__ void restr_cell(const T (&v)[4 * K + 1], T (&out)[K])
+{
+  const DegreeTables<K, T> &tb = c_tables<K, T>;
+#pragma unroll
+  for (int b = 0; b < K; ++b) {
+    T s = T(0);
+#pragma unroll
+    for (int f = 0; f <= 2 * K; ++f) s += tb.prol[f * (K + 1) + b] * v[2 * K + f];
+    if (b == 0) {
+      // left cell; its last child node 2k is the shared vertex counted above
+#pragma unroll
+      for (int f = 0; f < 2 * K; ++f) s += tb.prol[f * (K + 1) + K] * v[f];
+    }
+    out[b] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// xy pass, prolongation: coarse plane (N1c x N1c) -> fine plane (N1f x N1f).
+// in/out advance by the plane strides per blockIdx.z (plane index offset by
+// plane0).  Coarse boundary entries are read as zero when mask_in != 0.
+template <int K, typename T, XYOut OUT>
+__global__ void __launch_bounds__(XYTile<K>::NT)
+    prolong_xy_kernel(T *__restrict__ out, const T *__restrict__ in, int N1c, int N1f,
+                      int64_t in_plane, int64_t out_plane, int plane0, int mask_in)
+{
+  constexpr int C = XYTile<K>::C, NT = XYTile<K>::NT;
+  constexpr int WI = C * K + 1;  // coarse inputs per direction
+  constexpr int WO = 2 * K * C;  // fine outputs per direction
+  __shared__ T sIn[WI * WI];
+  __shared__ T sX[WI * WO];
+  const int plane = plane0 + blockIdx.z;
+  const T *inp = in + plane * in_plane;
+  T *outp = out + plane * out_plane;
+  const int cx0 = blockIdx.x * C, cy0 = blockIdx.y * C;
+  for (int e = threadIdx.x; e < WI * WI; e += NT) {
+    const int lx = e % WI, ly = e / WI;
+    const int gx = cx0 * K + lx, gy = cy0 * K + ly;
+    T v = T(0);
+    if (gx < N1c && gy < N1c) {
+      const bool bnd = gx == 0 || gx == N1c - 1 || gy == 0 || gy == N1c - 1;
+      if (!(mask_in && bnd)) v = inp[gx + static_cast<int64_t>(gy) * N1c];
+    }
+    sIn[e] = v;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < WI * C; t += NT) {
+    const int c = t % C, y = t / C;
+    T v[K + 1], o[2 * K];
+#pragma unroll
+    for (int b = 0; b <= K; ++b) v[b] = sIn[y * WI + c * K + b];
+    prol_cell<K, T>(v, o);
+#pragma unroll
+    for (int f = 0; f < 2 * K; ++f) sX[y * WO + c * 2 * K + f] = o[f];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < WO * C; t += NT) {
+    const int xx = t % WO, c = t / WO;
+    T v[K + 1], o[2 * K];
+#pragma unroll
+    for (int b = 0; b <= K; ++b) v[b] = sX[(c * K + b) * WO + xx];
+    prol_cell<K, T>(v, o);
+    const int gx = 2 * K * cx0 + xx;
+    if (gx >= N1f) continue;
+#pragma unroll
+    for (int f = 0; f < 2 * K; ++f) {
+      const int gy = 2 * K * (cy0 + c) + f;
+      if (gy >= N1f) continue;
+      const int64_t gi = gx + static_cast<int64_t>(gy) * N1f;
+      const bool interior = gx > 0 && gx < N1f - 1 && gy > 0 && gy < N1f - 1;
+      if constexpr (OUT == XYOut::AddInterior) {
+        if (interior) outp[gi] += o[f];
+      } else if constexpr (OUT == XYOut::SetInterior) {
+        if (interior) outp[gi] = o[f];
+      } else {
+        outp[gi] = o[f];
+      }
+    }
+  }
+}
+
+// xy pass, restriction: fine plane -> coarse plane.  Fine boundary entries
+// are read as zero (weight 0 on Dirichlet DoFs).  zero_plane != 0 writes
+// zeros instead (fine z-boundary planes).
+template <int K, typename T, XYOut OUT>
+__global__ void __launch_bounds__(XYTile<K>::NT)
+    restrict_xy_kernel(T *__restrict__ out, const T *__restrict__ in, int N1c, int N1f,
+                       int64_t in_plane, int64_t out_plane, int plane0, int n_planes_total)
+{
+  constexpr int C = XYTile<K>::C, NT = XYTile<K>::NT;
+  constexpr int WI = 2 * K * (C + 1) + 1;  // fine inputs per direction
+  constexpr int WO = C * K;                // coarse outputs per direction
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *sIn = reinterpret_cast<T *>(smem_raw);
+  T *sX = sIn + WI * WI;
+  const int plane = plane0 + blockIdx.z;
+  const bool zero_plane = n_planes_total > 1 && (plane == 0 || plane == n_planes_total - 1);
+  const T *inp = in + plane * in_plane;
+  T *outp = out + plane * out_plane;
+  const int cx0 = blockIdx.x * C, cy0 = blockIdx.y * C;
+  const int fx0 = 2 * K * (cx0 - 1), fy0 = 2 * K * (cy0 - 1);
+  for (int e = threadIdx.x; e < WI * WI; e += NT) {
+    const int lx = e % WI, ly = e / WI;
+    const int gx = fx0 + lx, gy = fy0 + ly;
+    T v = T(0);
+    if (!zero_plane && gx > 0 && gx < N1f - 1 && gy > 0 && gy < N1f - 1)
+      v = __ldg(&inp[gx + static_cast<int64_t>(gy) * N1f]);
+    sIn[e] = v;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < WI * C; t += NT) {
+    const int c = t % C, y = t / C;
+    T v[4 * K + 1], o[K];
+#pragma unroll
+    for (int j = 0; j <= 4 * K; ++j) v[j] = sIn[y * WI + c * 2 * K + j];
+    restr_cell<K, T>(v, o);
+#pragma unroll
+    for (int b = 0; b < K; ++b) sX[y * WO + c * K + b] = o[b];
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < WO * C; t += NT) {
+    const int xx = t % WO, c = t / WO;
+    T v[4 * K + 1], o[K];
+#pragma unroll
+    for (int j = 0; j <= 4 * K; ++j) v[j] = sX[(c * 2 * K + j) * WO + xx];
+    restr_cell<K, T>(v, o);
+    const int gx = K * cx0 + xx;
+    if (gx >= N1c) continue;
+#pragma unroll
+    for (int b = 0; b < K; ++b) {
+      const int gy = K * (cy0 + c) + b;
+      if (gy >= N1c) continue;
+      const int64_t gi = gx + static_cast<int64_t>(gy) * N1c;
+      const bool interior = gx > 0 && gx < N1c - 1 && gy > 0 && gy < N1c - 1;
+      if constexpr (OUT == XYOut::AddInterior) {
+        if (interior) outp[gi] += o[b];
+      } else if constexpr (OUT == XYOut::SetInterior) {
+        if (interior) outp[gi] = o[b];
+      } else {
+        outp[gi] = o[b];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z pass, prolongation: coarse (N1c planes of P entries) -> tmp (N1f planes of
+// P entries), P = N1c^2.  Input entries on the coarse boundary read as zero.
+template <int K, typename T>
+__global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coarse, int N1c,
+                                 int N1f, int n_cells_c)
+{
+  const int64_t P = static_cast<int64_t>(N1c) * N1c;
+  const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  const int c = blockIdx.y;  // coarse cell along z
+  if (idx >= P) return;
+  const int gx = static_cast<int>(idx % N1c), gy = static_cast<int>(idx / N1c);
+  const bool bxy = gx == 0 || gx == N1c - 1 || gy == 0 || gy == N1c - 1;
+  T v[K + 1], o[2 * K];
+#pragma unroll
+  for (int b = 0; b <= K; ++b) {
+    const int gz = c * K + b;
+    v[b] = (bxy || gz == 0 || gz == N1c - 1) ? T(0) : __ldg(&coarse[gz * P + idx]);
+  }
+  prol_cell<K, T>(v, o);
+#pragma unroll
+  for (int f = 0; f < 2 * K; ++f) tmp[(2 * K * c + f) * P + idx] = o[f];
+  if (c == n_cells_c - 1) tmp[(N1f - 1) * P + idx] = T(0);
+}
+
+// z pass, restriction: tmp (N1f planes of P = N1c^2 entries) -> coarse.
+template <int K, typename T, bool ADD>
+__global__ void restrict_z_kernel(T *__restrict__ coarse, const T *__restrict__ tmp, int N1c,
+                                  int N1f)
+{
+  const int64_t P = static_cast<int64_t>(N1c) * N1c;
+  const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  const int c = blockIdx.y;  // coarse cell along z: outputs c*k + b, b < k
+  if (idx >= P) return;
+  const int gx = static_cast<int>(idx % N1c), gy = static_cast<int>(idx / N1c);
+  if (gx == 0 || gx == N1c - 1 || gy == 0 || gy == N1c - 1) return;
+  T v[4 * K + 1], o[K];
+#pragma unroll
+  for (int j = 0; j <= 4 * K; ++j) {
+    const int fz = 2 * K * (c - 1) + j;
+    v[j] = (fz <= 0 || fz >= N1f - 1) ? T(0) : __ldg(&tmp[fz * P + idx]);
+  }
+  restr_cell<K, T>(v, o);
+#pragma unroll
+  for (int b = 0; b < K; ++b) {
+    const int gz = c * K + b;
+    if (gz == 0 || gz >= N1c - 1) continue;
+    if constexpr (ADD)
+      coarse[gz * P + idx] += o[b];
+    else
+      coarse[gz * P + idx] = o[b];
+  }
+}
+
+}  // namespace tps

@@ -1,0 +1,136 @@
+/*
+ * tps.h -- C ABI of the B200-native vertex-patch Schwarz multigrid path
+ * (continuous Q_k, uniform Cartesian meshes of the unit square/cube,
+ * homogeneous Dirichlet boundary, lexicographic DoF numbering x fastest).
+ *
+ * Every entry point returns a tps_status; no C++ exception crosses the ABI.
+ * Vectors are caller-owned DEVICE buffers of n_dofs(level) entries in the
+ * lexicographic layout of the reference (include/utilities.cuh:44-100), the
+ * element type given by `dtype`.  `stream` is a cudaStream_t (NULL = legacy
+ * default stream).  A handle is not re-entrant: use one handle per host
+ * thread / stream.
+ */
+#ifndef TPS_H
+#define TPS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  TPS_OK = 0,
+  TPS_ERR_INVALID = 1,      /* bad argument (null pointer, level, size, dtype) */
+  TPS_ERR_CUDA = 2,         /* CUDA runtime/driver error */
+  TPS_ERR_ALLOC = 3,        /* device or host allocation failed */
+  TPS_ERR_NOT_CONVERGED = 4,/* solver hit max_iter before the tolerance */
+  TPS_ERR_BREAKDOWN = 5,    /* Krylov breakdown (p^T A p <= 0, zero norm) */
+  TPS_ERR_NONFINITE = 6,    /* NaN/Inf met in a residual or input */
+  TPS_ERR_UNSUPPORTED = 7   /* degree/dimension not compiled in */
+} tps_status;
+
+typedef enum { TPS_F64 = 0, TPS_F32 = 1 } tps_dtype;
+
+typedef struct tps_handle tps_handle;
+
+/* Problem description (replaces the reference's compile-time CT:: constants,
+ * scripts/ct_parameter.py.in:109-124, and the DoFHandler/Triangulation set-up
+ * of apps/poisson.cu:152-181). */
+typedef struct {
+  int dim;             /* 2 or 3 */
+  int degree;          /* k, 1..7 */
+  int n_coarse;        /* cells per direction of the coarsest level (>= 2) */
+  int n_levels;        /* the finest level has n_coarse * 2^(n_levels-1) cells/direction */
+  double relaxation;   /* smoother damping omega (reference default 1.0) */
+  const double *kappa; /* HOST array of per-cell coefficients on the finest level
+                          (lexicographic cells) or NULL for kappa = 1 */
+  int device;          /* CUDA device ordinal */
+} tps_problem;
+
+/* Lifecycle.  Replaces MultigridSolvers' constructor (include/solver.cuh:1545-1744):
+ * builds every level's patch colouring, 1D matrices, FP64 eigendecompositions,
+ * transfer data and the device work vectors. */
+int tps_create(const tps_problem *problem, tps_handle **out);
+int tps_destroy(tps_handle *h);
+/* Message of the last failing call on `h` (or of the last failing tps_create when
+ * h is NULL).  Valid until the next call on the same handle/thread. */
+const char *tps_last_error(const tps_handle *h);
+/* Number of DoFs (boundary included) and cells per direction of `level`
+ * (0 = coarsest, n_levels-1 = finest). */
+int tps_level_info(const tps_handle *h, int level, int64_t *n_dofs, int *cells_per_dim);
+
+/* LaplaceOperator::vmult (include/laplace_operator.cuh:86-101):
+ * dst = A_level src on interior rows, dst = src on Dirichlet rows. */
+int tps_laplace_vmult(tps_handle *h, int level, int dtype, void *dst, const void *src,
+                      void *stream);
+
+/* PatchSmoother::vmult / step (include/patch_smoother.cuh:155-292): one 2^d-coloured
+ * multiplicative vertex-patch sweep x <- S(x, b); zero_init=1 is vmult (x := 0 first).
+ * reverse=1 runs the colours in reverse order (symmetric post-smoothing). */
+int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *b,
+                      int zero_init, int reverse, void *stream);
+
+/* MGTransferCUDA::prolongate_and_add / restrict_and_add
+ * (include/cuda_mg_transfer.template.cuh:575-671).  to_level / from_level is the
+ * finer level (>= 1). */
+int tps_prolongate_add(tps_handle *h, int to_level, int dtype, void *fine, const void *coarse,
+                       void *stream);
+int tps_restrict_add(tps_handle *h, int from_level, int dtype, void *coarse, const void *fine,
+                     void *stream);
+
+/* V-cycle precision. */
+typedef enum {
+  TPS_VCYCLE_F64 = 0,        /* FP64 V-cycle */
+  TPS_VCYCLE_F32 = 1,        /* FP32 smoother/operator/transfer inside the V-cycle */
+  TPS_VCYCLE_F64_ROUNDED = 2 /* FP64 V-cycle fed with FP32-rounded input: the
+                                reference's "double" V-cycle (include/solver.cuh:64-78) */
+} tps_vcycle_precision;
+
+/* MultigridSolvers::vmult (include/solver.cuh:1915-1930): dst = V-cycle(src) on the
+ * finest level, FP64 in and out. symmetric=1 post-smooths in reverse colour order. */
+int tps_vcycle(tps_handle *h, int precision, int symmetric, double *dst, const double *src,
+               void *stream);
+
+typedef enum {
+  TPS_DRIVER_CG = 0,    /* flexible CG, FP64 outer iteration (iterative refinement) */
+  TPS_DRIVER_GMRES = 1  /* deal.II SolverGMRES semantics: left-preconditioned, basis 28,
+                           convergence on the preconditioned residual (include/solver.cuh:1865-1910) */
+} tps_driver;
+
+typedef struct {
+  int driver;          /* tps_driver */
+  int precision;       /* tps_vcycle_precision */
+  int symmetric;       /* reverse-order post-smoothing (CG default 1; GMRES parity 0) */
+  int max_iter;        /* CG default 100; reference GMRES default 20 (MAX_STEPS_) */
+  double rel_tol;      /* CG: ||b-Ax||/||b||; GMRES: reduction of the preconditioned residual */
+  double abs_tol;      /* GMRES absolute tolerance (reference: 1e-16) */
+  int use_graph;       /* capture one iteration as a CUDA graph (CG) */
+} tps_solve_opts;
+
+#define TPS_MAX_HISTORY 256
+typedef struct {
+  int iterations;
+  int converged;
+  double initial_residual;  /* ||r_0|| (CG: true residual; GMRES: preconditioned) */
+  double final_residual;    /* relative to initial */
+  double history[TPS_MAX_HISTORY]; /* relative residual per iteration, history[0] = 1 */
+  double time_ms;           /* device time of the solve (CUDA events on the stream) */
+} tps_report;
+
+void tps_solve_opts_default(tps_solve_opts *opts);
+
+/* Solve A x = b on the finest level.  b, x: DEVICE FP64 buffers (x holds the initial
+ * guess on entry).  Replaces MultigridSolvers::solve_gmres and adds the MG-CG driver. */
+int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double *x,
+              tps_report *report, void *stream);
+
+/* Same solve with HOST buffers; the host<->device copies are part of the call. */
+int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
+                   double *x_host, tps_report *report);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

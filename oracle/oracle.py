@@ -1,0 +1,206 @@
+"""TEST INFRASTRUCTURE ONLY: ctypes binding of the CPU oracle (liboracle.so).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg use
+this module, and only as the checker.  Parity status: UNPINNED against the
+reference (LuciaZhang9/GPUTensorProductSmoother cannot be built here: it needs
+deal.II with CUDA+MPI, CMakeLists.txt:81-102, and ships no golden vectors).  The
+oracle is pinned instead against the independent numpy/scipy fixtures in
+tests/golden/ and against mathematical known answers.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_fp = ctypes.POINTER(ctypes.c_float)
+
+
+def build() -> str:
+    """Compile liboracle.so with the oracle's own Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.orc_fe1d.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
+        L.orc_patch_matrices.argtypes = [ctypes.c_int, _dp, _dp]
+        L.orc_gen_eig.argtypes = [ctypes.c_int, _dp, _dp, _dp, _dp]
+        L.orc_patch_eigen.argtypes = [ctypes.c_int, ctypes.c_double, _dp, _dp]
+        L.orc_gauss.argtypes = [ctypes.c_int, _dp, _dp]
+        L.orc_gauss_lobatto.argtypes = [ctypes.c_int, _dp]
+        for suf, ptr in (("_d", _dp), ("_f", _fp)):
+            getattr(L, "orc_laplace_vmult" + suf).argtypes = [
+                ctypes.c_int, ctypes.c_int, ctypes.c_int, ptr, ptr, _dp]
+            getattr(L, "orc_smoother_step" + suf).argtypes = [
+                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ptr, ptr,
+                ctypes.c_int, ctypes.c_int, _dp]
+            getattr(L, "orc_prolongate_add" + suf).argtypes = [
+                ctypes.c_int, ctypes.c_int, ctypes.c_int, ptr, ptr]
+            getattr(L, "orc_restrict_add" + suf).argtypes = [
+                ctypes.c_int, ctypes.c_int, ctypes.c_int, ptr, ptr]
+        L.orc_hier_create.restype = ctypes.c_void_p
+        L.orc_hier_create.argtypes = [ctypes.c_int] * 4 + [_dp]
+        L.orc_hier_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_hier_ndofs.restype = ctypes.c_long
+        L.orc_hier_ndofs.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.orc_vcycle.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]
+        L.orc_vcycle_level.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, _dp, _dp]
+        L.orc_fine_vmult.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_coarse_solve.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_solve_cg.restype = ctypes.c_int
+        L.orc_solve_cg.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp,
+                                   ctypes.c_double, ctypes.c_int, _dp]
+        L.orc_solve_gmres.restype = ctypes.c_int
+        L.orc_solve_gmres.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_double,
+                                      ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(_dp)
+    return a.ctypes.data_as(_fp)
+
+
+def _sfx(dtype):
+    return "_d" if np.dtype(dtype) == np.float64 else "_f"
+
+
+def fe1d(k):
+    nodes = np.zeros(k + 1)
+    mass = np.zeros((k + 1, k + 1))
+    lap = np.zeros((k + 1, k + 1))
+    prol = np.zeros((2 * k + 1, k + 1))
+    assert lib().orc_fe1d(k, _p(nodes), _p(mass), _p(lap), _p(prol)) == 0
+    return nodes, mass, lap, prol
+
+
+def gauss(nq):
+    x = np.zeros(nq)
+    w = np.zeros(nq)
+    lib().orc_gauss(nq, _p(x), _p(w))
+    return x, w
+
+
+def patch_matrices(k):
+    n1 = 2 * k + 1
+    pm = np.zeros((n1, n1))
+    pl = np.zeros((n1, n1))
+    assert lib().orc_patch_matrices(k, _p(pm), _p(pl)) == 0
+    return pm, pl
+
+
+def patch_eigen(k, h):
+    m = 2 * k - 1
+    S = np.zeros((m, m))
+    lam = np.zeros(m)
+    assert lib().orc_patch_eigen(k, h, _p(S), _p(lam)) == 0
+    return S, lam
+
+
+def ndofs(dim, k, n):
+    return (n * k + 1) ** dim
+
+
+def laplace_vmult(dim, k, n, src, kappa=None):
+    src = np.ascontiguousarray(src)
+    dst = np.zeros_like(src)
+    kap = None if kappa is None else np.ascontiguousarray(kappa, dtype=np.float64)
+    getattr(lib(), "orc_laplace_vmult" + _sfx(src.dtype))(dim, k, n, _p(dst), _p(src), _p(kap))
+    return dst
+
+
+def smoother_step(dim, k, n, x, b, omega=1.0, zero_init=False, reverse=False, kappa=None):
+    """In-place coloured sweep on a copy of x; returns the new x."""
+    x = np.array(x, copy=True)
+    b = np.ascontiguousarray(b, dtype=x.dtype)
+    kap = None if kappa is None else np.ascontiguousarray(kappa, dtype=np.float64)
+    getattr(lib(), "orc_smoother_step" + _sfx(x.dtype))(
+        dim, k, n, omega, _p(x), _p(b), int(zero_init), int(reverse), _p(kap))
+    return x
+
+
+def prolongate_add(dim, k, nc, fine, coarse):
+    fine = np.array(fine, copy=True)
+    coarse = np.ascontiguousarray(coarse, dtype=fine.dtype)
+    getattr(lib(), "orc_prolongate_add" + _sfx(fine.dtype))(dim, k, nc, _p(fine), _p(coarse))
+    return fine
+
+
+def restrict_add(dim, k, nc, coarse, fine):
+    coarse = np.array(coarse, copy=True)
+    fine = np.ascontiguousarray(fine, dtype=coarse.dtype)
+    getattr(lib(), "orc_restrict_add" + _sfx(coarse.dtype))(dim, k, nc, _p(coarse), _p(fine))
+    return coarse
+
+
+class Hierarchy:
+    """Geometric MG hierarchy of n_coarse * 2^l cells per direction, l < n_levels."""
+
+    def __init__(self, dim, k, n_coarse, n_levels, kappa=None):
+        self.dim, self.k, self.n_coarse, self.n_levels = dim, k, n_coarse, n_levels
+        self._kappa = None if kappa is None else np.ascontiguousarray(kappa, dtype=np.float64)
+        self.h = lib().orc_hier_create(dim, k, n_coarse, n_levels, _p(self._kappa))
+        if not self.h:
+            raise ValueError("invalid hierarchy parameters")
+        self.N = lib().orc_hier_ndofs(self.h, n_levels - 1)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().orc_hier_destroy(self.h)
+            self.h = None
+
+    def ndofs(self, level):
+        return lib().orc_hier_ndofs(self.h, level)
+
+    def vmult(self, src):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        dst = np.zeros_like(src)
+        lib().orc_fine_vmult(self.h, _p(dst), _p(src))
+        return dst
+
+    def vcycle(self, src, precision=0, symmetric=False, level=None):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        dst = np.zeros_like(src)
+        lvl = self.n_levels - 1 if level is None else level
+        lib().orc_vcycle_level(self.h, precision, int(symmetric), lvl, _p(dst), _p(src))
+        return dst
+
+    def coarse_solve(self, src):
+        src = np.ascontiguousarray(src, dtype=np.float64)
+        dst = np.zeros_like(src)
+        lib().orc_coarse_solve(self.h, _p(dst), _p(src))
+        return dst
+
+    def solve_cg(self, b, precision=0, symmetric=True, rel_tol=1e-10, max_it=100, x0=None):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b) if x0 is None else np.array(x0, dtype=np.float64, copy=True)
+        hist = np.zeros(max_it + 1)
+        it = lib().orc_solve_cg(self.h, precision, int(symmetric), _p(b), _p(x), rel_tol, max_it,
+                                _p(hist))
+        return x, it, hist[: it + 1]
+
+    def solve_gmres(self, b, precision=2, reduce=1e-9, abs_tol=1e-16, max_it=20, basis=28):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        hist = np.zeros(max_it + 1)
+        it = lib().orc_solve_gmres(self.h, precision, _p(b), _p(x), reduce, abs_tol, max_it, basis,
+                                   _p(hist))
+        return x, it, hist[: it + 1]
