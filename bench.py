@@ -40,7 +40,34 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson3d_q4_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--mode", default="solve", choices=["solve", "smoother"],
+                    help="smoother: only time the finest-level FP32 smoother sweeps "
+                         "(a small command for kernel profiling)")
     return ap.parse_args()
+
+
+def run_smoother_only(args):
+    """Times --steps sweeps of the finest-level FP32 smoother (8 colour launches
+    each) after --warmup sweeps and prints one JSON line."""
+    import torch
+    import gputensorproductsmoother_b200 as tps
+    from gputensorproductsmoother_b200 import _lib as L
+    from gputensorproductsmoother_b200 import problems
+    dim, k, n, _ = problems.WORKLOADS[args.workload]
+    P = tps.PoissonProblem(dim, k, n)
+    lf = P.n_levels - 1
+    stream = torch.cuda.Stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    ms = ctypes.c_double()
+    if args.warmup > 0:
+        L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, args.warmup, ctypes.byref(ms), sp),
+                P.handle)
+    L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, max(args.steps, 1), ctypes.byref(ms), sp),
+            P.handle)
+    total, per = smoother_bytes(dim, k, n, 4)
+    print(json.dumps({"mode": "smoother", "workload": args.workload, "ms_per_sweep": ms.value,
+                      "algorithmic_GBps": total / (ms.value * 1e-3) / 1e9}), flush=True)
+    P.close()
 
 
 class ClockSampler:
@@ -203,6 +230,9 @@ def main():
     if args.impl == "reference":
         run_reference(args)
         return
+    if args.mode == "smoother":
+        run_smoother_only(args)
+        return
     import numpy as np
     import torch
     import torch.distributed as dist
@@ -265,21 +295,14 @@ def main():
         err = (torch.linalg.norm(x - x64) / torch.linalg.norm(x64)).item()
         resid_check = rep.final_residual
 
-        # dominant kernel: the FP32 fine-level smoother sweep (8 colour launches)
+        # dominant kernel: the FP32 fine-level smoother sweep (8 colour launches of
+        # the TMA-staged kernel on the V-cycle's work vectors), CUDA events on `stream`
         lf = P.n_levels - 1
-        d32 = torch.randn(P.n_dofs(lf), dtype=torch.float32, device="cuda")
-        s32 = torch.zeros_like(d32)
-        sm = tps.PatchSmoother(P, lf)
-        for _ in range(3):
-            sm.step(s32, d32)
-        reps = 20
-        torch.cuda.synchronize()
-        e0.record(stream)
-        for _ in range(reps):
-            sm.step(s32, d32)
-        e1.record(stream)
-        torch.cuda.synchronize()
-        sweep_ms = e0.elapsed_time(e1) / reps
+        msw = ctypes.c_double()
+        sp = ctypes.c_void_p(stream.cuda_stream)
+        L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, 3, ctypes.byref(msw), sp), P.handle)
+        L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, 20, ctypes.byref(msw), sp), P.handle)
+        sweep_ms = msw.value
         bytes_sweep, per_colour = smoother_bytes(dim, k, n, 4)
         colours = sum(1 for c in per_colour if c > 0)
         launch_ms = sweep_ms / colours
@@ -335,7 +358,7 @@ def main():
                 "h2d_bytes_per_step": 2 * 8 * P.n_dofs(), "d2h_bytes_per_step": 8 * P.n_dofs()},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak, "traffic": None,
-                     "kernel": "smoother_colour_kernel<3,4,float>",
+                     "kernel": "smoother3d_kernel<4,float,TMA>",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": launch_bytes, "launch_ms": launch_ms},
         "gpu_launches": args.steps * launches_per_solve(dim, P.n_levels, rep.iterations),

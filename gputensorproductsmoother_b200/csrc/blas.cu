@@ -6,6 +6,13 @@
 namespace tps {
 namespace {
 
+__device__ __forceinline__ int64_t pad_index(int64_t i, PadMap pm)
+{
+  if (pm.sy == pm.N1) return i;
+  const int64_t row = i / pm.N1;
+  return row * pm.sy + (i - row * pm.N1);
+}
+
 // d_kind/z_kind: 0 = FP64, 1 = FP32, 2 = FP64 rounded through FP32
 __device__ __forceinline__ void store_kind(void *d, int kind, int64_t i, double v)
 {
@@ -103,7 +110,7 @@ __global__ void __launch_bounds__(kRedThreads) reduce_kernel(const double *parti
 }
 
 __global__ void __launch_bounds__(kRedThreads)
-    cg_init_kernel(const double *r, const double *b, void *d, int d_kind, int64_t n,
+    cg_init_kernel(const double *r, const double *b, void *d, int d_kind, PadMap pm, int64_t n,
                    double *partial)
 {
   __shared__ double sh[32];
@@ -113,7 +120,7 @@ __global__ void __launch_bounds__(kRedThreads)
     const double ri = r[i], bi = b[i];
     s_rr += ri * ri;
     s_bb += bi * bi;
-    store_kind(d, d_kind, i, ri);
+    store_kind(d, d_kind, pad_index(i, pm), ri);
   }
   s_rr = block_sum<kRedThreads>(s_rr, sh);
   s_bb = block_sum<kRedThreads>(s_bb, sh);
@@ -179,14 +186,14 @@ struct OpBeta {
 };
 
 __global__ void __launch_bounds__(kRedThreads)
-    cg_first_direction_kernel(double *p, const void *z, int z_kind, const double *r, int64_t n,
-                              double *partial)
+    cg_first_direction_kernel(double *p, const void *z, int z_kind, PadMap pm, const double *r,
+                              int64_t n, double *partial)
 {
   __shared__ double sh[32];
   double s = 0.0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const double zi = load_kind(z, z_kind, i);
+    const double zi = load_kind(z, z_kind, pad_index(i, pm));
     p[i] = zi;
     s += r[i] * zi;
   }
@@ -196,7 +203,7 @@ __global__ void __launch_bounds__(kRedThreads)
 
 __global__ void __launch_bounds__(kRedThreads)
     cg_update_xr_kernel(double *x, double *r, const double *p, const double *q, void *d,
-                        int d_kind, int64_t n, double *partial, const CGScalars *sc)
+                        int d_kind, PadMap pm, int64_t n, double *partial, const CGScalars *sc)
 {
   __shared__ double sh[32];
   const double alpha = sc->alpha;
@@ -207,21 +214,21 @@ __global__ void __launch_bounds__(kRedThreads)
     const double ri = r[i] - alpha * q[i];
     r[i] = ri;
     s += ri * ri;
-    store_kind(d, d_kind, i, ri);
+    store_kind(d, d_kind, pad_index(i, pm), ri);
   }
   s = block_sum<kRedThreads>(s, sh);
   if (threadIdx.x == 0) partial[blockIdx.x] = s;
 }
 
 __global__ void __launch_bounds__(kRedThreads)
-    cg_dots_z_kernel(const void *z, int z_kind, const double *q, const double *r, int64_t n,
-                     double *partial)
+    cg_dots_z_kernel(const void *z, int z_kind, PadMap pm, const double *q, const double *r,
+                     int64_t n, double *partial)
 {
   __shared__ double sh[32];
   double s1 = 0.0, s2 = 0.0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-    const double zi = load_kind(z, z_kind, i);
+    const double zi = load_kind(z, z_kind, pad_index(i, pm));
     s1 += zi * q[i];
     s2 += zi * r[i];
   }
@@ -233,13 +240,13 @@ __global__ void __launch_bounds__(kRedThreads)
   }
 }
 
-__global__ void cg_update_p_kernel(double *p, const void *z, int z_kind, int64_t n,
+__global__ void cg_update_p_kernel(double *p, const void *z, int z_kind, PadMap pm, int64_t n,
                                    const CGScalars *sc)
 {
   const double beta = sc->beta;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    p[i] = load_kind(z, z_kind, i) + beta * p[i];
+    p[i] = load_kind(z, z_kind, pad_index(i, pm)) + beta * p[i];
 }
 
 __global__ void axpy_kernel(double *y, double a, const double *x, int64_t n)
@@ -263,18 +270,18 @@ __global__ void sub_kernel(double *dst, const double *a, const double *b, int64_
     dst[i] = a[i] - b[i];
 }
 
-__global__ void to_vcycle_kernel(void *d, int d_kind, const double *src, int64_t n)
+__global__ void to_vcycle_kernel(void *d, int d_kind, PadMap pm, const double *src, int64_t n)
 {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    store_kind(d, d_kind, i, src[i]);
+    store_kind(d, d_kind, pad_index(i, pm), src[i]);
 }
 
-__global__ void from_vcycle_kernel(double *dst, const void *z, int z_kind, int64_t n)
+__global__ void from_vcycle_kernel(double *dst, const void *z, int z_kind, PadMap pm, int64_t n)
 {
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
-    dst[i] = load_kind(z, z_kind, i);
+    dst[i] = load_kind(z, z_kind, pad_index(i, pm));
 }
 
 // dense coarse solve: su[idx[i]] = sum_j inv[i][j] d[idx[j]], one warp per row
@@ -337,10 +344,10 @@ cudaError_t launch_reduce(const double *partial, int n_dots, double *out, cudaSt
   reduce_kernel<<<n_dots, kRedThreads, 0, s>>>(partial, out);
   return cudaGetLastError();
 }
-cudaError_t launch_cg_init(const double *r, const double *b, void *d, int d_kind, int64_t n,
-                           double *partial, cudaStream_t s)
+cudaError_t launch_cg_init(const double *r, const double *b, void *d, int d_kind, PadMap pm,
+                           int64_t n, double *partial, cudaStream_t s)
 {
-  cg_init_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(r, b, d, d_kind, n, partial);
+  cg_init_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(r, b, d, d_kind, pm, n, partial);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_finalize_init(const double *partial, CGScalars *sc, cudaStream_t s)
@@ -348,10 +355,10 @@ cudaError_t launch_cg_finalize_init(const double *partial, CGScalars *sc, cudaSt
   finalize_kernel<2><<<1, kRedThreads, 0, s>>>(partial, sc, OpInit{});
   return cudaGetLastError();
 }
-cudaError_t launch_cg_first_direction(double *p, const void *z, int z_kind, const double *r,
-                                      int64_t n, double *partial, cudaStream_t s)
+cudaError_t launch_cg_first_direction(double *p, const void *z, int z_kind, PadMap pm,
+                                      const double *r, int64_t n, double *partial, cudaStream_t s)
 {
-  cg_first_direction_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(p, z, z_kind, r, n, partial);
+  cg_first_direction_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(p, z, z_kind, pm, r, n, partial);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_finalize_rz(const double *partial, CGScalars *sc, cudaStream_t s)
@@ -367,10 +374,10 @@ cudaError_t launch_cg_alpha(const double *p, const double *q, int64_t n, double 
   return cudaGetLastError();
 }
 cudaError_t launch_cg_update_xr(double *x, double *r, const double *p, const double *q, void *d,
-                                int d_kind, int64_t n, double *partial, const CGScalars *sc,
-                                cudaStream_t s)
+                                int d_kind, PadMap pm, int64_t n, double *partial,
+                                const CGScalars *sc, cudaStream_t s)
 {
-  cg_update_xr_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, q, d, d_kind, n, partial, sc);
+  cg_update_xr_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, q, d, d_kind, pm, n, partial, sc);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_finalize_rr(const double *partial, CGScalars *sc, cudaStream_t s)
@@ -378,17 +385,17 @@ cudaError_t launch_cg_finalize_rr(const double *partial, CGScalars *sc, cudaStre
   finalize_kernel<1><<<1, kRedThreads, 0, s>>>(partial, sc, OpRr{});
   return cudaGetLastError();
 }
-cudaError_t launch_cg_beta(const void *z, int z_kind, const double *q, const double *r, int64_t n,
-                           double *partial, CGScalars *sc, cudaStream_t s)
+cudaError_t launch_cg_beta(const void *z, int z_kind, PadMap pm, const double *q, const double *r,
+                           int64_t n, double *partial, CGScalars *sc, cudaStream_t s)
 {
-  cg_dots_z_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(z, z_kind, q, r, n, partial);
+  cg_dots_z_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(z, z_kind, pm, q, r, n, partial);
   finalize_kernel<2><<<1, kRedThreads, 0, s>>>(partial, sc, OpBeta{});
   return cudaGetLastError();
 }
-cudaError_t launch_cg_update_p(double *p, const void *z, int z_kind, int64_t n,
+cudaError_t launch_cg_update_p(double *p, const void *z, int z_kind, PadMap pm, int64_t n,
                                const CGScalars *sc, cudaStream_t s)
 {
-  cg_update_p_kernel<<<stream_grid(n, 256), 256, 0, s>>>(p, z, z_kind, n, sc);
+  cg_update_p_kernel<<<stream_grid(n, 256), 256, 0, s>>>(p, z, z_kind, pm, n, sc);
   return cudaGetLastError();
 }
 cudaError_t launch_axpy_f64(double *y, double a, const double *x, int64_t n, cudaStream_t s)
@@ -406,14 +413,16 @@ cudaError_t launch_sub_f64(double *dst, const double *a, const double *b, int64_
   sub_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, a, b, n);
   return cudaGetLastError();
 }
-cudaError_t launch_to_vcycle(void *d, int d_kind, const double *src, int64_t n, cudaStream_t s)
+cudaError_t launch_to_vcycle(void *d, int d_kind, PadMap pm, const double *src, int64_t n,
+                             cudaStream_t s)
 {
-  to_vcycle_kernel<<<stream_grid(n, 256), 256, 0, s>>>(d, d_kind, src, n);
+  to_vcycle_kernel<<<stream_grid(n, 256), 256, 0, s>>>(d, d_kind, pm, src, n);
   return cudaGetLastError();
 }
-cudaError_t launch_from_vcycle(double *dst, const void *z, int z_kind, int64_t n, cudaStream_t s)
+cudaError_t launch_from_vcycle(double *dst, const void *z, int z_kind, PadMap pm, int64_t n,
+                               cudaStream_t s)
 {
-  from_vcycle_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, z, z_kind, n);
+  from_vcycle_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, z, z_kind, pm, n);
   return cudaGetLastError();
 }
 cudaError_t launch_coarse_dense(const void *inv, const int *idx, int n_int, void *su,

@@ -12,6 +12,13 @@ namespace tps {
 constexpr int kRedBlocks = 592;   // 4 x 148 SMs
 constexpr int kRedThreads = 512;
 
+// Index map from a lexicographic vector to a level vector whose rows of N1
+// entries are sy apart (sy == N1: identity).
+struct PadMap {
+  int N1;
+  int64_t sy;
+};
+
 // Device-resident scalars of the CG iteration (no host round trip inside an
 // iteration, so one iteration can be captured in a CUDA graph).
 struct CGScalars {
@@ -43,27 +50,27 @@ cudaError_t launch_reduce(const double *partial, int n_dots, double *out, cudaSt
 // --- fused CG steps (flexible CG, FP64 outer) ---------------------------
 // r = b - A x was formed by the operator; rr, and the V-cycle input d
 // (FP32, FP64, or FP64 rounded through FP32) are produced from r.
-cudaError_t launch_cg_init(const double *r, const double *b, void *d, int d_kind, int64_t n,
-                           double *partial, cudaStream_t s);
+cudaError_t launch_cg_init(const double *r, const double *b, void *d, int d_kind, PadMap pm,
+                           int64_t n, double *partial, cudaStream_t s);
 // finalize: sc.rr = sum, sc.bb = sum
 cudaError_t launch_cg_finalize_init(const double *partial, CGScalars *sc, cudaStream_t s);
 // p = z, partial(r.z) ; z in V-cycle precision
-cudaError_t launch_cg_first_direction(double *p, const void *z, int z_kind, const double *r,
-                                      int64_t n, double *partial, cudaStream_t s);
+cudaError_t launch_cg_first_direction(double *p, const void *z, int z_kind, PadMap pm,
+                                      const double *r, int64_t n, double *partial, cudaStream_t s);
 cudaError_t launch_cg_finalize_rz(const double *partial, CGScalars *sc, cudaStream_t s);
 // partial(p.q) then alpha = rz / pq
 cudaError_t launch_cg_alpha(const double *p, const double *q, int64_t n, double *partial,
                             CGScalars *sc, cudaStream_t s);
 // x += alpha p, r -= alpha q, d = conv(r), partial(r.r)
 cudaError_t launch_cg_update_xr(double *x, double *r, const double *p, const double *q, void *d,
-                                int d_kind, int64_t n, double *partial, const CGScalars *sc,
-                                cudaStream_t s);
+                                int d_kind, PadMap pm, int64_t n, double *partial,
+                                const CGScalars *sc, cudaStream_t s);
 cudaError_t launch_cg_finalize_rr(const double *partial, CGScalars *sc, cudaStream_t s);
 // partial(z.q), partial(z.r) then beta = -alpha zq / rz, rz = z.r
-cudaError_t launch_cg_beta(const void *z, int z_kind, const double *q, const double *r, int64_t n,
-                           double *partial, CGScalars *sc, cudaStream_t s);
+cudaError_t launch_cg_beta(const void *z, int z_kind, PadMap pm, const double *q, const double *r,
+                           int64_t n, double *partial, CGScalars *sc, cudaStream_t s);
 // p = z + beta p
-cudaError_t launch_cg_update_p(double *p, const void *z, int z_kind, int64_t n,
+cudaError_t launch_cg_update_p(double *p, const void *z, int z_kind, PadMap pm, int64_t n,
                                const CGScalars *sc, cudaStream_t s);
 
 // generic FP64 helpers for the GMRES driver
@@ -72,8 +79,10 @@ cudaError_t launch_scale_f64(double *y, double a, int64_t n, cudaStream_t s);
 cudaError_t launch_sub_f64(double *dst, const double *a, const double *b, int64_t n,
                            cudaStream_t s);  // dst = a - b
 // V-cycle input from an FP64 vector and FP64 output from the V-cycle result
-cudaError_t launch_to_vcycle(void *d, int d_kind, const double *src, int64_t n, cudaStream_t s);
-cudaError_t launch_from_vcycle(double *dst, const void *z, int z_kind, int64_t n, cudaStream_t s);
+cudaError_t launch_to_vcycle(void *d, int d_kind, PadMap pm, const double *src, int64_t n,
+                             cudaStream_t s);
+cudaError_t launch_from_vcycle(double *dst, const void *z, int z_kind, PadMap pm, int64_t n,
+                               cudaStream_t s);
 cudaError_t launch_fill(void *dst, int elem_bytes, int64_t n, cudaStream_t s);  // zero
 
 }  // namespace tps

@@ -17,24 +17,49 @@ struct LevelGeomH {
   double h;   // cell size
 };
 
+// Layout of a level vector: x fastest, row pitch sy >= N1, plane pitch sz
+// (lexicographic: sy = N1, sz = N1^2; V-cycle work vectors pad sy to 16 bytes).
+struct VecLayout {
+  int N1;
+  int64_t sy, sz;
+};
+
+// Opaque storage of the two TMA descriptors (CUtensorMap, 128 bytes each)
+// of one smoother launch: x (patch boxes) and b (patch interiors).
+struct SmootherMaps {
+  alignas(64) unsigned char x[128];
+  alignas(64) unsigned char b[128];
+  int valid = 0;
+};
+
 struct KernelTable {
   int degree;
   // copy the 1D tables of this degree into constant memory of the current device
   cudaError_t (*upload)(const DegreeData &);
   // dst = A src on interior rows (mode 0) or dst = rhs - A src (mode 1);
   // boundary rows of dst are not written
-  cudaError_t (*laplace[2][2])(const LevelGeomH &, void *dst, const void *src, const void *rhs,
-                               int mode, cudaStream_t);
-  // one colour of the patch sweep
-  cudaError_t (*smoother[2][2])(const LevelGeomH &, void *x, const void *b, int colour,
-                                double omega, cudaStream_t);
+  cudaError_t (*laplace[2][2])(const LevelGeomH &, const VecLayout &, void *dst, const void *src,
+                               const void *rhs, int mode, cudaStream_t);
+  // one colour of the patch sweep; maps (3D, TMA path) may be null; zero_x
+  // declares x == 0 on entry; err receives 1 if a bounded wait gave up
+  cudaError_t (*smoother[2][2])(const LevelGeomH &, const VecLayout &, void *x, const void *b,
+                                int colour, double omega, int zero_x, const SmootherMaps *maps,
+                                int *err, cudaStream_t);
+  // TMA descriptors of the 3D smoother for vectors x, b with layout l ([dtype])
+  cudaError_t (*encode_maps[2])(const VecLayout &l, void *x, const void *b, SmootherMaps *out);
   // fine += P coarse (interior fine DoFs); geometry of the COARSE level
-  cudaError_t (*prolong[2][2])(const LevelGeomH &coarse, void *fine, const void *coarse_v,
-                               void *tmp, cudaStream_t);
+  cudaError_t (*prolong[2][2])(const LevelGeomH &coarse, const VecLayout &lc, const VecLayout &lf,
+                               void *fine, const void *coarse_v, void *tmp, cudaStream_t);
   // coarse (+)= R fine on interior coarse DoFs; geometry of the COARSE level
-  cudaError_t (*restrict_[2][2])(const LevelGeomH &coarse, void *coarse_v, const void *fine,
-                                 void *tmp, int add, cudaStream_t);
+  cudaError_t (*restrict_[2][2])(const LevelGeomH &coarse, const VecLayout &lc,
+                                 const VecLayout &lf, void *coarse_v, const void *fine, void *tmp,
+                                 int add, cudaStream_t);
 };
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda
+// link dependency): rank-3 tiled map, no swizzle, zero out-of-bounds fill.
+cudaError_t encode_tiled_3d(void *map_out, bool f64, void *base, const uint64_t dims[3],
+                            const uint64_t strides_bytes[2], const uint32_t box[3]);
 
 const KernelTable *kernel_table(int degree);
 

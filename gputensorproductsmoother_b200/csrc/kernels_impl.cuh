@@ -8,6 +8,7 @@
 #include "kernel_table.h"
 #include "laplace.cuh"
 #include "smoother.cuh"
+#include "smoother3d.cuh"
 #include "transfer.cuh"
 
 namespace tps {
@@ -32,6 +33,19 @@ cudaError_t upload_one(const DegreeData &D)
   for (int i = 0; i < M * M; ++i) t.evec[i] = static_cast<T>(D.evec[i]);
   for (int i = 0; i < M; ++i) t.eval[i] = static_cast<T>(D.eval[i]);
   for (int i = 0; i < N1 * NP; ++i) t.prol[i] = static_cast<T>(D.prol[i]);
+  // folded interior rows of the centro-symmetric patch matrices (FP64, then rounded)
+  auto fold = [&](const std::vector<double> &A, T *fe, T *fo) {
+    for (int r = 0; r < K; ++r) {
+      const int i = r + 1;  // matrix row; r == K-1 is the centre row K
+      for (int j = 0; j < K; ++j) {
+        fe[r * (K + 1) + j] = static_cast<T>(0.5 * (A[i * N1 + j] + A[i * N1 + N1 - 1 - j]));
+        if (r < K - 1) fo[r * K + j] = static_cast<T>(0.5 * (A[i * N1 + j] - A[i * N1 + N1 - 1 - j]));
+      }
+      fe[r * (K + 1) + K] = static_cast<T>(A[i * N1 + K]);
+    }
+  };
+  fold(D.pmass, t.pmass_fe, t.pmass_fo);
+  fold(D.plap, t.plap_fe, t.plap_fo);
   return cudaMemcpyToSymbol(c_tables<K, T>, &t, sizeof(t));
 }
 
@@ -65,7 +79,8 @@ cudaError_t set_attributes()
                            static_cast<int>(bytes));                                    \
   if (e != cudaSuccess) return e;
   TPS_SET((smoother_colour_kernel<2, K, T>), (smoother_smem<2, T>()));
-  TPS_SET((smoother_colour_kernel<3, K, T>), (smoother_smem<3, T>()));
+  TPS_SET((smoother3d_kernel<K, T, true>), (Sm3<K, T>::BYTES));
+  TPS_SET((smoother3d_kernel<K, T, false>), (Sm3<K, T>::BYTES));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Vmult>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Residual>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<3, K, T, OpMode::Vmult>), (laplace_smem<3, T>()));
@@ -87,8 +102,8 @@ cudaError_t upload(const DegreeData &D)
 }
 
 template <int DIM, typename T>
-cudaError_t laplace(const LevelGeomH &g, void *dst, const void *src, const void *rhs, int mode,
-                    cudaStream_t s)
+cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const void *src,
+                    const void *rhs, int mode, cudaStream_t s)
 {
   using Tl = OpTile<DIM, K>;
   const dim3 grid(ceil_div(g.n, Tl::CX), ceil_div(g.n, Tl::CY), DIM == 3 ? ceil_div(g.n, Tl::CZ) : 1);
@@ -96,56 +111,121 @@ cudaError_t laplace(const LevelGeomH &g, void *dst, const void *src, const void 
   const size_t smem = laplace_smem<DIM, T>();
   if (mode == 0)
     laplace_kernel<DIM, K, T, OpMode::Vmult><<<grid, Tl::NT, smem, s>>>(
-        static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, scale);
+        static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, l.sy, l.sz, scale);
   else
     laplace_kernel<DIM, K, T, OpMode::Residual><<<grid, Tl::NT, smem, s>>>(
         static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1,
-        g.n, scale);
+        l.sy, l.sz, scale);
   return cudaGetLastError();
 }
 
-template <int DIM, typename T>
-cudaError_t smoother(const LevelGeomH &g, void *x, const void *b, int colour, double omega,
-                     cudaStream_t s)
+template <typename T, bool TMA>
+int sm3_grid(int n_batches)
 {
-  using S = SmootherShape<DIM, K>;
+  static int per_sm = -1, n_sm = 0;
+  if (per_sm < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_kernel<K, T, TMA>,
+                                                      Sm3<K, T>::NT, Sm3<K, T>::BYTES) != cudaSuccess ||
+        per_sm < 1)
+      per_sm = 1;
+  }
+  const int g = per_sm * n_sm;
+  return n_batches < g ? n_batches : g;
+}
+
+template <int DIM, typename T>
+cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const void *b, int colour,
+                     double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t s)
+{
   int nx, ny, nz, count;
   colour_lattice(DIM, g.n, colour, nx, ny, nz, count);
   if (count == 0) return cudaSuccess;
   const double sc = stiffness_scale(DIM, g.h);
   const int cx = colour & 1, cy = (colour >> 1) & 1, cz = (colour >> 2) & 1;
-  smoother_colour_kernel<DIM, K, T><<<ceil_div(count, S::PPB), S::NT, smoother_smem<DIM, T>(), s>>>(
-      static_cast<T *>(x), static_cast<const T *>(b), g.N1, nx, ny, count, cx, cy, cz,
-      static_cast<T>(sc), static_cast<T>(1.0 / sc), static_cast<T>(omega));
+  if constexpr (DIM == 2) {
+    using S = SmootherShape<DIM, K>;
+    (void)zero_x;  // the 2D kernel always reads x (x == 0 gives the same sweep)
+    (void)maps;
+    (void)err;
+    smoother_colour_kernel<DIM, K, T><<<ceil_div(count, S::PPB), S::NT, smoother_smem<DIM, T>(), s>>>(
+        static_cast<T *>(x), static_cast<const T *>(b), l.sy, l.sz, nx, ny, count, cx, cy, cz,
+        static_cast<T>(sc), static_cast<T>(1.0 / sc), static_cast<T>(omega));
+  } else {
+    using S = Sm3<K, T>;
+    Sm3Args a;
+    a.nx_c = nx;
+    a.ny_c = ny;
+    a.n_patches = count;
+    a.cx = cx;
+    a.cy = cy;
+    a.cz = cz;
+    a.n_batches = static_cast<int>(ceil_div(count, S::PPB));
+    a.zero_x = zero_x;
+    a.sy = l.sy;
+    a.sz = l.sz;
+    const T scale = static_cast<T>(sc), fd = static_cast<T>(omega / sc);
+    if (maps && maps->valid) {
+      smoother3d_kernel<K, T, true><<<sm3_grid<T, true>(a.n_batches), S::NT, S::BYTES, s>>>(
+          *reinterpret_cast<const CUtensorMap *>(maps->x),
+          *reinterpret_cast<const CUtensorMap *>(maps->b), static_cast<T *>(x),
+          static_cast<const T *>(b), a, scale, fd, err);
+    } else {
+      CUtensorMap none{};
+      smoother3d_kernel<K, T, false><<<a.n_batches, S::NT, S::BYTES, s>>>(
+          none, none, static_cast<T *>(x), static_cast<const T *>(b), a, scale, fd, err);
+    }
+  }
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t encode_maps(const VecLayout &l, void *x, const void *b, SmootherMaps *out)
+{
+  using S = Sm3<K, T>;
+  out->valid = 0;
+  const uint64_t es = sizeof(T);
+  if ((l.sy * es) % 16 || (l.sz * es) % 16 || reinterpret_cast<uintptr_t>(x) % 16 ||
+      reinterpret_cast<uintptr_t>(b) % 16)
+    return cudaSuccess;  // pitch not TMA-compatible: the plain-load variant is used
+  const uint64_t dims[3] = {static_cast<uint64_t>(l.N1), static_cast<uint64_t>(l.N1),
+                            static_cast<uint64_t>(l.N1)};
+  const uint64_t str[2] = {static_cast<uint64_t>(l.sy) * es, static_cast<uint64_t>(l.sz) * es};
+  const uint32_t bx[3] = {S::W, S::N1, S::N1}, bb[3] = {S::W, S::M, S::M};
+  cudaError_t e = encode_tiled_3d(out->x, sizeof(T) == 8, x, dims, str, bx);
+  if (e == cudaSuccess) e = encode_tiled_3d(out->b, sizeof(T) == 8, const_cast<void *>(b), dims, str, bb);
+  if (e == cudaSuccess) out->valid = 1;
+  return e;
+}
+
 template <int DIM, typename T>
-cudaError_t prolong(const LevelGeomH &gc, void *fine, const void *coarse, void *tmp, cudaStream_t s)
+cudaError_t prolong(const LevelGeomH &gc, const VecLayout &lc, const VecLayout &lf, void *fine,
+                    const void *coarse, void *tmp, cudaStream_t s)
 {
   constexpr int C = XYTile<K>::C;
   const int N1c = gc.N1, N1f = 2 * gc.n * K + 1;
   const unsigned gxy = ceil_div(gc.n, C);
   if constexpr (DIM == 2) {
     prolong_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, 1), XYTile<K>::NT, 0, s>>>(
-        static_cast<T *>(fine), static_cast<const T *>(coarse), N1c, N1f, 0, 0, 0, 1);
+        static_cast<T *>(fine), static_cast<const T *>(coarse), N1c, N1f, lc.sy, 0, lf.sy, 0, 0, 1);
   } else {
     const int64_t P = static_cast<int64_t>(N1c) * N1c;
     prolong_z_kernel<K, T><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
-        static_cast<T *>(tmp), static_cast<const T *>(coarse), N1c, N1f, gc.n);
+        static_cast<T *>(tmp), static_cast<const T *>(coarse), N1c, N1f, gc.n, lc.sy, lc.sz);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // fine interior planes 1..N1f-2 from tmp planes 1..N1f-2
     prolong_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, N1f - 2), XYTile<K>::NT, 0, s>>>(
-        static_cast<T *>(fine), static_cast<const T *>(tmp), N1c, N1f, P,
-        static_cast<int64_t>(N1f) * N1f, 1, 0);
+        static_cast<T *>(fine), static_cast<const T *>(tmp), N1c, N1f, N1c, P, lf.sy, lf.sz, 1, 0);
   }
   return cudaGetLastError();
 }
 
 template <int DIM, typename T>
-cudaError_t restrict_(const LevelGeomH &gc, void *coarse, const void *fine, void *tmp, int add,
-                      cudaStream_t s)
+cudaError_t restrict_(const LevelGeomH &gc, const VecLayout &lc, const VecLayout &lf, void *coarse,
+                      const void *fine, void *tmp, int add, cudaStream_t s)
 {
   constexpr int C = XYTile<K>::C;
   const int N1c = gc.N1, N1f = 2 * gc.n * K + 1;
@@ -154,23 +234,22 @@ cudaError_t restrict_(const LevelGeomH &gc, void *coarse, const void *fine, void
   if constexpr (DIM == 2) {
     if (add)
       restrict_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, 1), XYTile<K>::NT, smem, s>>>(
-          static_cast<T *>(coarse), static_cast<const T *>(fine), N1c, N1f, 0, 0, 0, 1);
+          static_cast<T *>(coarse), static_cast<const T *>(fine), N1c, N1f, lf.sy, 0, lc.sy, 0, 0, 1);
     else
       restrict_xy_kernel<K, T, XYOut::SetInterior><<<dim3(gxy, gxy, 1), XYTile<K>::NT, smem, s>>>(
-          static_cast<T *>(coarse), static_cast<const T *>(fine), N1c, N1f, 0, 0, 0, 1);
+          static_cast<T *>(coarse), static_cast<const T *>(fine), N1c, N1f, lf.sy, 0, lc.sy, 0, 0, 1);
   } else {
     const int64_t P = static_cast<int64_t>(N1c) * N1c;
     restrict_xy_kernel<K, T, XYOut::SetAll><<<dim3(gxy, gxy, N1f), XYTile<K>::NT, smem, s>>>(
-        static_cast<T *>(tmp), static_cast<const T *>(fine), N1c, N1f,
-        static_cast<int64_t>(N1f) * N1f, P, 0, N1f);
+        static_cast<T *>(tmp), static_cast<const T *>(fine), N1c, N1f, lf.sy, lf.sz, N1c, P, 0, N1f);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (add)
       restrict_z_kernel<K, T, true><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
-          static_cast<T *>(coarse), static_cast<const T *>(tmp), N1c, N1f);
+          static_cast<T *>(coarse), static_cast<const T *>(tmp), N1c, N1f, lc.sy, lc.sz);
     else
       restrict_z_kernel<K, T, false><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
-          static_cast<T *>(coarse), static_cast<const T *>(tmp), N1c, N1f);
+          static_cast<T *>(coarse), static_cast<const T *>(tmp), N1c, N1f, lc.sy, lc.sz);
   }
   return cudaGetLastError();
 }
@@ -188,6 +267,7 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
      {&deg_impl::laplace<3, double>, &deg_impl::laplace<3, float>}},
     {{&deg_impl::smoother<2, double>, &deg_impl::smoother<2, float>},
      {&deg_impl::smoother<3, double>, &deg_impl::smoother<3, float>}},
+    {&deg_impl::encode_maps<double>, &deg_impl::encode_maps<float>},
     {{&deg_impl::prolong<2, double>, &deg_impl::prolong<2, float>},
      {&deg_impl::prolong<3, double>, &deg_impl::prolong<3, float>}},
     {{&deg_impl::restrict_<2, double>, &deg_impl::restrict_<2, float>},

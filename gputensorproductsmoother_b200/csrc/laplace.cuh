@@ -67,7 +67,7 @@ __device__ __forceinline__ void band_apply(const T *mat /* (k+1)^2 cell matrix *
 template <int DIM, int K, typename T, OpMode MODE>
 __global__ void __launch_bounds__(OpTile<DIM, K>::NT)
     laplace_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs,
-                   int N1g, int n_cells, T scale)
+                   int N1g, int64_t sy, int64_t sz, T scale)
 {
   using Tl = OpTile<DIM, K>;
   constexpr int NT = Tl::NT, WX = Tl::WX, WY = Tl::WY, WZ = Tl::WZ;
@@ -80,16 +80,29 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT)
 
   const int cx0 = blockIdx.x * Tl::CX, cy0 = blockIdx.y * Tl::CY, cz0 = blockIdx.z * Tl::CZ;
   const int gx0 = cx0 * K, gy0 = cy0 * K, gz0 = DIM == 3 ? cz0 * K : 0;
-  const int64_t sy = N1g, sz = static_cast<int64_t>(N1g) * N1g;
-
-  // stage 0: input brick with a one-cell halo (zero outside the mesh)
-  for (int e = threadIdx.x; e < Tl::IN; e += NT) {
-    const int lx = e % WX, ly = (e / WX) % WY, lz = DIM == 3 ? e / (WX * WY) : 0;
-    const int gx = gx0 - K + lx, gy = gy0 - K + ly, gz = DIM == 3 ? gz0 - K + lz : 0;
-    T v = T(0);
-    if (gx >= 0 && gx < N1g && gy >= 0 && gy < N1g && (DIM == 2 || (gz >= 0 && gz < N1g)))
-      v = __ldg(&src[gx + gy * sy + gz * sz]);
-    sIn[e] = v;
+  // stage 0: input brick with a one-cell halo (zero outside the mesh); the
+  // loop has a compile-time trip count and is unrolled in chunks so that
+  // every thread keeps a chunk of independent loads in flight
+  constexpr int NLOAD = (Tl::IN + NT - 1) / NT;
+  constexpr int CH = NLOAD < 8 ? NLOAD : 8;
+#pragma unroll 1
+  for (int i0 = 0; i0 < NLOAD; i0 += CH) {
+    T v[CH];
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      const int e = threadIdx.x + (i0 + c) * NT;
+      const int lx = e % WX, ly = (e / WX) % WY, lz = DIM == 3 ? e / (WX * WY) : 0;
+      const int gx = gx0 - K + lx, gy = gy0 - K + ly, gz = DIM == 3 ? gz0 - K + lz : 0;
+      v[c] = T(0);
+      if (i0 + c < NLOAD && e < Tl::IN && gx >= 0 && gx < N1g && gy >= 0 && gy < N1g &&
+          (DIM == 2 || (gz >= 0 && gz < N1g)))
+        v[c] = __ldg(&src[gx + gy * sy + gz * sz]);
+    }
+#pragma unroll
+    for (int c = 0; c < CH; ++c) {
+      const int e = threadIdx.x + (i0 + c) * NT;
+      if (i0 + c < NLOAD && e < Tl::IN) sIn[e] = v[c];
+    }
   }
   __syncthreads();
 
@@ -185,7 +198,6 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT)
       }
     }
   }
-  (void)n_cells;
   (void)OZ;
 }
 

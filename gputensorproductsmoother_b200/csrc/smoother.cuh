@@ -1,4 +1,5 @@
-// Fused vertex-patch smoother kernel (one launch per colour), sm_100a.
+// Fused vertex-patch smoother kernel (one launch per colour), sm_100a; used
+// for 2D levels (3D levels use smoother3d.cuh).
 //
 // Reference behaviour: LevelVertexPatch::patch_loop_fused + loop_kernel_fused_cf
 // / loop_kernel_fused_l (include/patch_base.template.cuh:379-543,
@@ -95,8 +96,8 @@ __device__ __forceinline__ void apply_evec(const T (&in)[Dims<K>::M], T (&out)[D
 
 template <int DIM, int K, typename T>
 __global__ void __launch_bounds__(SmootherShape<DIM, K>::NT)
-    smoother_colour_kernel(T *__restrict__ x, const T *__restrict__ b, int N1g, int nx_c,
-                           int ny_c, int n_patches_c, int cx, int cy, int cz, T scale,
+    smoother_colour_kernel(T *__restrict__ x, const T *__restrict__ b, int64_t sy, int64_t sz,
+                           int nx_c, int ny_c, int n_patches_c, int cx, int cy, int cz, T scale,
                            T inv_scale, T omega)
 {
   using S = SmootherShape<DIM, K>;
@@ -106,7 +107,6 @@ __global__ void __launch_bounds__(SmootherShape<DIM, K>::NT)
   T *smem = reinterpret_cast<T *>(smem_raw);
 
   const int p0 = blockIdx.x * PPB;
-  const int64_t sy = N1g, sz = static_cast<int64_t>(N1g) * N1g;
 
   // first DoF of local patch lp (include/patch_base.template.cuh:1371-1397)
   auto first_dof = [&](int lp, bool &valid) -> int64_t {

@@ -99,11 +99,15 @@ struct DevBuf {
   T *as() const { return static_cast<T *>(p); }
 };
 
-// V-cycle work vectors of one precision
+// V-cycle work vectors of one precision.  In 3D their rows are padded to a
+// 16-byte pitch so the smoother can stage patch boxes with TMA.
 struct VcycleVectors {
   bool ready = false;
   std::vector<std::unique_ptr<DevBuf>> d, su, t, tmp;  // per level
+  std::vector<VecLayout> layout;                       // per level
+  std::vector<SmootherMaps> maps;                      // TMA descriptors (x = su, b = d)
   DevBuf coarse_inv;                                   // dense coarse inverse
+  DevBuf coarse_idx;                                   // interior DoFs of the coarse level
 };
 
 }  // namespace
@@ -119,8 +123,9 @@ struct tps_handle {
   bool dense_coarse = false;
   int n_int_coarse = 0;
   std::vector<double> coarse_inv_host;  // n_int^2, FP64
-  DevBuf coarse_idx;
+  std::vector<int> coarse_coord;        // (x, y, z) of each interior coarse DoF
   VcycleVectors vc[2];  // [0] FP64, [1] FP32
+  DevBuf err_flag;      // set by a kernel whose bounded wait gave up
   // Krylov work vectors (fine level, FP64)
   DevBuf r, p, q, partial, scalars;
   std::vector<std::unique_ptr<DevBuf>> gmres_v;
@@ -253,14 +258,15 @@ void build_dense_coarse(tps_handle *h)
     for (int i = 0; i < ni; ++i) inv[static_cast<size_t>(i) * ni + c] = col[i];
   }
   h->coarse_inv_host = std::move(inv);
-  std::vector<int> gidx(ni);
-  for (int i = 0; i < ni; ++i) {
-    int x, y, z;
-    coord(i, x, y, z);
-    gidx[i] = x + y * N1 + (dim == 3 ? z * N1 * N1 : 0);
-  }
-  h->coarse_idx.alloc(sizeof(int) * ni);
-  TPS_CUDA(cudaMemcpy(h->coarse_idx.p, gidx.data(), sizeof(int) * ni, cudaMemcpyHostToDevice));
+  h->coarse_coord.resize(3 * static_cast<size_t>(ni));
+  for (int i = 0; i < ni; ++i) coord(i, h->coarse_coord[3 * i], h->coarse_coord[3 * i + 1],
+                                     h->coarse_coord[3 * i + 2]);
+}
+
+VecLayout lex_layout(const tps_handle *h, int level)
+{
+  const int N1 = h->lv[level].N1;
+  return VecLayout{N1, N1, int64_t(N1) * N1};
 }
 
 VcycleVectors &vcycle_vectors(tps_handle *h, int p)
@@ -268,24 +274,46 @@ VcycleVectors &vcycle_vectors(tps_handle *h, int p)
   VcycleVectors &V = h->vc[p];
   if (V.ready) return V;
   const size_t es = p == 0 ? sizeof(double) : sizeof(float);
+  const int align = static_cast<int>(16 / es);
   V.d.clear();
   V.su.clear();
   V.t.clear();
   V.tmp.clear();
+  V.layout.clear();
+  V.maps.assign(h->n_levels, SmootherMaps{});
+  if (!h->err_flag.p) h->err_flag.alloc(sizeof(int));
   for (int l = 0; l < h->n_levels; ++l) {
     const LevelGeomH &g = h->lv[l];
+    VecLayout lay;
+    lay.N1 = g.N1;
+    lay.sy = h->dim == 3 ? (g.N1 + align - 1) / align * align : g.N1;
+    lay.sz = lay.sy * g.N1;
+    const size_t n = static_cast<size_t>(h->dim == 3 ? lay.sz * g.N1 : lay.sy * g.N1);
+    V.layout.push_back(lay);
     V.d.emplace_back(new DevBuf);
     V.su.emplace_back(new DevBuf);
     V.t.emplace_back(new DevBuf);
     V.tmp.emplace_back(new DevBuf);
-    V.d[l]->alloc(es * g.N);
-    V.su[l]->alloc(es * g.N);
-    V.t[l]->alloc(es * g.N);
+    V.d[l]->alloc(es * n);
+    V.su[l]->alloc(es * n);
+    V.t[l]->alloc(es * n);
     if (l > 0 && h->dim == 3) {
       // transfer scratch: fine z x coarse y x coarse x
       const int64_t N1c = h->lv[l - 1].N1;
       V.tmp[l]->alloc(es * static_cast<size_t>(g.N1) * N1c * N1c);
     }
+    if (h->dim == 3)
+      TPS_CUDA(h->kt->encode_maps[p](lay, V.su[l]->p, V.d[l]->p, &V.maps[l]));
+  }
+  if (h->dense_coarse) {
+    const VecLayout &lc = V.layout[0];
+    const int ni = h->n_int_coarse;
+    std::vector<int> gidx(ni);
+    for (int i = 0; i < ni; ++i)
+      gidx[i] = static_cast<int>(h->coarse_coord[3 * i] + h->coarse_coord[3 * i + 1] * lc.sy +
+                                 h->coarse_coord[3 * i + 2] * lc.sz);
+    V.coarse_idx.alloc(sizeof(int) * ni);
+    TPS_CUDA(cudaMemcpy(V.coarse_idx.p, gidx.data(), sizeof(int) * ni, cudaMemcpyHostToDevice));
   }
   if (h->dense_coarse) {
     const size_t n2 = h->coarse_inv_host.size();
@@ -302,13 +330,18 @@ VcycleVectors &vcycle_vectors(tps_handle *h, int p)
   return V;
 }
 
-void smoother_sweep(tps_handle *h, int level, int p, void *x, const void *b, bool reverse,
-                    cudaStream_t s)
+// one coloured sweep; x_zero declares x == 0 on entry (the first colour then
+// skips reading x); maps (may be null) select the TMA path
+void smoother_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void *x, const void *b,
+                    bool reverse, bool x_zero, const SmootherMaps *maps, cudaStream_t s)
 {
+  if (!h->err_flag.p) h->err_flag.alloc(sizeof(int));
   const int nc = 1 << h->dim;
   for (int i = 0; i < nc; ++i) {
     const int c = reverse ? nc - 1 - i : i;
-    TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], x, b, c, h->omega, s));
+    TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], lay, x, b, c, h->omega,
+                                            (x_zero && i == 0) ? 1 : 0, maps,
+                                            h->err_flag.as<int>(), s));
   }
 }
 
@@ -316,12 +349,13 @@ void coarse_solve(tps_handle *h, int p, cudaStream_t s)
 {
   VcycleVectors &V = h->vc[p];
   const size_t es = p == 0 ? sizeof(double) : sizeof(float);
-  TPS_CUDA(cudaMemsetAsync(V.su[0]->p, 0, es * h->lv[0].N, s));
+  const VecLayout &lay = V.layout[0];
+  TPS_CUDA(cudaMemsetAsync(V.su[0]->p, 0, es * V.su[0]->bytes / es, s));
   if (!h->dense_coarse) {
     // one vertex patch covers every interior DoF: the smoother is an exact solve
-    smoother_sweep(h, 0, p, V.su[0]->p, V.d[0]->p, false, s);
+    smoother_sweep(h, 0, p, lay, V.su[0]->p, V.d[0]->p, false, true, &V.maps[0], s);
   } else {
-    TPS_CUDA(launch_coarse_dense(V.coarse_inv.p, h->coarse_idx.as<int>(), h->n_int_coarse,
+    TPS_CUDA(launch_coarse_dense(V.coarse_inv.p, V.coarse_idx.as<int>(), h->n_int_coarse,
                                  V.su[0]->p, V.d[0]->p, static_cast<int>(es), s));
   }
 }
@@ -335,18 +369,19 @@ void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s)
     coarse_solve(h, p, s);
     return;
   }
-  const size_t es = p == 0 ? sizeof(double) : sizeof(float);
   const LevelGeomH &g = h->lv[level];
+  const VecLayout &lay = V.layout[level], &lc = V.layout[level - 1];
   const int di = h->dim - 2;
-  TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, es * g.N, s));
-  smoother_sweep(h, level, p, V.su[level]->p, V.d[level]->p, false, s);
-  TPS_CUDA(h->kt->laplace[di][p](g, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s));
-  TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], V.d[level - 1]->p, V.t[level]->p,
+  TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, V.su[level]->bytes, s));
+  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, true, &V.maps[level], s);
+  TPS_CUDA(h->kt->laplace[di][p](g, lay, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s));
+  TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], lc, lay, V.d[level - 1]->p, V.t[level]->p,
                                    V.tmp[level]->p, 0, s));
   vcycle_rec(h, level - 1, p, symmetric, s);
-  TPS_CUDA(h->kt->prolong[di][p](h->lv[level - 1], V.su[level]->p, V.su[level - 1]->p,
+  TPS_CUDA(h->kt->prolong[di][p](h->lv[level - 1], lc, lay, V.su[level]->p, V.su[level - 1]->p,
                                  V.tmp[level]->p, s));
-  smoother_sweep(h, level, p, V.su[level]->p, V.d[level]->p, symmetric, s);
+  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, symmetric, false,
+                 &V.maps[level], s);
 }
 
 int vprec_index(int precision)
@@ -356,10 +391,16 @@ int vprec_index(int precision)
 }
 int input_kind(int precision) { return precision; }  // 0 f64, 1 f32, 2 f64-rounded
 
+PadMap fine_padmap(tps_handle *h, int p)
+{
+  const VecLayout &l = h->vc[p].layout.back();
+  return PadMap{l.N1, l.sy};
+}
+
 void fine_vmult64(tps_handle *h, double *dst, const double *src, cudaStream_t s)
 {
   const LevelGeomH &g = h->fine();
-  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, dst, src, nullptr, 0, s));
+  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, lex_layout(h, h->n_levels - 1), dst, src, nullptr, 0, s));
   TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, 8, s));
 }
 
@@ -390,13 +431,15 @@ void cg_iteration_body(tps_handle *h, int prec, bool symmetric, double *x, cudaS
   CGScalars *sc = h->scalars.as<CGScalars>();
   double *part = h->partial.as<double>();
   const int zk = p == 1 ? 1 : 0;
+  const PadMap pm = fine_padmap(h, p);
+  const VecLayout lex = lex_layout(h, L);
   vcycle_rec(h, L, p, symmetric, s);
-  TPS_CUDA(launch_cg_beta(V.su[L]->p, zk, h->q.as<double>(), h->r.as<double>(), N, part, sc, s));
-  TPS_CUDA(launch_cg_update_p(h->p.as<double>(), V.su[L]->p, zk, N, sc, s));
-  TPS_CUDA(h->kt->laplace[h->dim - 2][0](h->fine(), h->q.p, h->p.p, nullptr, 0, s));
+  TPS_CUDA(launch_cg_beta(V.su[L]->p, zk, pm, h->q.as<double>(), h->r.as<double>(), N, part, sc, s));
+  TPS_CUDA(launch_cg_update_p(h->p.as<double>(), V.su[L]->p, zk, pm, N, sc, s));
+  TPS_CUDA(h->kt->laplace[h->dim - 2][0](h->fine(), lex, h->q.p, h->p.p, nullptr, 0, s));
   TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
   TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
-                               V.d[L]->p, input_kind(prec), N, part, sc, s));
+                               V.d[L]->p, input_kind(prec), pm, N, part, sc, s));
   TPS_CUDA(launch_cg_finalize_rr(part, sc, s));
 }
 
@@ -420,13 +463,15 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
   double *part = h->partial.as<double>();
   const int zk = p == 1 ? 1 : 0;
   const bool sym = o.symmetric != 0;
+  const PadMap pm = fine_padmap(h, p);
+  const VecLayout lex = lex_layout(h, L);
   TPS_CUDA(cudaEventRecord(h->ev0, s));
   // Dirichlet rows: x_b = b_b, so r_b = 0 and the iteration lives on the interior
   TPS_CUDA(launch_copy_boundary(x, b, h->dim, g.N1, 8, s));
   TPS_CUDA(cudaMemsetAsync(h->r.p, 0, sizeof(double) * N, s));
   TPS_CUDA(cudaMemsetAsync(h->q.p, 0, sizeof(double) * N, s));
-  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, h->r.p, x, b, 1, s));
-  TPS_CUDA(launch_cg_init(h->r.as<double>(), b, V.d[L]->p, input_kind(o.precision), N, part, s));
+  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, lex, h->r.p, x, b, 1, s));
+  TPS_CUDA(launch_cg_init(h->r.as<double>(), b, V.d[L]->p, input_kind(o.precision), pm, N, part, s));
   TPS_CUDA(launch_cg_finalize_init(part, sc, s));
   CGScalars hs{};
   read_scalars(h, hs, s);
@@ -441,12 +486,13 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
   if (!converged && status == TPS_OK) {
     // first direction: z = V(r), p = z, rz; then q, alpha, x/r update
     vcycle_rec(h, L, p, sym, s);
-    TPS_CUDA(launch_cg_first_direction(h->p.as<double>(), V.su[L]->p, zk, h->r.as<double>(), N, part, s));
+    TPS_CUDA(launch_cg_first_direction(h->p.as<double>(), V.su[L]->p, zk, pm, h->r.as<double>(), N,
+                                       part, s));
     TPS_CUDA(launch_cg_finalize_rz(part, sc, s));
-    TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, h->q.p, h->p.p, nullptr, 0, s));
+    TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, lex, h->q.p, h->p.p, nullptr, 0, s));
     TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
     TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
-                                 V.d[L]->p, input_kind(o.precision), N, part, sc, s));
+                                 V.d[L]->p, input_kind(o.precision), pm, N, part, sc, s));
     TPS_CUDA(launch_cg_finalize_rr(part, sc, s));
     it = 1;
     const int key = (o.precision << 1) | (sym ? 1 : 0);
@@ -532,9 +578,10 @@ void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, c
   VcycleVectors &V = vcycle_vectors(h, p);
   const int L = h->n_levels - 1;
   const int64_t N = h->fine().N;
-  TPS_CUDA(launch_to_vcycle(V.d[L]->p, input_kind(precision), src, N, s));
+  const PadMap pm = fine_padmap(h, p);
+  TPS_CUDA(launch_to_vcycle(V.d[L]->p, input_kind(precision), pm, src, N, s));
   vcycle_rec(h, L, p, symmetric, s);
-  TPS_CUDA(launch_from_vcycle(dst, V.su[L]->p, p == 1 ? 1 : 0, N, s));
+  TPS_CUDA(launch_from_vcycle(dst, V.su[L]->p, p == 1 ? 1 : 0, pm, N, s));
 }
 
 // deal.II SolverGMRES semantics (left preconditioning, MGS, Givens) as used by
@@ -749,7 +796,7 @@ int tps_laplace_vmult(tps_handle *h, int level, int dtype, void *dst, const void
     if (dst == src) throw ApiError(TPS_ERR_INVALID, "dst and src must not alias");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const LevelGeomH &g = h->lv[level];
-    TPS_CUDA(h->kt->laplace[h->dim - 2][p](g, dst, src, nullptr, 0, s));
+    TPS_CUDA(h->kt->laplace[h->dim - 2][p](g, lex_layout(h, level), dst, src, nullptr, 0, s));
     TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, p == 0 ? 8 : 4, s));
   });
 }
@@ -765,7 +812,7 @@ int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const LevelGeomH &g = h->lv[level];
     if (zero_init) TPS_CUDA(cudaMemsetAsync(x, 0, (p == 0 ? 8 : 4) * g.N, s));
-    smoother_sweep(h, level, p, x, b, reverse != 0, s);
+    smoother_sweep(h, level, p, lex_layout(h, level), x, b, reverse != 0, zero_init != 0, nullptr, s);
   });
 }
 
@@ -778,7 +825,8 @@ int tps_prolongate_add(tps_handle *h, int to_level, int dtype, void *fine, const
     if (!fine || !coarse) throw ApiError(TPS_ERR_INVALID, "null vector");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     VcycleVectors &V = vcycle_vectors(h, p);
-    TPS_CUDA(h->kt->prolong[h->dim - 2][p](h->lv[to_level - 1], fine, coarse,
+    TPS_CUDA(h->kt->prolong[h->dim - 2][p](h->lv[to_level - 1], lex_layout(h, to_level - 1),
+                                           lex_layout(h, to_level), fine, coarse,
                                            V.tmp[to_level]->p, s));
   });
 }
@@ -792,7 +840,8 @@ int tps_restrict_add(tps_handle *h, int from_level, int dtype, void *coarse, con
     if (!fine || !coarse) throw ApiError(TPS_ERR_INVALID, "null vector");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     VcycleVectors &V = vcycle_vectors(h, p);
-    TPS_CUDA(h->kt->restrict_[h->dim - 2][p](h->lv[from_level - 1], coarse, fine,
+    TPS_CUDA(h->kt->restrict_[h->dim - 2][p](h->lv[from_level - 1], lex_layout(h, from_level - 1),
+                                             lex_layout(h, from_level), coarse, fine,
                                              V.tmp[from_level]->p, 1, s));
   });
 }
@@ -827,6 +876,28 @@ int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double
   if (status == TPS_ERR_BREAKDOWN) h->err = "Krylov breakdown (p^T A p <= 0)";
   if (status == TPS_ERR_NONFINITE) h->err = "non-finite residual";
   return status;
+}
+
+int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *ms_per_sweep,
+                      void *stream)
+{
+  return guarded(h, [&] {
+    check_level(h, level);
+    const int p = dt_index(dtype);
+    if (sweeps < 1 || !ms_per_sweep) throw ApiError(TPS_ERR_INVALID, "sweeps >= 1 and an output are required");
+    ensure_krylov(h);
+    VcycleVectors &V = vcycle_vectors(h, p);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    TPS_CUDA(cudaEventRecord(h->ev0, s));
+    for (int i = 0; i < sweeps; ++i)
+      smoother_sweep(h, level, p, V.layout[level], V.su[level]->p, V.d[level]->p, false, false,
+                     &V.maps[level], s);
+    TPS_CUDA(cudaEventRecord(h->ev1, s));
+    TPS_CUDA(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    *ms_per_sweep = ms / sweeps;
+  });
 }
 
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host, double *x_host,

@@ -29,7 +29,17 @@ struct DegreeTables {
   T evec[Dims<K>::M * Dims<K>::M];      // interior eigenvectors (columns)
   T eval[Dims<K>::M];                   // interior eigenvalues (reference scaling)
   T prol[Dims<K>::N1 * Dims<K>::NP];    // 1D prolongation (child node x coarse basis)
+  // even/odd folded interior rows of the centro-symmetric patch matrices A:
+  // row r < k-1 (A row r+1, paired with row 2k-1-r):
+  //   fe[r][j] = (A[r+1][j] + A[r+1][2k-j])/2 (j < k), fe[r][k] = A[r+1][k]
+  //   fo[r][j] = (A[r+1][j] - A[r+1][2k-j])/2 (j < k)
+  // row k-1 is the centre row A[k][.] (fe only)
+  T pmass_fe[K * (K + 1)];
+  T plap_fe[K * (K + 1)];
+  T pmass_fo[K > 1 ? (K - 1) * K : 1];
+  T plap_fo[K > 1 ? (K - 1) * K : 1];
 };
+
 
 template <int K, typename T>
 __constant__ DegreeTables<K, T> c_tables;

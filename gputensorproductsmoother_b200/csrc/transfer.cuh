@@ -67,12 +67,13 @@ __device__ __forceinline__ void restr_cell(const T (&v)[4 * K + 1], T (&out)[K])
 
 // ---------------------------------------------------------------------------
 // xy pass, prolongation: coarse plane (N1c x N1c) -> fine plane (N1f x N1f).
-// in/out advance by the plane strides per blockIdx.z (plane index offset by
-// plane0).  Coarse boundary entries are read as zero when mask_in != 0.
+// Rows are in_sy / out_sy apart; in/out advance by the plane strides per
+// blockIdx.z (plane index offset by plane0).  Coarse boundary entries are read as zero when mask_in != 0.
 template <int K, typename T, XYOut OUT>
 __global__ void __launch_bounds__(XYTile<K>::NT)
     prolong_xy_kernel(T *__restrict__ out, const T *__restrict__ in, int N1c, int N1f,
-                      int64_t in_plane, int64_t out_plane, int plane0, int mask_in)
+                      int64_t in_sy, int64_t in_plane, int64_t out_sy, int64_t out_plane,
+                      int plane0, int mask_in)
 {
   constexpr int C = XYTile<K>::C, NT = XYTile<K>::NT;
   constexpr int WI = C * K + 1;  // coarse inputs per direction
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
     T v = T(0);
     if (gx < N1c && gy < N1c) {
       const bool bnd = gx == 0 || gx == N1c - 1 || gy == 0 || gy == N1c - 1;
-      if (!(mask_in && bnd)) v = inp[gx + static_cast<int64_t>(gy) * N1c];
+      if (!(mask_in && bnd)) v = inp[gx + gy * in_sy];
     }
     sIn[e] = v;
   }
@@ -116,7 +117,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
     for (int f = 0; f < 2 * K; ++f) {
       const int gy = 2 * K * (cy0 + c) + f;
       if (gy >= N1f) continue;
-      const int64_t gi = gx + static_cast<int64_t>(gy) * N1f;
+      const int64_t gi = gx + gy * out_sy;
       const bool interior = gx > 0 && gx < N1f - 1 && gy > 0 && gy < N1f - 1;
       if constexpr (OUT == XYOut::AddInterior) {
         if (interior) outp[gi] += o[f];
@@ -135,7 +136,8 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
 template <int K, typename T, XYOut OUT>
 __global__ void __launch_bounds__(XYTile<K>::NT)
     restrict_xy_kernel(T *__restrict__ out, const T *__restrict__ in, int N1c, int N1f,
-                       int64_t in_plane, int64_t out_plane, int plane0, int n_planes_total)
+                       int64_t in_sy, int64_t in_plane, int64_t out_sy, int64_t out_plane,
+                       int plane0, int n_planes_total)
 {
   constexpr int C = XYTile<K>::C, NT = XYTile<K>::NT;
   constexpr int WI = 2 * K * (C + 1) + 1;  // fine inputs per direction
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
     const int gx = fx0 + lx, gy = fy0 + ly;
     T v = T(0);
     if (!zero_plane && gx > 0 && gx < N1f - 1 && gy > 0 && gy < N1f - 1)
-      v = __ldg(&inp[gx + static_cast<int64_t>(gy) * N1f]);
+      v = __ldg(&inp[gx + gy * in_sy]);
     sIn[e] = v;
   }
   __syncthreads();
@@ -180,7 +182,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
     for (int b = 0; b < K; ++b) {
       const int gy = K * (cy0 + c) + b;
       if (gy >= N1c) continue;
-      const int64_t gi = gx + static_cast<int64_t>(gy) * N1c;
+      const int64_t gi = gx + gy * out_sy;
       const bool interior = gx > 0 && gx < N1c - 1 && gy > 0 && gy < N1c - 1;
       if constexpr (OUT == XYOut::AddInterior) {
         if (interior) outp[gi] += o[b];
@@ -198,7 +200,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
 // P entries), P = N1c^2.  Input entries on the coarse boundary read as zero.
 template <int K, typename T>
 __global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coarse, int N1c,
-                                 int N1f, int n_cells_c)
+                                 int N1f, int n_cells_c, int64_t c_sy, int64_t c_sz)
 {
   const int64_t P = static_cast<int64_t>(N1c) * N1c;
   const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
@@ -210,7 +212,7 @@ __global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coar
 #pragma unroll
   for (int b = 0; b <= K; ++b) {
     const int gz = c * K + b;
-    v[b] = (bxy || gz == 0 || gz == N1c - 1) ? T(0) : __ldg(&coarse[gz * P + idx]);
+    v[b] = (bxy || gz == 0 || gz == N1c - 1) ? T(0) : __ldg(&coarse[gz * c_sz + gy * c_sy + gx]);
   }
   prol_cell<K, T>(v, o);
 #pragma unroll
@@ -221,7 +223,7 @@ __global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coar
 // z pass, restriction: tmp (N1f planes of P = N1c^2 entries) -> coarse.
 template <int K, typename T, bool ADD>
 __global__ void restrict_z_kernel(T *__restrict__ coarse, const T *__restrict__ tmp, int N1c,
-                                  int N1f)
+                                  int N1f, int64_t c_sy, int64_t c_sz)
 {
   const int64_t P = static_cast<int64_t>(N1c) * N1c;
   const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
@@ -240,10 +242,11 @@ __global__ void restrict_z_kernel(T *__restrict__ coarse, const T *__restrict__ 
   for (int b = 0; b < K; ++b) {
     const int gz = c * K + b;
     if (gz == 0 || gz >= N1c - 1) continue;
+    T &dst = coarse[gz * c_sz + gy * c_sy + gx];
     if constexpr (ADD)
-      coarse[gz * P + idx] += o[b];
+      dst += o[b];
     else
-      coarse[gz * P + idx] = o[b];
+      dst = o[b];
   }
 }
 

@@ -126,6 +126,13 @@ void tps_solve_opts_default(tps_solve_opts *opts);
 int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double *x,
               tps_report *report, void *stream);
 
+/* Measurement hook: runs `sweeps` coloured sweeps of the level's smoother on
+ * the V-cycle's own work vectors (the padded, TMA-staged path that the V-cycle
+ * uses) on `stream` and returns the mean device time of one sweep (CUDA events
+ * on that stream).  Used by the benchmark to time the dominant kernel. */
+int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *ms_per_sweep,
+                      void *stream);
+
 /* Same solve with HOST buffers; the host<->device copies are part of the call. */
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
                    double *x_host, tps_report *report);
