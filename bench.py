@@ -40,10 +40,37 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson3d_q4_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "smoother"],
-                    help="smoother: only time the finest-level FP32 smoother sweeps "
-                         "(a small command for kernel profiling)")
+    ap.add_argument("--mode", default="solve", choices=["solve", "smoother", "operator"],
+                    help="smoother / operator: only time the finest-level FP32 smoother "
+                         "sweeps / FP64 operator applications (small commands for kernel "
+                         "profiling)")
     return ap.parse_args()
+
+
+def run_operator_only(args):
+    """Times --steps finest-level FP64 operator applications (the CG's q = A p)
+    after --warmup applications and prints one JSON line."""
+    import torch
+    import gputensorproductsmoother_b200 as tps
+    from gputensorproductsmoother_b200 import problems
+    dim, k, n, _ = problems.WORKLOADS[args.workload]
+    P = tps.PoissonProblem(dim, k, n)
+    A = tps.LaplaceOperator(P)
+    src = problems.make_rhs(args.workload)
+    dst = torch.empty_like(src)
+    for _ in range(args.warmup):
+        A.vmult(dst, src)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(max(args.steps, 1)):
+        A.vmult(dst, src)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / max(args.steps, 1)
+    print(json.dumps({"mode": "operator", "workload": args.workload, "ms_per_apply": ms,
+                      "algorithmic_GBps": 2 * 8 * P.n_dofs() / (ms * 1e-3) / 1e9}), flush=True)
+    P.close()
 
 
 def run_smoother_only(args):
@@ -232,6 +259,9 @@ def main():
         return
     if args.mode == "smoother":
         run_smoother_only(args)
+        return
+    if args.mode == "operator":
+        run_operator_only(args)
         return
     import numpy as np
     import torch

@@ -37,8 +37,12 @@ struct OpTile {
   static constexpr int WZ = DIM == 3 ? (CZ + 1) * K + 1 : 1;
   static constexpr int OX = CX * K, OY = CY * K, OZ = DIM == 3 ? CZ * K : 1;  // outputs
   static constexpr int IN = WX * WY * WZ;
-  static constexpr int TS = WZ * WY * OX;          // one x-contracted array
-  static constexpr int US = DIM == 3 ? WZ * OY * OX : 0;  // one xy-contracted array
+  // contracted arrays store x permuted, x' = a*CX + c for node c*K+a of the
+  // tile, in rows of RX >= OX entries: consecutive threads (consecutive c)
+  // then touch consecutive shared-memory words
+  static constexpr int RX = OX + CX;
+  static constexpr int TS = WZ * WY * RX;          // one x-contracted array
+  static constexpr int US = DIM == 3 ? WZ * OY * RX : 0;  // one xy-contracted array
   // U1/U2 reuse the input region once the x stage is done
   static constexpr int REGION0 = IN > 2 * US ? IN : 2 * US;
   static constexpr int SMEM_ELEMS = REGION0 + 2 * TS;
@@ -65,13 +69,13 @@ __device__ __forceinline__ void band_apply(const T *mat /* (k+1)^2 cell matrix *
 }
 
 template <int DIM, int K, typename T, OpMode MODE>
-__global__ void __launch_bounds__(OpTile<DIM, K>::NT)
+__global__ void __launch_bounds__(OpTile<DIM, K>::NT, 2)
     laplace_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs,
                    int N1g, int64_t sy, int64_t sz, T scale)
 {
   using Tl = OpTile<DIM, K>;
   constexpr int NT = Tl::NT, WX = Tl::WX, WY = Tl::WY, WZ = Tl::WZ;
-  constexpr int OX = Tl::OX, OY = Tl::OY, OZ = Tl::OZ;
+  constexpr int OX = Tl::OX, OY = Tl::OY, OZ = Tl::OZ, RX = Tl::RX;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T *sIn = reinterpret_cast<T *>(smem_raw);
@@ -115,11 +119,11 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT)
     for (int j = 0; j <= 2 * K; ++j) v[j] = s[j];
     band_apply<K, T>(tb.cmass, v, o1);
     band_apply<K, T>(tb.clap, v, o2);
-    T *d1 = T1 + line * OX + c * K, *d2 = T2 + line * OX + c * K;
+    T *d1 = T1 + line * RX + c, *d2 = T2 + line * RX + c;
 #pragma unroll
     for (int a = 0; a < K; ++a) {
-      d1[a] = o1[a];
-      d2[a] = o2[a];
+      d1[a * Tl::CX] = o1[a];
+      d2[a * Tl::CX] = o2[a];
     }
   }
   __syncthreads();
@@ -127,16 +131,16 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT)
   if constexpr (DIM == 2) {
     // stage y: out = s (L_y T1 + M_y T2)
     for (int t = threadIdx.x; t < OX * Tl::CY; t += NT) {
-      const int xx = t % OX, c = t / OX;
+      const int xp = t % OX, c = t / OX;  // xp: permuted x
       T v1[2 * K + 1], v2[2 * K + 1], o1[K], o2[K];
 #pragma unroll
       for (int j = 0; j <= 2 * K; ++j) {
-        v1[j] = T1[(c * K + j) * OX + xx];
-        v2[j] = T2[(c * K + j) * OX + xx];
+        v1[j] = T1[(c * K + j) * RX + xp];
+        v2[j] = T2[(c * K + j) * RX + xp];
       }
       band_apply<K, T>(tb.clap, v1, o1);
       band_apply<K, T>(tb.cmass, v2, o2);
-      const int gx = gx0 + xx;
+      const int gx = gx0 + (xp % Tl::CX) * K + xp / Tl::CX;
       if (gx < 1 || gx > N1g - 2) continue;
 #pragma unroll
       for (int a = 0; a < K; ++a) {
@@ -153,37 +157,37 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT)
   } else {
     // stage y: U1 = M_y T1, U2 = L_y T1 + M_y T2
     for (int t = threadIdx.x; t < WZ * OX * Tl::CY; t += NT) {
-      const int xx = t % OX, r = t / OX;
+      const int xp = t % OX, r = t / OX;
       const int c = r % Tl::CY, z = r / Tl::CY;
       T v1[2 * K + 1], v2[2 * K + 1], o1[K], o2[K], o3[K];
 #pragma unroll
       for (int j = 0; j <= 2 * K; ++j) {
-        v1[j] = T1[(z * WY + c * K + j) * OX + xx];
-        v2[j] = T2[(z * WY + c * K + j) * OX + xx];
+        v1[j] = T1[(z * WY + c * K + j) * RX + xp];
+        v2[j] = T2[(z * WY + c * K + j) * RX + xp];
       }
       band_apply<K, T>(tb.cmass, v1, o1);
       band_apply<K, T>(tb.clap, v1, o2);
       band_apply<K, T>(tb.cmass, v2, o3);
 #pragma unroll
       for (int a = 0; a < K; ++a) {
-        U1[(z * OY + c * K + a) * OX + xx] = o1[a];
-        U2[(z * OY + c * K + a) * OX + xx] = o2[a] + o3[a];
+        U1[(z * OY + c * K + a) * RX + xp] = o1[a];
+        U2[(z * OY + c * K + a) * RX + xp] = o2[a] + o3[a];
       }
     }
     __syncthreads();
     // stage z: out = s (L_z U1 + M_z U2)
     for (int t = threadIdx.x; t < OY * OX * Tl::CZ; t += NT) {
       const int yx = t % (OY * OX), c = t / (OY * OX);
-      const int xx = yx % OX, yy = yx / OX;
+      const int xp = yx % OX, yy = yx / OX;
       T v1[2 * K + 1], v2[2 * K + 1], o1[K], o2[K];
 #pragma unroll
       for (int j = 0; j <= 2 * K; ++j) {
-        v1[j] = U1[(c * K + j) * OY * OX + yx];
-        v2[j] = U2[(c * K + j) * OY * OX + yx];
+        v1[j] = U1[((c * K + j) * OY + yy) * RX + xp];
+        v2[j] = U2[((c * K + j) * OY + yy) * RX + xp];
       }
       band_apply<K, T>(tb.clap, v1, o1);
       band_apply<K, T>(tb.cmass, v2, o2);
-      const int gx = gx0 + xx, gy = gy0 + yy;
+      const int gx = gx0 + (xp % Tl::CX) * K + xp / Tl::CX, gy = gy0 + yy;
       if (gx < 1 || gx > N1g - 2 || gy < 1 || gy > N1g - 2) continue;
 #pragma unroll
       for (int a = 0; a < K; ++a) {

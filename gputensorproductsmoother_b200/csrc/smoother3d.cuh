@@ -44,10 +44,12 @@ struct Sm3 {
   static constexpr int XBOX = N1 * N1 * W;
   static constexpr int BBOX = M * M * W;
   static constexpr int ALIGN = 128 / static_cast<int>(sizeof(T));  // TMA destinations: 128 B
-  static constexpr int BOFF = (XBOX + ALIGN - 1) / ALIGN * ALIGN;    // b slab inside a stage
+  static constexpr int VSZ = M * M * N1;   // zy-contracted [zi][yi][x]
+  // the x box region also holds V1/V2 once the z stage is done
+  static constexpr int XREG = XBOX > 2 * VSZ ? XBOX : 2 * VSZ;
+  static constexpr int BOFF = (XREG + ALIGN - 1) / ALIGN * ALIGN;    // b slab inside a stage
   static constexpr int STAGE = (BOFF + BBOX + ALIGN - 1) / ALIGN * ALIGN;  // per patch
   static constexpr int ZSZ = M * N1 * N1;  // z-contracted  [zi][y][x]
-  static constexpr int VSZ = M * M * N1;   // zy-contracted [zi][yi][x]
   static constexpr int QSZ = M * M * M;
   static constexpr int RING = N1 * N1 - M * M;  // boundary lines of a z-face
   // patches per batch: enough lines per stage, two CTAs per SM within 227 KB
@@ -55,12 +57,14 @@ struct Sm3 {
                                             : (K == 1 ? 16 : K == 2 ? 8 : K == 3 ? 4 : K == 4 ? 2 : 1);
   static constexpr int NT_RAW = (PPB * M * M + 31) / 32 * 32;
   static constexpr int NT = NT_RAW < 128 ? 128 : NT_RAW;
-  // shared memory layout (elements of T): 2 stages | Z1 | Z2 | V1 | V2 ; Q1/Q2 alias Z1/Z2
+  // shared memory layout (elements of T): 2 stages | Z1 | Z2 | 1/(lambda sums) ;
+  // V1/V2 of a patch live in the x box of its own stage (dead after the z stage),
+  // Q1/Q2 alias Z1/Z2
+  static_assert(2 * VSZ <= BOFF, "V arrays must fit in the staged x box");
   static constexpr int OFF_Z1 = 2 * PPB * STAGE;
   static constexpr int OFF_Z2 = OFF_Z1 + PPB * ZSZ;
-  static constexpr int OFF_V1 = OFF_Z2 + PPB * ZSZ;
-  static constexpr int OFF_V2 = OFF_V1 + PPB * VSZ;
-  static constexpr int ELEMS = (OFF_V2 + PPB * VSZ + ALIGN - 1) / ALIGN * ALIGN;
+  static constexpr int OFF_RL = OFF_Z2 + PPB * ZSZ;
+  static constexpr int ELEMS = (OFF_RL + QSZ + ALIGN - 1) / ALIGN * ALIGN;
   // + two mbarriers and the wait-status flag
   static constexpr size_t BYTES = sizeof(T) * ELEMS + 2 * sizeof(uint64_t) + 16;
 };
@@ -134,14 +138,18 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
     fz = (a.cz + 2 * jz) * K;
   };
 
+  // fd_scale / (lambda_x + lambda_y + lambda_z) for every mode triple
+  T *RL = sm + S::OFF_RL;
+  for (int e = tid; e < S::QSZ; e += NT)
+    RL[e] = fd_scale / (tb.eval[e % M] + tb.eval[(e / M) % M] + tb.eval[e / (M * M)]);
   if constexpr (USE_TMA) {
     if (tid == 0) {
       mbar_init(&bars[0], 1);
       mbar_init(&bars[1], 1);
       fence_mbar_init();
     }
-    __syncthreads();
   }
+  __syncthreads();
 
   // issue the TMA loads of batch `bt` into stage `st` (one thread)
   auto issue = [&](int bt, int st) {
@@ -247,7 +255,10 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
       return fx & (AL - 1);
     };
 
-    T *Z1 = sm + S::OFF_Z1, *Z2 = sm + S::OFF_Z2, *V1 = sm + S::OFF_V1, *V2 = sm + S::OFF_V2;
+    T *Z1 = sm + S::OFF_Z1, *Z2 = sm + S::OFF_Z2;
+    // V1/V2 of patch lp at stage + lp*STAGE (+VSZ): the x box is dead after the z stage
+    T *V1 = stage, *V2 = stage + S::VSZ;
+    constexpr int VST = S::STAGE;  // V1/V2 patch stride
     T *Q1 = Z1, *Q2 = Z2;  // the fast-diagonalization stages reuse the Z arrays
 
     if (!a.zero_x) {
@@ -318,7 +329,7 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
         fold_rows<K, T>(tb.pmass_fe, tb.pmass_fo, e2, o2, ra);
         fold_rows<K, T>(tb.plap_fe, tb.plap_fo, e1, o1, rb);
         fold_rows<K, T>(tb.pmass_fe, tb.pmass_fo, e1, o1, rc);
-        T *d1 = V1 + lp * S::VSZ + zi * M * N1 + xx, *d2 = V2 + lp * S::VSZ + zi * M * N1 + xx;
+        T *d1 = V1 + lp * VST + zi * M * N1 + xx, *d2 = V2 + lp * VST + zi * M * N1 + xx;
 #pragma unroll
         for (int i = 0; i < M; ++i) {
           d1[i * N1] = ra[i] + rb[i];
@@ -333,7 +344,7 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
       T res[M];
       const T *bb = stage + lp * S::STAGE + S::BOFF + r * W + xoff(lp) + 1;
       if (!a.zero_x) {
-        const T *s1 = V1 + lp * S::VSZ + r * N1, *s2 = V2 + lp * S::VSZ + r * N1;
+        const T *s1 = V1 + lp * VST + r * N1, *s2 = V2 + lp * VST + r * N1;
         T v[N1], e1[K + 1], o1[K > 1 ? K : 1], e2[K + 1], o2[K > 1 ? K : 1];
 #pragma unroll
         for (int j = 0; j < N1; ++j) v[j] = s1[j];
@@ -380,9 +391,8 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j * M * M];
       apply_evec<K, T, true>(v, q);
-      const T lxy = tb.eval[qx] + tb.eval[qy];
 #pragma unroll
-      for (int j = 0; j < M; ++j) q[j] = q[j] * fd_scale / (lxy + tb.eval[j]);
+      for (int j = 0; j < M; ++j) q[j] *= RL[j * M * M + r];
       apply_evec<K, T, false>(q, v);
       T *d = Q1 + lp * S::QSZ + r;
 #pragma unroll
