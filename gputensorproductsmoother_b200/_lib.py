@@ -70,6 +70,8 @@ SIGNATURES = [
                                       ctypes.POINTER(TpsReport)]),
     ("tps_time_smoother", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_double), _VP]),
+    ("tps_restrict_add_noalloc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, _VP, _VP, _VP]),
 ]
 
 

@@ -54,8 +54,14 @@ cudaError_t launch_coarse_dense(const void *inv, const int *idx, int n_int, void
 using namespace tps;
 
 namespace {
-
 thread_local std::string g_create_error;
+}  // namespace
+
+namespace tps {
+void set_handle_free_error(const std::string &msg) { g_create_error = msg; }
+}  // namespace tps
+
+namespace {
 
 struct ApiError : std::runtime_error {
   int code;

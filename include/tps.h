@@ -54,8 +54,9 @@ typedef struct {
  * transfer data and the device work vectors. */
 int tps_create(const tps_problem *problem, tps_handle **out);
 int tps_destroy(tps_handle *h);
-/* Message of the last failing call on `h` (or of the last failing tps_create when
- * h is NULL).  Valid until the next call on the same handle/thread. */
+/* Message of the last failing call on `h` (or, when h is NULL, of the last
+ * failing tps_create or tps_restrict_add_noalloc of this thread).  Valid until
+ * the next call on the same handle/thread. */
 const char *tps_last_error(const tps_handle *h);
 /* Number of DoFs (boundary included) and cells per direction of `level`
  * (0 = coarsest, n_levels-1 = finest). */
@@ -136,6 +137,19 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
 /* Same solve with HOST buffers; the host<->device copies are part of the call. */
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
                    double *x_host, tps_report *report);
+
+/* coarse += R fine, like tps_restrict_add, without a handle and without any
+ * device allocation, for callers that must not allocate device memory (their
+ * framework owns it all, e.g. a caching allocator or a pre-reserved arena).
+ * No counterpart in the reference.  The 3D intermediate lives in a fixed
+ * 16 MiB array inside the library (held on every GPU that loads it until the
+ * process exits); 8 * (2n_c k+1) * (n_c k+1)^2 bytes (FP64; half for FP32)
+ * must fit, larger sizes return TPS_ERR_INVALID.  n_coarse_cells: cells per
+ * direction of the coarse level; vectors lexicographic.  The first call on a
+ * device does the set-up (symbol address, 1D tables): make it before any
+ * stream capture.  Calls share the array: calls that overlap on the GPU race. */
+int tps_restrict_add_noalloc(int dim, int degree, int n_coarse_cells, int dtype, void *coarse,
+                             const void *fine, void *stream);
 
 #ifdef __cplusplus
 }
