@@ -46,6 +46,15 @@ cudaError_t upload_one(const DegreeData &D)
   };
   fold(D.pmass, t.pmass_fe, t.pmass_fo);
   fold(D.plap, t.plap_fe, t.plap_fo);
+  for (int r = 0; r < K - 1; ++r)
+    for (int j = 0; j < K; ++j) {
+      t.pmass_fp[r * K + j] = Pair<T>::make(t.pmass_fe[r * (K + 1) + j], t.pmass_fo[r * K + j]);
+      t.plap_fp[r * K + j] = Pair<T>::make(t.plap_fe[r * (K + 1) + j], t.plap_fo[r * K + j]);
+    }
+  const int C = K - 1;
+  for (int r = 0; r < C; ++r)
+    for (int q = 0; q < C; ++q)
+      t.evec_p[r * C + q] = Pair<T>::make(t.evec[r * M + q], t.evec[r * M + C + 1 + q]);
   return cudaMemcpyToSymbol(c_tables<K, T>, &t, sizeof(t));
 }
 

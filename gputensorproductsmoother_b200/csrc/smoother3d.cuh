@@ -9,7 +9,7 @@
 //     omega (x_I + A_II^{-1}(b_I - A_II x_I - A_IB x_B)) = omega A_II^{-1}(b_I - A_IB x_B),
 // so the old interior values are never needed (the idea of the reference's
 // FUSED_BD variant, include/loop_kernel.cuh:667-783): the box residual is
-// evaluated with the interior of x set to zero, which turns the 49 interior
+// evaluated with the interior of x set to zero, which turns the interior
 // z-lines of the first contraction into two-term lines.
 //
 // B200 design:
@@ -20,9 +20,14 @@
 //    tracked by one mbarrier per stage with a bounded wait;
 //  * contractions: z (M, L) -> y (3 products) -> x (2 products) + S^T_x ->
 //    S^T_y -> S^T_z, scale, S_z -> S_x -> S_y + store.  Every contraction keeps
-//    one 1D line per thread in registers, applies the centro-symmetric 1D
-//    matrices in even/odd folded form (constant-bank operands, about half the
-//    multiply-adds), and the last one stores x_I straight to global memory;
+//    one 1D line per thread in registers and applies the centro-symmetric 1D
+//    matrices in even/odd folded form; the even and odd partial sums of an
+//    output pair travel together through one packed FP32x2 FMA (__ffma2_rn),
+//    so a folded contraction costs about a quarter of the dense FMA
+//    instructions; coefficients are constant-bank data;
+//  * per-batch patch offsets are computed once into shared memory; the
+//    thread count matches the widest stage (the y stage), and the cheap
+//    interior z-lines are processed two per thread;
 //  * a second loader variant (plain coalesced loads) serves vectors whose
 //    pitch is not 16-byte aligned (the C-ABI level operations on caller
 //    vectors); the compute path is shared.
@@ -31,7 +36,6 @@
 #include <cuda.h>
 
 #include "ptx.cuh"
-#include "smoother.cuh"
 #include "tps_common.cuh"
 
 namespace tps {
@@ -44,66 +48,107 @@ struct Sm3 {
   static constexpr int XBOX = N1 * N1 * W;
   static constexpr int BBOX = M * M * W;
   static constexpr int ALIGN = 128 / static_cast<int>(sizeof(T));  // TMA destinations: 128 B
+  static constexpr int ZSZ = M * N1 * N1;  // z-contracted  [zi][y][x]
   static constexpr int VSZ = M * M * N1;   // zy-contracted [zi][yi][x]
+  static constexpr int QSZ = M * M * M;
   // the x box region also holds V1/V2 once the z stage is done
   static constexpr int XREG = XBOX > 2 * VSZ ? XBOX : 2 * VSZ;
   static constexpr int BOFF = (XREG + ALIGN - 1) / ALIGN * ALIGN;    // b slab inside a stage
   static constexpr int STAGE = (BOFF + BBOX + ALIGN - 1) / ALIGN * ALIGN;  // per patch
-  static constexpr int ZSZ = M * N1 * N1;  // z-contracted  [zi][y][x]
-  static constexpr int QSZ = M * M * M;
   static constexpr int RING = N1 * N1 - M * M;  // boundary lines of a z-face
-  // patches per batch: enough lines per stage, two CTAs per SM within 227 KB
+  static constexpr int IPAIR = (M * M + 1) / 2;  // interior z-lines, two per task
+  // patches per batch: enough lines per stage, two to three CTAs per SM
   static constexpr int PPB = sizeof(T) == 4 ? (K == 1 ? 32 : K == 2 ? 16 : K == 3 ? 8 : K == 4 ? 4 : K <= 6 ? 2 : 1)
                                             : (K == 1 ? 16 : K == 2 ? 8 : K == 3 ? 4 : K == 4 ? 2 : 1);
-  static constexpr int NT_RAW = (PPB * M * M + 31) / 32 * 32;
+  // threads = widest stage (y lines), rounded to warps
+  static constexpr int NT_RAW = (PPB * M * N1 + 31) / 32 * 32;
   static constexpr int NT = NT_RAW < 128 ? 128 : NT_RAW;
-  // shared memory layout (elements of T): 2 stages | Z1 | Z2 | 1/(lambda sums) ;
-  // V1/V2 of a patch live in the x box of its own stage (dead after the z stage),
-  // Q1/Q2 alias Z1/Z2
-  static_assert(2 * VSZ <= BOFF, "V arrays must fit in the staged x box");
+  // shared memory layout (elements of T): 2 stages | Z1 | Z2 | 1/(lambda sums)
   static constexpr int OFF_Z1 = 2 * PPB * STAGE;
   static constexpr int OFF_Z2 = OFF_Z1 + PPB * ZSZ;
   static constexpr int OFF_RL = OFF_Z2 + PPB * ZSZ;
   static constexpr int ELEMS = (OFF_RL + QSZ + ALIGN - 1) / ALIGN * ALIGN;
-  // + two mbarriers and the wait-status flag
-  static constexpr size_t BYTES = sizeof(T) * ELEMS + 2 * sizeof(uint64_t) + 16;
+  // tail: two mbarriers, the wait flag, per-batch patch offsets
+  static constexpr size_t TAIL_BAR = sizeof(T) * ELEMS;
+  static constexpr size_t TAIL_BASE = TAIL_BAR + 32;
+  static constexpr size_t TAIL_XO = TAIL_BASE + 8 * PPB;
+  static constexpr size_t BYTES = TAIL_XO + 4 * PPB + 16;
 };
 
-// out[0..M) = interior rows 1..M of A v for a centro-symmetric (2k+1)^2 patch
-// matrix, from the folded input e[j] = v_j + v_{2k-j}, o[j] = v_j - v_{2k-j}
-// (j < k), e[k] = v_k.
+// v (2k+1 values) -> (e_j, o_j) pairs, j < k, and the centre e_k
 template <int K, typename T>
-__device__ __forceinline__ void fold_rows(const T *fe, const T *fo, const T (&e)[K + 1],
-                                          const T (&o)[K > 1 ? K : 1], T (&out)[2 * K - 1])
+__device__ __forceinline__ void fold_pairs(const T (&v)[2 * K + 1],
+                                           typename Pair<T>::type (&eo)[K > 1 ? K : 1], T &ec)
 {
+#pragma unroll
+  for (int j = 0; j < K; ++j) eo[j] = Pair<T>::make(v[j] + v[2 * K - j], v[j] - v[2 * K - j]);
+  ec = v[K];
+}
+
+// interior rows 1..2k-1 of A v for a centro-symmetric (2k+1)^2 patch matrix
+// from the folded input; the even/odd partial sums of the output pair
+// (r, 2k-2-r) share one packed accumulator
+template <int K, typename T>
+__device__ __forceinline__ void fold_rows2(const typename Pair<T>::type *fp, const T *fe,
+                                           const typename Pair<T>::type (&eo)[K > 1 ? K : 1],
+                                           const T ec, T (&out)[2 * K - 1])
+{
+  using P = Pair<T>;
   constexpr int M = 2 * K - 1;
 #pragma unroll
   for (int r = 0; r < K - 1; ++r) {
-    T se = fe[r * (K + 1) + K] * e[K];
-    T so = T(0);
+    typename P::type acc = P::make(fe[r * (K + 1) + K] * ec, T(0));
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-      se += fe[r * (K + 1) + j] * e[j];
-      so += fo[r * K + j] * o[j];
-    }
-    out[r] = se + so;
-    out[M - 1 - r] = se - so;
+    for (int j = 0; j < K; ++j) acc = P::fma(fp[r * K + j], eo[j], acc);
+    out[r] = acc.x + acc.y;
+    out[M - 1 - r] = acc.x - acc.y;
   }
-  T sc = fe[(K - 1) * (K + 1) + K] * e[K];
+  T sc = fe[(K - 1) * (K + 1) + K] * ec;
 #pragma unroll
-  for (int j = 0; j < K; ++j) sc += fe[(K - 1) * (K + 1) + j] * e[j];
+  for (int j = 0; j < K; ++j) sc += fe[(K - 1) * (K + 1) + j] * (eo[j].x);
   out[K - 1] = sc;
 }
 
-template <int K, typename T>
-__device__ __forceinline__ void fold_in(const T (&v)[2 * K + 1], T (&e)[K + 1], T (&o)[K > 1 ? K : 1])
+// Fast-diagonalization factor S (eigenvectors as columns; modes 0..k-1 even,
+// k..2k-2 odd) or its transpose applied to a line of 2k-1 values, with packed
+// (even, odd) pairs.
+template <int K, typename T, bool TRANSPOSE>
+__device__ __forceinline__ void apply_evec2(const T (&in)[2 * K - 1], T (&out)[2 * K - 1])
 {
+  using P = Pair<T>;
+  constexpr int M = 2 * K - 1, C = K - 1;
+  const DegreeTables<K, T> &tb = c_tables<K, T>;
+  if constexpr (TRANSPOSE) {
+    typename P::type eo[C > 0 ? C : 1];
 #pragma unroll
-  for (int j = 0; j < K; ++j) {
-    e[j] = v[j] + v[2 * K - j];
-    o[j] = v[j] - v[2 * K - j];
+    for (int j = 0; j < C; ++j) eo[j] = P::make(in[j] + in[M - 1 - j], in[j] - in[M - 1 - j]);
+    const T ec = in[C];
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      typename P::type acc = P::make(tb.evec[C * M + q] * ec, T(0));
+#pragma unroll
+      for (int j = 0; j < C; ++j) acc = P::fma(tb.evec_p[j * C + q], eo[j], acc);
+      out[q] = acc.x;          // even mode q
+      out[C + 1 + q] = acc.y;  // odd mode k+q
+    }
+    T sc = tb.evec[C * M + C] * ec;
+#pragma unroll
+    for (int j = 0; j < C; ++j) sc += tb.evec[j * M + C] * eo[j].x;
+    out[C] = sc;
+  } else {
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+      typename P::type acc = P::make(tb.evec[i * M + C] * in[C], T(0));
+#pragma unroll
+      for (int q = 0; q < C; ++q) acc = P::fma(tb.evec_p[i * C + q], P::make(in[q], in[C + 1 + q]), acc);
+      out[i] = acc.x + acc.y;
+      out[M - 1 - i] = acc.x - acc.y;
+    }
+    T sc = T(0);
+#pragma unroll
+    for (int q = 0; q <= C; ++q) sc += tb.evec[C * M + q] * in[q];
+    out[C] = sc;
   }
-  e[K] = v[K];
 }
 
 struct Sm3Args {
@@ -122,12 +167,15 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
                       int *__restrict__ err)
 {
   using S = Sm3<K, T>;
+  using P2 = typename Pair<T>::type;
   constexpr int N1 = S::N1, M = S::M, W = S::W, PPB = S::PPB, NT = S::NT, AL = S::A;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + sizeof(T) * S::ELEMS);
-  int &s_ok = *reinterpret_cast<int *>(bars + 2);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem_raw + S::TAIL_BAR);
+  int &s_ok = *reinterpret_cast<int *>(smem_raw + S::TAIL_BAR + 16);
+  int64_t *s_base = reinterpret_cast<int64_t *>(smem_raw + S::TAIL_BASE);
+  int *s_xo = reinterpret_cast<int *>(smem_raw + S::TAIL_XO);
   const int tid = threadIdx.x;
 
   // patch j of the colour -> first DoF coordinates of its box
@@ -154,9 +202,8 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
   // issue the TMA loads of batch `bt` into stage `st` (one thread)
   auto issue = [&](int bt, int st) {
     T *stage = sm + st * PPB * S::STAGE;
-    uint32_t bytes = 0;
     const int np = min(PPB, a.n_patches - bt * PPB);
-    bytes = np * sizeof(T) * (S::BBOX + (a.zero_x ? 0 : S::XBOX));
+    const uint32_t bytes = np * sizeof(T) * (S::BBOX + (a.zero_x ? 0 : S::XBOX));
     mbar_arrive_expect_tx(&bars[st], bytes);
     for (int lp = 0; lp < np; ++lp) {
       int fx, fy, fz;
@@ -177,6 +224,14 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
     const int st = USE_TMA ? (it & 1) : 0;
     T *stage = sm + st * PPB * S::STAGE;
     const int np = min(PPB, a.n_patches - bt * PPB);
+    // per-batch patch offsets (threads 1..PPB while thread 0 waits for TMA)
+    if (tid >= 1 && tid <= PPB) {
+      const int lp = tid - 1;
+      int fx, fy, fz;
+      patch_xyz(bt * PPB + (lp < np ? lp : 0), fx, fy, fz);
+      s_base[lp] = lp < np ? fx + 1 + (fy + 1) * a.sy + (fz + 1) * a.sz : int64_t(-1);
+      s_xo[lp] = USE_TMA ? (fx & (AL - 1)) : 0;
+    }
     if constexpr (USE_TMA) {
       if (tid == 0) {
         const int nb = bt + gridDim.x;
@@ -247,29 +302,19 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
       __syncthreads();
     }
 
-    // x offset of each patch's box inside its staged rows
-    auto xoff = [&](int lp) -> int {
-      if constexpr (!USE_TMA) return 0;
-      int fx, fy, fz;
-      patch_xyz(bt * PPB + (lp < np ? lp : 0), fx, fy, fz);
-      return fx & (AL - 1);
-    };
-
     T *Z1 = sm + S::OFF_Z1, *Z2 = sm + S::OFF_Z2;
     // V1/V2 of patch lp at stage + lp*STAGE (+VSZ): the x box is dead after the z stage
     T *V1 = stage, *V2 = stage + S::VSZ;
     constexpr int VST = S::STAGE;  // V1/V2 patch stride
-    T *Q1 = Z1, *Q2 = Z2;  // the fast-diagonalization stages reuse the Z arrays
+    T *Q1 = Z1, *Q2 = Z2;          // the fast-diagonalization stages reuse the Z arrays
 
     if (!a.zero_x) {
       // ---- z: Z1 = M_z x~, Z2 = L_z x~ (x~ = x with zero interior) ----------
-      // ring lines (y or x on the box boundary) first, then interior lines
-      for (int t = tid; t < PPB * N1 * N1; t += NT) {
-        int lp, y, xx;
-        const bool ring = t < PPB * S::RING;
-        if (ring) {
-          lp = t / S::RING;
-          const int r = t % S::RING;
+      // ring lines (y or x on the box boundary) first, then pairs of interior lines
+      for (int t = tid; t < PPB * (S::RING + S::IPAIR); t += NT) {
+        if (t < PPB * S::RING) {
+          const int lp = t / S::RING, r = t % S::RING;
+          int y, xx;
           if (r < N1) {
             y = 0;
             xx = r;
@@ -281,33 +326,36 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
             y = 1 + (q >> 1);
             xx = (q & 1) ? N1 - 1 : 0;
           }
-        } else {
-          const int u = t - PPB * S::RING;
-          lp = u / (M * M);
-          const int r = u % (M * M);
-          y = 1 + r / M;
-          xx = 1 + r % M;
-        }
-        const T *src = stage + lp * S::STAGE + y * W + xoff(lp) + xx;
-        T *d1 = Z1 + lp * S::ZSZ + y * N1 + xx, *d2 = Z2 + lp * S::ZSZ + y * N1 + xx;
-        if (ring) {
-          T v[N1], e[K + 1], o[K > 1 ? K : 1], r1[M], r2[M];
+          const T *src = stage + lp * S::STAGE + y * W + s_xo[lp] + xx;
+          T v[N1], ec, r1[M], r2[M];
+          P2 eo[K > 1 ? K : 1];
 #pragma unroll
           for (int z = 0; z < N1; ++z) v[z] = src[z * N1 * W];
-          fold_in<K, T>(v, e, o);
-          fold_rows<K, T>(tb.pmass_fe, tb.pmass_fo, e, o, r1);
-          fold_rows<K, T>(tb.plap_fe, tb.plap_fo, e, o, r2);
+          fold_pairs<K, T>(v, eo, ec);
+          fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo, ec, r1);
+          fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo, ec, r2);
+          T *d1 = Z1 + lp * S::ZSZ + y * N1 + xx, *d2 = Z2 + lp * S::ZSZ + y * N1 + xx;
 #pragma unroll
           for (int i = 0; i < M; ++i) {
             d1[i * N1 * N1] = r1[i];
             d2[i * N1 * N1] = r2[i];
           }
         } else {
-          const T v0 = src[0], vn = src[(N1 - 1) * N1 * W];
+          const int u = t - PPB * S::RING;
+          const int lp = u / S::IPAIR, r0 = 2 * (u % S::IPAIR);
 #pragma unroll
-          for (int i = 0; i < M; ++i) {
-            d1[i * N1 * N1] = tb.pmass[(i + 1) * N1] * v0 + tb.pmass[(i + 1) * N1 + N1 - 1] * vn;
-            d2[i * N1 * N1] = tb.plap[(i + 1) * N1] * v0 + tb.plap[(i + 1) * N1 + N1 - 1] * vn;
+          for (int h = 0; h < 2; ++h) {
+            const int r = r0 + h;
+            if (r >= M * M) break;
+            const int y = 1 + r / M, xx = 1 + r % M;
+            const T *src = stage + lp * S::STAGE + y * W + s_xo[lp] + xx;
+            const T v0 = src[0], vn = src[(N1 - 1) * N1 * W];
+            T *d1 = Z1 + lp * S::ZSZ + y * N1 + xx, *d2 = Z2 + lp * S::ZSZ + y * N1 + xx;
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+              d1[i * N1 * N1] = tb.pmass[(i + 1) * N1] * v0 + tb.pmass[(i + 1) * N1 + N1 - 1] * vn;
+              d2[i * N1 * N1] = tb.plap[(i + 1) * N1] * v0 + tb.plap[(i + 1) * N1 + N1 - 1] * vn;
+            }
           }
         }
       }
@@ -318,17 +366,18 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
         const int zi = r / N1, xx = r % N1;
         const T *s1 = Z1 + lp * S::ZSZ + zi * N1 * N1 + xx;
         const T *s2 = Z2 + lp * S::ZSZ + zi * N1 * N1 + xx;
-        T v[N1], e1[K + 1], o1[K > 1 ? K : 1], e2[K + 1], o2[K > 1 ? K : 1];
+        T v[N1], ec1, ec2;
+        P2 eo1[K > 1 ? K : 1], eo2[K > 1 ? K : 1];
 #pragma unroll
         for (int j = 0; j < N1; ++j) v[j] = s1[j * N1];
-        fold_in<K, T>(v, e1, o1);
+        fold_pairs<K, T>(v, eo1, ec1);
 #pragma unroll
         for (int j = 0; j < N1; ++j) v[j] = s2[j * N1];
-        fold_in<K, T>(v, e2, o2);
+        fold_pairs<K, T>(v, eo2, ec2);
         T ra[M], rb[M], rc[M];
-        fold_rows<K, T>(tb.pmass_fe, tb.pmass_fo, e2, o2, ra);
-        fold_rows<K, T>(tb.plap_fe, tb.plap_fo, e1, o1, rb);
-        fold_rows<K, T>(tb.pmass_fe, tb.pmass_fo, e1, o1, rc);
+        fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo2, ec2, ra);
+        fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo1, ec1, rb);
+        fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo1, ec1, rc);
         T *d1 = V1 + lp * VST + zi * M * N1 + xx, *d2 = V2 + lp * VST + zi * M * N1 + xx;
 #pragma unroll
         for (int i = 0; i < M; ++i) {
@@ -342,19 +391,20 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
     for (int t = tid; t < PPB * M * M; t += NT) {
       const int lp = t / (M * M), r = t % (M * M);  // r = zi * M + yi
       T res[M];
-      const T *bb = stage + lp * S::STAGE + S::BOFF + r * W + xoff(lp) + 1;
+      const T *bb = stage + lp * S::STAGE + S::BOFF + r * W + s_xo[lp] + 1;
       if (!a.zero_x) {
         const T *s1 = V1 + lp * VST + r * N1, *s2 = V2 + lp * VST + r * N1;
-        T v[N1], e1[K + 1], o1[K > 1 ? K : 1], e2[K + 1], o2[K > 1 ? K : 1];
+        T v[N1], ec1, ec2;
+        P2 eo1[K > 1 ? K : 1], eo2[K > 1 ? K : 1];
 #pragma unroll
         for (int j = 0; j < N1; ++j) v[j] = s1[j];
-        fold_in<K, T>(v, e1, o1);
+        fold_pairs<K, T>(v, eo1, ec1);
 #pragma unroll
         for (int j = 0; j < N1; ++j) v[j] = s2[j];
-        fold_in<K, T>(v, e2, o2);
+        fold_pairs<K, T>(v, eo2, ec2);
         T ra[M], rb[M];
-        fold_rows<K, T>(tb.pmass_fe, tb.pmass_fo, e1, o1, ra);
-        fold_rows<K, T>(tb.plap_fe, tb.plap_fo, e2, o2, rb);
+        fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo1, ec1, ra);
+        fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo2, ec2, rb);
 #pragma unroll
         for (int i = 0; i < M; ++i) res[i] = bb[i] - scale * (ra[i] + rb[i]);
       } else {
@@ -362,7 +412,7 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
         for (int i = 0; i < M; ++i) res[i] = bb[i];
       }
       T q[M];
-      apply_evec<K, T, true>(res, q);
+      apply_evec2<K, T, true>(res, q);
       T *d = Q1 + lp * S::QSZ + r * M;
 #pragma unroll
       for (int i = 0; i < M; ++i) d[i] = q[i];
@@ -376,7 +426,7 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j * M];
-      apply_evec<K, T, true>(v, q);
+      apply_evec2<K, T, true>(v, q);
       T *d = Q2 + lp * S::QSZ + zi * M * M + qx;
 #pragma unroll
       for (int j = 0; j < M; ++j) d[j * M] = q[j];
@@ -385,15 +435,14 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
     // ---- S^T along z, eigenvalue scaling, S along z: Q2 -> Q1 ---------------
     for (int t = tid; t < PPB * M * M; t += NT) {
       const int lp = t / (M * M), r = t % (M * M);
-      const int qy = r / M, qx = r % M;
       const T *s = Q2 + lp * S::QSZ + r;
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j * M * M];
-      apply_evec<K, T, true>(v, q);
+      apply_evec2<K, T, true>(v, q);
 #pragma unroll
       for (int j = 0; j < M; ++j) q[j] *= RL[j * M * M + r];
-      apply_evec<K, T, false>(q, v);
+      apply_evec2<K, T, false>(q, v);
       T *d = Q1 + lp * S::QSZ + r;
 #pragma unroll
       for (int j = 0; j < M; ++j) d[j * M * M] = v[j];
@@ -406,7 +455,7 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j];
-      apply_evec<K, T, false>(v, q);
+      apply_evec2<K, T, false>(v, q);
       T *d = Q2 + lp * S::QSZ + r * M;
 #pragma unroll
       for (int j = 0; j < M; ++j) d[j] = q[j];
@@ -420,11 +469,10 @@ __global__ void __launch_bounds__(Sm3<K, T>::NT)
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j * M];
-      apply_evec<K, T, false>(v, q);
-      if (lp < np) {
-        int fx, fy, fz;
-        patch_xyz(bt * PPB + lp, fx, fy, fz);
-        T *dst = x + (fx + 1 + xx) + (fy + 1) * a.sy + (fz + 1 + z) * a.sz;
+      apply_evec2<K, T, false>(v, q);
+      const int64_t base = s_base[lp];
+      if (base >= 0) {
+        T *dst = x + base + xx + z * a.sz;
 #pragma unroll
         for (int j = 0; j < M; ++j) dst[j * a.sy] = q[j];
       }

@@ -20,6 +20,26 @@ struct Dims {
   static constexpr int M = 2 * K - 1;   // interior DoFs per patch and direction
 };
 
+// Two values processed by one instruction: packed FP32x2 arithmetic on sm_100
+// (__ffma2_rn), component-wise FP64.
+template <typename T>
+struct Pair;
+template <>
+struct Pair<float> {
+  using type = float2;
+  static __host__ __device__ __forceinline__ float2 make(float a, float b) { return make_float2(a, b); }
+  static __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+};
+template <>
+struct Pair<double> {
+  using type = double2;
+  static __host__ __device__ __forceinline__ double2 make(double a, double b) { return make_double2(a, b); }
+  static __device__ __forceinline__ double2 fma(double2 a, double2 b, double2 c)
+  {
+    return make_double2(::fma(a.x, b.x, c.x), ::fma(a.y, b.y, c.y));
+  }
+};
+
 template <int K, typename T>
 struct DegreeTables {
   T pmass[Dims<K>::N1 * Dims<K>::N1];   // patch mass (reference cells)
@@ -38,6 +58,11 @@ struct DegreeTables {
   T plap_fe[K * (K + 1)];
   T pmass_fo[K > 1 ? (K - 1) * K : 1];
   T plap_fo[K > 1 ? (K - 1) * K : 1];
+  // the same folded rows as (even, odd) coefficient pairs {fe[r][j], fo[r][j]}, r < k-1, j < k
+  typename Pair<T>::type pmass_fp[K > 1 ? (K - 1) * K : 1];
+  typename Pair<T>::type plap_fp[K > 1 ? (K - 1) * K : 1];
+  // eigenvector pairs {S[r][q], S[r][k+q]} for r, q < k-1 (even mode q, odd mode k+q)
+  typename Pair<T>::type evec_p[K > 1 ? (K - 1) * (K - 1) : 1];
 };
 
 
