@@ -7,6 +7,7 @@ that ABI.
 from .api import (LaplaceOperator, MGTransferCUDA, MultigridSolvers, PatchSmoother,
                   PoissonProblem, SolveReport, split_cells)
 from ._lib import TpsError
+from .autograd import PoissonSolve
 
 __all__ = ["LaplaceOperator", "MGTransferCUDA", "MultigridSolvers", "PatchSmoother",
-           "PoissonProblem", "SolveReport", "TpsError", "split_cells"]
+           "PoissonProblem", "PoissonSolve", "SolveReport", "TpsError", "split_cells"]

@@ -50,7 +50,7 @@ class PoissonProblem:
     level set-up of MultigridSolvers, include/solver.cuh:1545-1744)."""
 
     def __init__(self, dim: int, degree: int, n_cells: int, relaxation: float = 1.0,
-                 n_coarse: int | None = None, device: int | None = None):
+                 n_coarse: int | None = None, device: int | None = None, kappa=None):
         if n_coarse is None:
             n_coarse, n_levels = split_cells(n_cells)
         else:
@@ -63,10 +63,51 @@ class PoissonProblem:
         self.dim, self.degree, self.n_cells = dim, degree, n_cells
         self.n_coarse, self.n_levels = n_coarse, n_levels
         self.device = torch.cuda.current_device() if device is None else device
-        pb = L.TpsProblem(dim, degree, n_coarse, n_levels, relaxation, None, self.device)
+        self.has_kappa = kappa is not None
+        kap = None
+        if kappa is not None:
+            self._kappa_host = self._kappa_array(kappa)
+            kap = self._kappa_host.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        pb = L.TpsProblem(dim, degree, n_coarse, n_levels, relaxation, kap, self.device)
         h = ctypes.c_void_p()
         L.check(L.lib().tps_create(ctypes.byref(pb), ctypes.byref(h)), None)
         self._h = h
+
+    def n_cells_total(self) -> int:
+        return self.n_cells ** self.dim
+
+    def _kappa_array(self, kappa):
+        import numpy as np
+        if isinstance(kappa, torch.Tensor):
+            kappa = kappa.detach().to("cpu", torch.float64).numpy()
+        a = np.ascontiguousarray(kappa, dtype=np.float64).ravel()
+        if a.size != self.n_cells ** self.dim:
+            raise ValueError(f"kappa needs {self.n_cells ** self.dim} per-cell values, got {a.size}")
+        return a
+
+    def set_kappa(self, kappa, rebuild_coarse: bool = True) -> None:
+        """Replace the per-cell coefficient (handle created with a kappa)."""
+        self._kappa_host = self._kappa_array(kappa)
+        L.check(L.lib().tps_set_kappa(self.handle, self._kappa_host.ctypes.data, int(rebuild_coarse)),
+                self.handle)
+
+    def mass_vmult(self, dst: torch.Tensor, src: torch.Tensor) -> None:
+        """dst = M src (finest level, all rows, FP64)."""
+        lvl = self.n_levels - 1
+        self._check_vec(dst, lvl, torch.float64)
+        self._check_vec(src, lvl, torch.float64)
+        L.check(L.lib().tps_mass_vmult(self.handle, dst.data_ptr(), src.data_ptr(), _stream()),
+                self.handle)
+
+    def cell_energy(self, u: torch.Tensor, lam: torch.Tensor) -> torch.Tensor:
+        """Per finest-level cell: lambda_c^T A_cell u_c (FP64)."""
+        lvl = self.n_levels - 1
+        self._check_vec(u, lvl, torch.float64)
+        self._check_vec(lam, lvl, torch.float64)
+        e = torch.empty(self.n_cells ** self.dim, dtype=torch.float64, device=u.device)
+        L.check(L.lib().tps_cell_energy(self.handle, u.data_ptr(), lam.data_ptr(), e.data_ptr(),
+                                        _stream()), self.handle)
+        return e
 
     def close(self):
         if getattr(self, "_h", None):

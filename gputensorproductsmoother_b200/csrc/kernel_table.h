@@ -54,6 +54,19 @@ struct KernelTable {
   cudaError_t (*restrict_[2][2])(const LevelGeomH &coarse, const VecLayout &lc,
                                  const VecLayout &lf, void *coarse_v, const void *fine, void *tmp,
                                  int add, cudaStream_t);
+  // variable coefficient (kappa per cell, lexicographic cells, precision of the vector):
+  // dst = A(kappa) src on interior rows (mode 0) or rhs - A(kappa) src (mode 1)
+  cudaError_t (*kappa_laplace[2][2])(const LevelGeomH &, const VecLayout &, void *dst,
+                                     const void *src, const void *rhs, const void *kappa, int mode,
+                                     cudaStream_t);
+  // one colour of the kappa patch sweep
+  cudaError_t (*kappa_smoother[2][2])(const LevelGeomH &, const VecLayout &, void *x, const void *b,
+                                      const void *kappa, int colour, double omega, cudaStream_t);
+  // dst = M src (all rows, FP64) and e_c = lambda_c^T A_cell u_c (FP64)
+  cudaError_t (*mass[2])(const LevelGeomH &, const VecLayout &, double *dst, const double *src,
+                         cudaStream_t);
+  cudaError_t (*cell_energy[2])(const LevelGeomH &, const VecLayout &, double *e, const double *u,
+                                const double *lam, cudaStream_t);
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda

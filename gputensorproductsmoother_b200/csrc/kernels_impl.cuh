@@ -5,6 +5,7 @@
 
 #include <vector>
 
+#include "kappa.cuh"
 #include "kernel_table.h"
 #include "laplace.cuh"
 #include "smoother.cuh"
@@ -97,6 +98,8 @@ cudaError_t set_attributes()
   TPS_SET((restrict_xy_kernel<K, T, XYOut::AddInterior>), (restrict_smem<T>()));
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetInterior>), (restrict_smem<T>()));
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetAll>), (restrict_smem<T>()));
+  TPS_SET((kappa_smoother_kernel<2, K, T>), (sizeof(T) * KSm<2, K, T>::ELEMS));
+  TPS_SET((kappa_smoother_kernel<3, K, T>), (sizeof(T) * KSm<3, K, T>::ELEMS));
 #undef TPS_SET
   return cudaSuccess;
 }
@@ -263,6 +266,84 @@ cudaError_t restrict_(const LevelGeomH &gc, const VecLayout &lc, const VecLayout
   return cudaGetLastError();
 }
 
+// cells of colour c: parities of (cx, cy, cz)
+inline void cell_lattice(int dim, int n, int colour, int &nx, int &ny, int &nz)
+{
+  auto cnt = [&](int parity) { return n > parity ? (n - parity + 1) / 2 : 0; };
+  nx = cnt(colour & 1);
+  ny = cnt((colour >> 1) & 1);
+  nz = dim == 3 ? cnt((colour >> 2) & 1) : 1;
+}
+
+template <int DIM, typename T, bool MASS>
+cudaError_t cell_sweep(const LevelGeomH &g, const VecLayout &l, T *dst, const T *src, const T *kappa,
+                       double s, cudaStream_t st)
+{
+  for (int c = 0; c < (1 << DIM); ++c) {
+    int nx, ny, nz;
+    cell_lattice(DIM, g.n, c, nx, ny, nz);
+    const int count = nx * ny * nz;
+    if (count == 0) continue;
+    cell_apply_kernel<DIM, K, T, MASS><<<count, KappaCfg<DIM, K>::NT, 0, st>>>(
+        dst, src, kappa, g.n, c, nx, ny, l.sy, l.sz, static_cast<T>(s));
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+template <int DIM, typename T>
+cudaError_t kappa_laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const void *src,
+                          const void *rhs, const void *kappa, int mode, cudaStream_t st)
+{
+  const int64_t n = DIM == 3 ? l.sz * g.N1 : l.sy * g.N1;
+  cudaError_t e = cudaMemsetAsync(dst, 0, sizeof(T) * n, st);
+  if (e != cudaSuccess) return e;
+  e = cell_sweep<DIM, T, false>(g, l, static_cast<T *>(dst), static_cast<const T *>(src),
+                                static_cast<const T *>(kappa), stiffness_scale(DIM, g.h), st);
+  if (e != cudaSuccess) return e;
+  // Dirichlet rows end at 0 like the unit-coefficient kernel's untouched rows
+  // of zero-initialised work vectors; tps_laplace_vmult then copies src there
+  finish_residual_kernel<DIM, T><<<1184, 256, 0, st>>>(
+      static_cast<T *>(dst), mode == 1 ? static_cast<const T *>(rhs) : nullptr, g.N1, l.sy, l.sz);
+  return cudaGetLastError();
+}
+
+template <int DIM, typename T>
+cudaError_t kappa_smoother(const LevelGeomH &g, const VecLayout &l, void *x, const void *b,
+                           const void *kappa, int colour, double omega, cudaStream_t st)
+{
+  int nx, ny, nz, count;
+  colour_lattice(DIM, g.n, colour, nx, ny, nz, count);
+  if (count == 0) return cudaSuccess;
+  const double sc = stiffness_scale(DIM, g.h);
+  kappa_smoother_kernel<DIM, K, T><<<count, KSm<DIM, K, T>::NT, sizeof(T) * KSm<DIM, K, T>::ELEMS, st>>>(
+      static_cast<T *>(x), static_cast<const T *>(b), static_cast<const T *>(kappa), g.n, colour,
+      nx, ny, l.sy, l.sz, static_cast<T>(sc), static_cast<T>(1.0 / sc), static_cast<T>(omega));
+  return cudaGetLastError();
+}
+
+template <int DIM>
+cudaError_t mass(const LevelGeomH &g, const VecLayout &l, double *dst, const double *src, cudaStream_t st)
+{
+  const int64_t n = DIM == 3 ? l.sz * g.N1 : l.sy * g.N1;
+  cudaError_t e = cudaMemsetAsync(dst, 0, sizeof(double) * n, st);
+  if (e != cudaSuccess) return e;
+  double hd = 1.0;
+  for (int d = 0; d < DIM; ++d) hd *= g.h;
+  return cell_sweep<DIM, double, true>(g, l, dst, src, nullptr, hd, st);
+}
+
+template <int DIM>
+cudaError_t cell_energy(const LevelGeomH &g, const VecLayout &l, double *e, const double *u,
+                        const double *lam, cudaStream_t st)
+{
+  const int64_t ncell = DIM == 3 ? int64_t(g.n) * g.n * g.n : int64_t(g.n) * g.n;
+  cell_energy_kernel<DIM, K><<<static_cast<unsigned>(ncell), KappaCfg<DIM, K>::NT, 0, st>>>(
+      e, u, lam, g.n, l.sy, l.sz, stiffness_scale(DIM, g.h));
+  return cudaGetLastError();
+}
+
 }  // namespace deg_impl
 }  // namespace
 
@@ -281,6 +362,12 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
      {&deg_impl::prolong<3, double>, &deg_impl::prolong<3, float>}},
     {{&deg_impl::restrict_<2, double>, &deg_impl::restrict_<2, float>},
      {&deg_impl::restrict_<3, double>, &deg_impl::restrict_<3, float>}},
+    {{&deg_impl::kappa_laplace<2, double>, &deg_impl::kappa_laplace<2, float>},
+     {&deg_impl::kappa_laplace<3, double>, &deg_impl::kappa_laplace<3, float>}},
+    {{&deg_impl::kappa_smoother<2, double>, &deg_impl::kappa_smoother<2, float>},
+     {&deg_impl::kappa_smoother<3, double>, &deg_impl::kappa_smoother<3, float>}},
+    {&deg_impl::mass<2>, &deg_impl::mass<3>},
+    {&deg_impl::cell_energy<2>, &deg_impl::cell_energy<3>},
 };
 
 }  // namespace tps

@@ -132,6 +132,10 @@ struct tps_handle {
   std::vector<int> coarse_coord;        // (x, y, z) of each interior coarse DoF
   VcycleVectors vc[2];  // [0] FP64, [1] FP32
   DevBuf err_flag;      // set by a kernel whose bounded wait gave up
+  // variable coefficient: per-level per-cell kappa (fine given, coarse = mean of children)
+  bool has_kappa = false;
+  std::vector<std::vector<double>> kappa_host;
+  std::vector<std::unique_ptr<DevBuf>> kappa_dev[2];  // [FP64, FP32][level]
   // Krylov work vectors (fine level, FP64)
   DevBuf r, p, q, partial, scalars;
   std::vector<std::unique_ptr<DevBuf>> gmres_v;
@@ -192,47 +196,54 @@ int guarded(tps_handle *h, F &&f)
   }
 }
 
-// dense interior operator of the coarse level, assembled on the host in FP64
-// as the Kronecker sum of the global 1D matrices, and its inverse
+// dense interior operator of the coarse level, assembled cell by cell on the
+// host in FP64 (with the coarse-level kappa when present), and its inverse
 void build_dense_coarse(tps_handle *h)
 {
   const int k = h->k, n = h->n_coarse, N1 = n * k + 1, dim = h->dim;
   const double hh = 1.0 / n, s = stiffness_scale(dim, hh);
   const int np = k + 1;
-  std::vector<double> M1(N1 * N1, 0.0), L1(N1 * N1, 0.0);
-  for (int c = 0; c < n; ++c)
-    for (int a = 0; a < np; ++a)
-      for (int b = 0; b < np; ++b) {
-        M1[(c * k + a) * N1 + c * k + b] += h->D.cmass[a * np + b];
-        L1[(c * k + a) * N1 + c * k + b] += h->D.clap[a * np + b];
-      }
   std::vector<int> idx1;
   for (int i = 1; i < N1 - 1; ++i) idx1.push_back(i);
   const int m1 = static_cast<int>(idx1.size());
   const int ni = dim == 3 ? m1 * m1 * m1 : m1 * m1;
   h->n_int_coarse = ni;
-  std::vector<double> A(static_cast<size_t>(ni) * ni, 0.0);
   auto coord = [&](int i, int &x, int &y, int &z) {
     x = idx1[i % m1];
     y = idx1[(i / m1) % m1];
     z = dim == 3 ? idx1[i / (m1 * m1)] : 0;
   };
-  for (int i = 0; i < ni; ++i) {
-    int xi, yi, zi;
-    coord(i, xi, yi, zi);
-    for (int j = 0; j < ni; ++j) {
-      int xj, yj, zj;
-      coord(j, xj, yj, zj);
-      const double mx = M1[xi * N1 + xj], my = M1[yi * N1 + yj];
-      const double lx = L1[xi * N1 + xj], ly = L1[yi * N1 + yj];
-      double v;
-      if (dim == 2) {
-        v = ly * mx + my * lx;
-      } else {
-        const double mz = M1[zi * N1 + zj], lz = L1[zi * N1 + zj];
-        v = lz * my * mx + mz * ly * mx + mz * my * lx;
+  // interior index of a global coarse DoF (-1 on the boundary)
+  auto interior = [&](int x, int y, int z) -> int {
+    if (x < 1 || x > N1 - 2 || y < 1 || y > N1 - 2) return -1;
+    if (dim == 3 && (z < 1 || z > N1 - 2)) return -1;
+    return (x - 1) + (y - 1) * m1 + (dim == 3 ? (z - 1) * m1 * m1 : 0);
+  };
+  std::vector<double> A(static_cast<size_t>(ni) * ni, 0.0);
+  const int ncell = dim == 3 ? n * n * n : n * n;
+  const int csz = dim == 3 ? np * np * np : np * np;
+  for (int c = 0; c < ncell; ++c) {
+    const int cx = c % n, cy = (c / n) % n, cz = dim == 3 ? c / (n * n) : 0;
+    const double kc = h->has_kappa ? h->kappa_host[0][c] : 1.0;
+    for (int a = 0; a < csz; ++a) {
+      const int ax = a % np, ay = (a / np) % np, az = dim == 3 ? a / (np * np) : 0;
+      const int ia = interior(cx * k + ax, cy * k + ay, cz * k + az);
+      if (ia < 0) continue;
+      for (int b2 = 0; b2 < csz; ++b2) {
+        const int bx = b2 % np, by = (b2 / np) % np, bz = dim == 3 ? b2 / (np * np) : 0;
+        const int ib = interior(cx * k + bx, cy * k + by, cz * k + bz);
+        if (ib < 0) continue;
+        const double mx = h->D.cmass[ax * np + bx], my = h->D.cmass[ay * np + by];
+        const double lx = h->D.clap[ax * np + bx], ly = h->D.clap[ay * np + by];
+        double v;
+        if (dim == 2) {
+          v = ly * mx + my * lx;
+        } else {
+          const double mz = h->D.cmass[az * np + bz], lz = h->D.clap[az * np + bz];
+          v = lz * my * mx + mz * ly * mx + mz * my * lx;
+        }
+        A[static_cast<size_t>(ia) * ni + ib] += kc * s * v;
       }
-      A[static_cast<size_t>(i) * ni + j] = s * v;
     }
   }
   // Cholesky and explicit inverse (coarse systems hold at most a few thousand DoFs)
@@ -345,9 +356,67 @@ void smoother_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void 
   const int nc = 1 << h->dim;
   for (int i = 0; i < nc; ++i) {
     const int c = reverse ? nc - 1 - i : i;
-    TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], lay, x, b, c, h->omega,
-                                            (x_zero && i == 0) ? 1 : 0, maps,
-                                            h->err_flag.as<int>(), s));
+    if (h->has_kappa)
+      TPS_CUDA(h->kt->kappa_smoother[h->dim - 2][p](h->lv[level], lay, x, b,
+                                                    h->kappa_dev[p][level]->p, c, h->omega, s));
+    else
+      TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], lay, x, b, c, h->omega,
+                                              (x_zero && i == 0) ? 1 : 0, maps,
+                                              h->err_flag.as<int>(), s));
+  }
+}
+
+// level operator: dst = A src (mode 0, interior rows) or rhs - A src (mode 1)
+void level_laplace(tps_handle *h, int level, int p, const VecLayout &lay, void *dst, const void *src,
+                   const void *rhs, int mode, cudaStream_t s)
+{
+  if (h->has_kappa)
+    TPS_CUDA(h->kt->kappa_laplace[h->dim - 2][p](h->lv[level], lay, dst, src, rhs,
+                                                 h->kappa_dev[p][level]->p, mode, s));
+  else
+    TPS_CUDA(h->kt->laplace[h->dim - 2][p](h->lv[level], lay, dst, src, rhs, mode, s));
+}
+
+// per-level coefficients from the finest-level kappa (coarse = mean of the 2^d children)
+void set_kappa_levels(tps_handle *h, const double *kappa_fine)
+{
+  const int L = h->n_levels - 1, dim = h->dim;
+  h->kappa_host.assign(h->n_levels, {});
+  const int64_t ncf = dim == 3 ? int64_t(h->lv[L].n) * h->lv[L].n * h->lv[L].n
+                               : int64_t(h->lv[L].n) * h->lv[L].n;
+  for (int64_t c = 0; c < ncf; ++c)
+    if (!(kappa_fine[c] > 0.0) || !std::isfinite(kappa_fine[c]))
+      throw ApiError(TPS_ERR_INVALID, "kappa must be positive and finite");
+  h->kappa_host[L].assign(kappa_fine, kappa_fine + ncf);
+  for (int l = L - 1; l >= 0; --l) {
+    const int n = h->lv[l].n, nf = h->lv[l + 1].n;
+    const int64_t nc = dim == 3 ? int64_t(n) * n * n : int64_t(n) * n;
+    h->kappa_host[l].assign(nc, 0.0);
+    for (int64_t c = 0; c < nc; ++c) {
+      const int cx = int(c % n), cy = int((c / n) % n), cz = dim == 3 ? int(c / (int64_t(n) * n)) : 0;
+      double acc = 0.0;
+      for (int q = 0; q < (1 << dim); ++q) {
+        const int fx = 2 * cx + (q & 1), fy = 2 * cy + ((q >> 1) & 1), fz = 2 * cz + ((q >> 2) & 1);
+        acc += h->kappa_host[l + 1][fx + int64_t(fy) * nf + (dim == 3 ? int64_t(fz) * nf * nf : 0)];
+      }
+      h->kappa_host[l][c] = acc / (1 << dim);
+    }
+  }
+  for (int p = 0; p < 2; ++p) {
+    h->kappa_dev[p].clear();
+    for (int l = 0; l < h->n_levels; ++l) {
+      h->kappa_dev[p].emplace_back(new DevBuf);
+      const size_t nc = h->kappa_host[l].size();
+      if (p == 0) {
+        h->kappa_dev[p][l]->alloc(sizeof(double) * nc);
+        TPS_CUDA(cudaMemcpy(h->kappa_dev[p][l]->p, h->kappa_host[l].data(), sizeof(double) * nc,
+                            cudaMemcpyHostToDevice));
+      } else {
+        std::vector<float> f(h->kappa_host[l].begin(), h->kappa_host[l].end());
+        h->kappa_dev[p][l]->alloc(sizeof(float) * nc);
+        TPS_CUDA(cudaMemcpy(h->kappa_dev[p][l]->p, f.data(), sizeof(float) * nc, cudaMemcpyHostToDevice));
+      }
+    }
   }
 }
 
@@ -380,7 +449,7 @@ void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s)
   const int di = h->dim - 2;
   TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, V.su[level]->bytes, s));
   smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, true, &V.maps[level], s);
-  TPS_CUDA(h->kt->laplace[di][p](g, lay, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s));
+  level_laplace(h, level, p, lay, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s);
   TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], lc, lay, V.d[level - 1]->p, V.t[level]->p,
                                    V.tmp[level]->p, 0, s));
   vcycle_rec(h, level - 1, p, symmetric, s);
@@ -406,7 +475,7 @@ PadMap fine_padmap(tps_handle *h, int p)
 void fine_vmult64(tps_handle *h, double *dst, const double *src, cudaStream_t s)
 {
   const LevelGeomH &g = h->fine();
-  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, lex_layout(h, h->n_levels - 1), dst, src, nullptr, 0, s));
+  level_laplace(h, h->n_levels - 1, 0, lex_layout(h, h->n_levels - 1), dst, src, nullptr, 0, s);
   TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, 8, s));
 }
 
@@ -442,7 +511,7 @@ void cg_iteration_body(tps_handle *h, int prec, bool symmetric, double *x, cudaS
   vcycle_rec(h, L, p, symmetric, s);
   TPS_CUDA(launch_cg_beta(V.su[L]->p, zk, pm, h->q.as<double>(), h->r.as<double>(), N, part, sc, s));
   TPS_CUDA(launch_cg_update_p(h->p.as<double>(), V.su[L]->p, zk, pm, N, sc, s));
-  TPS_CUDA(h->kt->laplace[h->dim - 2][0](h->fine(), lex, h->q.p, h->p.p, nullptr, 0, s));
+  level_laplace(h, L, 0, lex, h->q.p, h->p.p, nullptr, 0, s);
   TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
   TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
                                V.d[L]->p, input_kind(prec), pm, N, part, sc, s));
@@ -476,7 +545,7 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
   TPS_CUDA(launch_copy_boundary(x, b, h->dim, g.N1, 8, s));
   TPS_CUDA(cudaMemsetAsync(h->r.p, 0, sizeof(double) * N, s));
   TPS_CUDA(cudaMemsetAsync(h->q.p, 0, sizeof(double) * N, s));
-  TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, lex, h->r.p, x, b, 1, s));
+  level_laplace(h, L, 0, lex, h->r.p, x, b, 1, s);
   TPS_CUDA(launch_cg_init(h->r.as<double>(), b, V.d[L]->p, input_kind(o.precision), pm, N, part, s));
   TPS_CUDA(launch_cg_finalize_init(part, sc, s));
   CGScalars hs{};
@@ -495,7 +564,7 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
     TPS_CUDA(launch_cg_first_direction(h->p.as<double>(), V.su[L]->p, zk, pm, h->r.as<double>(), N,
                                        part, s));
     TPS_CUDA(launch_cg_finalize_rz(part, sc, s));
-    TPS_CUDA(h->kt->laplace[h->dim - 2][0](g, lex, h->q.p, h->p.p, nullptr, 0, s));
+    level_laplace(h, L, 0, lex, h->q.p, h->p.p, nullptr, 0, s);
     TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
     TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
                                  V.d[L]->p, input_kind(o.precision), pm, N, part, sc, s));
@@ -723,7 +792,6 @@ int tps_create(const tps_problem *pb, tps_handle **out)
       throw ApiError(TPS_ERR_UNSUPPORTED, "degree must be in 1..7");
     if (pb->n_coarse < 2) throw ApiError(TPS_ERR_INVALID, "n_coarse must be >= 2");
     if (pb->n_levels < 1 || pb->n_levels > 12) throw ApiError(TPS_ERR_INVALID, "n_levels must be in 1..12");
-    if (pb->kappa) throw ApiError(TPS_ERR_UNSUPPORTED, "variable coefficients are not supported by this build");
     if (!(pb->relaxation > 0.0)) throw ApiError(TPS_ERR_INVALID, "relaxation must be positive");
     const int64_t nf = static_cast<int64_t>(pb->n_coarse) << (pb->n_levels - 1);
     const int64_t N1f = nf * pb->degree + 1;
@@ -749,7 +817,12 @@ int tps_create(const tps_problem *pb, tps_handle **out)
     if (!h->kt) throw ApiError(TPS_ERR_UNSUPPORTED, "degree not compiled in");
     h->D = make_degree_data(pb->degree);
     TPS_CUDA(h->kt->upload(h->D));
-    h->dense_coarse = pb->n_coarse != 2;
+    if (pb->kappa) {
+      h->has_kappa = true;
+      set_kappa_levels(h.get(), pb->kappa);
+    }
+    // the single coarse patch is an exact solve only for a unit coefficient on 2 cells
+    h->dense_coarse = pb->n_coarse != 2 || h->has_kappa;
     if (h->dense_coarse) {
       const int64_t m1 = int64_t(pb->n_coarse) * pb->degree - 1;
       const int64_t ni = pb->dim == 3 ? m1 * m1 * m1 : m1 * m1;
@@ -802,7 +875,7 @@ int tps_laplace_vmult(tps_handle *h, int level, int dtype, void *dst, const void
     if (dst == src) throw ApiError(TPS_ERR_INVALID, "dst and src must not alias");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const LevelGeomH &g = h->lv[level];
-    TPS_CUDA(h->kt->laplace[h->dim - 2][p](g, lex_layout(h, level), dst, src, nullptr, 0, s));
+    level_laplace(h, level, p, lex_layout(h, level), dst, src, nullptr, 0, s);
     TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, p == 0 ? 8 : 4, s));
   });
 }
@@ -882,6 +955,54 @@ int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double
   if (status == TPS_ERR_BREAKDOWN) h->err = "Krylov breakdown (p^T A p <= 0)";
   if (status == TPS_ERR_NONFINITE) h->err = "non-finite residual";
   return status;
+}
+
+int tps_set_kappa(tps_handle *h, const double *kappa, int rebuild_coarse)
+{
+  return guarded(h, [&] {
+    if (!h->has_kappa) throw ApiError(TPS_ERR_INVALID, "the handle was created with kappa = NULL");
+    if (!kappa) throw ApiError(TPS_ERR_INVALID, "null kappa");
+    TPS_CUDA(cudaDeviceSynchronize());
+    set_kappa_levels(h, kappa);
+    if (rebuild_coarse) {
+      build_dense_coarse(h);
+      for (int p = 0; p < 2; ++p) {
+        VcycleVectors &V = h->vc[p];
+        if (!V.ready) continue;
+        const size_t n2 = h->coarse_inv_host.size();
+        if (p == 0) {
+          TPS_CUDA(cudaMemcpy(V.coarse_inv.p, h->coarse_inv_host.data(), 8 * n2, cudaMemcpyHostToDevice));
+        } else {
+          std::vector<float> f(h->coarse_inv_host.begin(), h->coarse_inv_host.end());
+          TPS_CUDA(cudaMemcpy(V.coarse_inv.p, f.data(), 4 * n2, cudaMemcpyHostToDevice));
+        }
+      }
+    }
+    if (h->graph) {  // the captured iteration reads the kappa buffers it was built with
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+  });
+}
+
+int tps_mass_vmult(tps_handle *h, double *dst, const double *src, void *stream)
+{
+  return guarded(h, [&] {
+    if (!dst || !src || dst == src) throw ApiError(TPS_ERR_INVALID, "bad vectors");
+    const int L = h->n_levels - 1;
+    TPS_CUDA(h->kt->mass[h->dim - 2](h->lv[L], lex_layout(h, L), dst, src,
+                                     static_cast<cudaStream_t>(stream)));
+  });
+}
+
+int tps_cell_energy(tps_handle *h, const double *u, const double *lam, double *energy, void *stream)
+{
+  return guarded(h, [&] {
+    if (!u || !lam || !energy) throw ApiError(TPS_ERR_INVALID, "null vector");
+    const int L = h->n_levels - 1;
+    TPS_CUDA(h->kt->cell_energy[h->dim - 2](h->lv[L], lex_layout(h, L), energy, u, lam,
+                                            static_cast<cudaStream_t>(stream)));
+  });
 }
 
 int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *ms_per_sweep,

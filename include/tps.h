@@ -44,8 +44,8 @@ typedef struct {
   int n_coarse;        /* cells per direction of the coarsest level (>= 2) */
   int n_levels;        /* the finest level has n_coarse * 2^(n_levels-1) cells/direction */
   double relaxation;   /* smoother damping omega (reference default 1.0) */
-  const double *kappa; /* HOST array of per-cell coefficients on the finest level
-                          (lexicographic cells) or NULL for kappa = 1 */
+  const double *kappa; /* HOST array of per-cell coefficients (> 0) on the finest
+                          level (lexicographic cells) or NULL for kappa = 1 */
   int device;          /* CUDA device ordinal */
 } tps_problem;
 
@@ -126,6 +126,24 @@ void tps_solve_opts_default(tps_solve_opts *opts);
  * guess on entry).  Replaces MultigridSolvers::solve_gmres and adds the MG-CG driver. */
 int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double *x,
               tps_report *report, void *stream);
+
+/* Variable coefficient -div(kappa grad u) (no reference counterpart; the
+ * reference's operator has kappa = 1).  A handle created with a kappa array can
+ * change it: the finest-level values are replaced, the coarser levels take the
+ * mean of their 2^d children; rebuild_coarse = 1 also refactors the dense
+ * coarse solve (otherwise the V-cycle keeps its previous coarse operator, which
+ * only affects the preconditioner).  Synchronises the device. */
+int tps_set_kappa(tps_handle *h, const double *kappa_host, int rebuild_coarse);
+
+/* dst = M src with the finest-level mass matrix (all rows), FP64, device
+ * buffers.  Used for b = M f and the gradient dJ/df = M lambda. */
+int tps_mass_vmult(tps_handle *h, double *dst, const double *src, void *stream);
+
+/* energy[c] = lambda_c^T A_cell u_c = int_c grad(lambda).grad(u) for every
+ * finest-level cell c (lexicographic cells), FP64: dJ/dkappa_c = -energy[c]
+ * for J(u(kappa)) with adjoint state lambda. */
+int tps_cell_energy(tps_handle *h, const double *u, const double *lam, double *energy,
+                    void *stream);
 
 /* Measurement hook: runs `sweeps` coloured sweeps of the level's smoother on
  * the V-cycle's own work vectors (the padded, TMA-staged path that the V-cycle

@@ -1,0 +1,131 @@
+"""GPU tests of the variable-coefficient path and the adjoint gradients
+(no reference counterpart; checked against the CPU oracle, dense algebra and
+central finite differences)."""
+import numpy as np
+import pytest
+import torch
+
+import gputensorproductsmoother_b200 as tps
+
+pytestmark = pytest.mark.gpu
+
+
+def relerr(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def kappa_field(dim, n, seed):
+    return np.exp(np.random.default_rng(seed).normal(0.0, 0.5, n ** dim))
+
+
+def bvec(dim, N1, seed):
+    b = np.random.default_rng(seed).uniform(-1, 1, N1 ** dim)
+    idx = np.stack(np.unravel_index(np.arange(N1 ** dim), (N1,) * dim))
+    b[np.any((idx == 0) | (idx == N1 - 1), axis=0)] = 0.0
+    return b
+
+
+@pytest.mark.parametrize("dim,k,n", [(2, 2, 8), (2, 3, 4), (3, 2, 4), (3, 4, 4), (3, 3, 6)])
+@pytest.mark.parametrize("dtype,tol", [(torch.float64, 1e-12), (torch.float32, 2e-5)])
+def test_kappa_level_ops(cuda, oracle, dim, k, n, dtype, tol):
+    kap = kappa_field(dim, n, 1)
+    P = tps.PoissonProblem(dim, k, n, kappa=kap)
+    N = P.n_dofs()
+    rng = np.random.default_rng(2)
+    x0, b = rng.uniform(-1, 1, N), rng.uniform(-1, 1, N)
+    npdt = np.float64 if dtype == torch.float64 else np.float32
+    ref = oracle.laplace_vmult(dim, k, n, x0.astype(npdt), kappa=kap)
+    y = P.new_vector(dtype=dtype)
+    tps.LaplaceOperator(P).vmult(y, torch.tensor(x0, dtype=dtype, device="cuda"))
+    torch.cuda.synchronize()
+    assert relerr(y.cpu().numpy(), ref) < tol
+    ref = oracle.smoother_step(dim, k, n, x0.astype(npdt), b.astype(npdt), kappa=kap)
+    x = torch.tensor(x0, dtype=dtype, device="cuda")
+    tps.PatchSmoother(P).step(x, torch.tensor(b, dtype=dtype, device="cuda"))
+    torch.cuda.synchronize()
+    assert relerr(x.cpu().numpy(), ref) < tol
+
+
+@pytest.mark.parametrize("dim,k,n", [(2, 2, 8), (3, 2, 6), (3, 3, 4)])
+def test_kappa_vcycle_and_cg(cuda, oracle, dim, k, n):
+    kap = kappa_field(dim, n, 3)
+    P = tps.PoissonProblem(dim, k, n, kappa=kap)
+    H = oracle.Hierarchy(dim, k, P.n_coarse, P.n_levels, kappa=kap)
+    b = bvec(dim, n * k + 1, 4)
+    ref = H.vcycle(b, precision=0, symmetric=True)
+    z = P.new_vector()
+    tps.MultigridSolvers(P).vmult(z, torch.tensor(b, device="cuda"), precision="fp64", symmetric=True)
+    torch.cuda.synchronize()
+    assert relerr(z.cpu().numpy(), ref) < 1e-11
+    xr, itr, _ = H.solve_cg(b, precision=0, symmetric=True, rel_tol=1e-10)
+    x, rep = tps.MultigridSolvers(P).solve_cg(torch.tensor(b, device="cuda"), precision="fp64",
+                                              rel_tol=1e-10)
+    # the patch-mean-kappa local solve makes the smoother weak for strongly
+    # varying kappa; in slowly converging runs rounding can shift the count
+    assert rep.converged and abs(rep.iterations - itr) <= 1 + itr // 20
+    assert relerr(x.cpu().numpy(), xr) < 1e-8
+    x32, rep32 = tps.MultigridSolvers(P).solve_cg(torch.tensor(b, device="cuda"), precision="fp32",
+                                                  rel_tol=1e-10, max_iter=400)
+    assert rep32.converged and relerr(x32.cpu().numpy(), xr) < 1e-8
+
+
+@pytest.mark.parametrize("dim,k,n", [(2, 3, 4), (3, 2, 4)])
+def test_mass_and_cell_energy(cuda, oracle, dim, k, n):
+    kap = kappa_field(dim, n, 5)
+    P = tps.PoissonProblem(dim, k, n, kappa=kap)
+    N1 = n * k + 1
+    from gputensorproductsmoother_b200 import problems
+    M1 = problems.mass_1d(k, n)
+    M = M1
+    for _ in range(dim - 1):
+        M = np.kron(M, M1)
+    rng = np.random.default_rng(6)
+    f = rng.uniform(-1, 1, N1 ** dim)
+    out = P.new_vector()
+    P.mass_vmult(out, torch.tensor(f, device="cuda"))
+    torch.cuda.synchronize()
+    assert relerr(out.cpu().numpy(), M @ f) < 1e-13
+    u, lam = bvec(dim, N1, 7), bvec(dim, N1, 8)
+    e = P.cell_energy(torch.tensor(u, device="cuda"), torch.tensor(lam, device="cuda")).cpu().numpy()
+    for c in [0, 3, n ** dim - 1]:
+        ind = np.zeros(n ** dim)
+        ind[c] = 1.0
+        Au = oracle.laplace_vmult(dim, k, n, u, kappa=ind)
+        assert abs(e[c] - lam @ Au) <= 1e-12 * max(1.0, abs(lam @ Au))
+    assert abs(e.sum() - lam @ oracle.laplace_vmult(dim, k, n, u)) < 1e-11 * np.abs(e).sum()
+
+
+def test_adjoint_gradients_match_finite_differences(cuda):
+    """J = 0.5 ||u - u_t||^2 with A(kappa) u = M f: the adjoint gradients agree
+    with central differences (h = 1e-6) to 1e-6 in random directions."""
+    dim, k, n = 3, 2, 6  # coarse 3^3 cells: dense coarse solve
+    rng = np.random.default_rng(9)
+    kap = torch.tensor(np.exp(rng.normal(0, 0.5, n ** dim)), dtype=torch.float64, device="cuda")
+    P = tps.PoissonProblem(dim, k, n, kappa=kap)
+    N = P.n_dofs()
+    f = torch.tensor(rng.standard_normal(N), device="cuda", requires_grad=True)
+    # target = perturbed solution, so J and its derivatives have one scale and
+    # central differences are not swamped by rounding of a large J
+    with torch.no_grad():
+        u0 = tps.autograd.solve(P, f, kap, rel_tol=1e-14)
+    ut = u0 * torch.tensor(1.0 + 0.3 * rng.standard_normal(N), device="cuda")
+    kv = kap.clone().requires_grad_(True)
+
+    def J(f_, k_):
+        u = tps.autograd.solve(P, f_, k_, rel_tol=1e-14)
+        return 0.5 * ((u - ut) ** 2).sum()
+
+    j = J(f, kv)
+    j.backward()
+    gf, gk = f.grad.detach().clone(), kv.grad.detach().clone()
+    h = 1e-6
+    for d in range(4):
+        df = torch.tensor(rng.standard_normal(N), device="cuda")
+        dk = torch.tensor(rng.standard_normal(n ** dim), device="cuda") * kap
+        with torch.no_grad():
+            fd_f = (J(f + h * df, kap) - J(f - h * df, kap)) / (2 * h)
+            fd_k = (J(f, kap + h * dk) - J(f, kap - h * dk)) / (2 * h)
+        ad_f, ad_k = (gf * df).sum(), (gk * dk).sum()
+        assert abs(ad_f - fd_f) <= 1e-6 * abs(fd_f), (d, ad_f.item(), fd_f.item())
+        assert abs(ad_k - fd_k) <= 1e-6 * abs(fd_k), (d, ad_k.item(), fd_k.item())
