@@ -17,8 +17,8 @@ STATUS_NAMES = {
     4: "TPS_ERR_NOT_CONVERGED", 5: "TPS_ERR_BREAKDOWN", 6: "TPS_ERR_NONFINITE",
     7: "TPS_ERR_UNSUPPORTED",
 }
-TPS_F64, TPS_F32 = 0, 1
-VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED = 0, 1, 2
+TPS_F64, TPS_F32, TPS_TF32 = 0, 1, 2
+VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32 = 0, 1, 2, 3
 DRIVER_CG, DRIVER_GMRES = 0, 1
 MAX_HISTORY = 256
 

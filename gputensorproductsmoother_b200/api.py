@@ -25,7 +25,8 @@ import torch
 from . import _lib as L
 
 _DTYPES = {torch.float64: L.TPS_F64, torch.float32: L.TPS_F32}
-_PRECISIONS = {"fp64": L.VCYCLE_F64, "fp32": L.VCYCLE_F32, "fp64_rounded": L.VCYCLE_F64_ROUNDED}
+_PRECISIONS = {"fp64": L.VCYCLE_F64, "fp32": L.VCYCLE_F32, "fp64_rounded": L.VCYCLE_F64_ROUNDED,
+               "tf32": L.VCYCLE_TF32}
 
 
 def split_cells(n_cells: int) -> tuple[int, int]:
@@ -90,6 +91,17 @@ class PoissonProblem:
         self._kappa_host = self._kappa_array(kappa)
         L.check(L.lib().tps_set_kappa(self.handle, self._kappa_host.ctypes.data, int(rebuild_coarse)),
                 self.handle)
+
+    def time_smoother(self, level: int | None = None, dtype: str = "fp32", sweeps: int = 20) -> float:
+        """Milliseconds per coloured sweep on the level's V-cycle work vectors
+        (CUDA events on the current stream); dtype "fp64", "fp32" or "tf32"
+        (tensor-core patch solves)."""
+        codes = {"fp64": L.TPS_F64, "fp32": L.TPS_F32, "tf32": L.TPS_TF32}
+        ms = ctypes.c_double()
+        lv = self.n_levels - 1 if level is None else level
+        L.check(L.lib().tps_time_smoother(self.handle, lv, codes[dtype], sweeps, ctypes.byref(ms), _stream()),
+                self.handle)
+        return ms.value
 
     def mass_vmult(self, dst: torch.Tensor, src: torch.Tensor) -> None:
         """dst = M src (finest level, all rows, FP64)."""
@@ -177,16 +189,23 @@ class LaplaceOperator:
 
 class PatchSmoother:
     """PatchSmoother (PreconditionRelaxation over the coloured vertex-patch
-    sweep): vmult zeroes dst and sweeps once, step sweeps once in place."""
+    sweep): vmult zeroes dst and sweeps once, step sweeps once in place.
+    tensor_cores=True runs the 3D patch solves of FP32 vectors on the tensor
+    cores (TF32 operands, FP32 accumulation)."""
 
-    def __init__(self, problem: PoissonProblem, level: int | None = None):
+    def __init__(self, problem: PoissonProblem, level: int | None = None, tensor_cores: bool = False):
         self.problem = problem
         self.level = problem.n_levels - 1 if level is None else level
+        self.tensor_cores = tensor_cores
 
     def _sweep(self, dst, src, zero_init: bool, reverse: bool):
         p = self.problem
         dt = p._check_vec(dst, self.level)
         p._check_vec(src, self.level, dst.dtype)
+        if self.tensor_cores:
+            if dst.dtype != torch.float32:
+                raise TypeError("the tensor-core smoother works on float32 vectors")
+            dt = L.TPS_TF32
         L.check(L.lib().tps_smoother_step(p.handle, self.level, dt, dst.data_ptr(), src.data_ptr(),
                                           int(zero_init), int(reverse), _stream()), p.handle)
 

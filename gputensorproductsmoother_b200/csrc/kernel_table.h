@@ -30,6 +30,11 @@ struct SmootherMaps {
   alignas(64) unsigned char x[128];
   alignas(64) unsigned char b[128];
   int valid = 0;
+  // views for the tensor-core smoother (FP32): the x box in its K-major
+  // operand layout (rank 4) and the b interior (rank 3)
+  alignas(64) unsigned char tx[128];
+  alignas(64) unsigned char tb[128];
+  int tc_valid = 0;
 };
 
 struct KernelTable {
@@ -67,12 +72,25 @@ struct KernelTable {
                          cudaStream_t);
   cudaError_t (*cell_energy[2])(const LevelGeomH &, const VecLayout &, double *e, const double *u,
                                 const double *lam, cudaStream_t);
+  // 3D colour step on the tensor cores (FP32 vectors, TF32 operands, FP32
+  // accumulation); null for degree 1; needs maps->tc_valid
+  cudaError_t (*smoother_tc)(const LevelGeomH &, const VecLayout &, void *x, const void *b, int colour,
+                             double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t);
+  // the rank-4 TMA views of FP32 x and b (sets tc_valid when the layout allows them)
+  cudaError_t (*encode_tc_maps)(const VecLayout &l, void *x, const void *b, SmootherMaps *out);
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda
-// link dependency): rank-3 tiled map, no swizzle, zero out-of-bounds fill.
-cudaError_t encode_tiled_3d(void *map_out, bool f64, void *base, const uint64_t dims[3],
-                            const uint64_t strides_bytes[2], const uint32_t box[3]);
+// link dependency): tiled map of rank 3..5, no swizzle, zero out-of-bounds
+// fill; strides_bytes holds the rank-1 strides of dimensions 1.. (dimension
+// 0 is contiguous)
+cudaError_t encode_tiled(void *map_out, bool f64, void *base, int rank, const uint64_t *dims,
+                         const uint64_t *strides_bytes, const uint32_t *box);
+inline cudaError_t encode_tiled_3d(void *map_out, bool f64, void *base, const uint64_t dims[3],
+                                   const uint64_t strides_bytes[2], const uint32_t box[3])
+{
+  return encode_tiled(map_out, f64, base, 3, dims, strides_bytes, box);
+}
 
 const KernelTable *kernel_table(int degree);
 

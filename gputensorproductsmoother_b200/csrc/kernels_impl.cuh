@@ -10,6 +10,7 @@
 #include "laplace.cuh"
 #include "smoother.cuh"
 #include "smoother3d.cuh"
+#include "smoother3d_tc.cuh"
 #include "transfer.cuh"
 
 namespace tps {
@@ -100,6 +101,9 @@ cudaError_t set_attributes()
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetAll>), (restrict_smem<T>()));
   TPS_SET((kappa_smoother_kernel<2, K, T>), (sizeof(T) * KSm<2, K, T>::ELEMS));
   TPS_SET((kappa_smoother_kernel<3, K, T>), (sizeof(T) * KSm<3, K, T>::ELEMS));
+#if TPS_DEGREE >= 2
+  if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_tc_kernel<K>), (Tc3<K>::BYTES));
+#endif
 #undef TPS_SET
   return cudaSuccess;
 }
@@ -192,6 +196,88 @@ cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const voi
   }
   return cudaGetLastError();
 }
+
+#if TPS_DEGREE >= 2
+// persistent grid of the tensor-core smoother: CTAs resident per SM x SMs,
+// capped so that every CTA's TMEM allocation fits at once
+int tc_grid(int n_units)
+{
+  {
+    using C = Tc3<K>;
+    static int per_sm = -1, n_sm = 0;
+    if (per_sm < 0) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_tc_kernel<K>, C::NT, C::BYTES) !=
+              cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+      if (per_sm * C::TMEM_COLS > 512) per_sm = 512 / C::TMEM_COLS;
+    }
+    const int g = per_sm * n_sm;
+    return n_units < g ? n_units : g;
+  }
+}
+
+cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const void *b, int colour,
+                        double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t s)
+{
+  {
+    using C = Tc3<K>;
+    if (!maps || !maps->tc_valid) return cudaErrorInvalidValue;
+    int nx, ny, nz, count;
+    colour_lattice(3, g.n, colour, nx, ny, nz, count);
+    if (count == 0) return cudaSuccess;
+    const double sc = stiffness_scale(3, g.h);
+    Sm3Args a;
+    a.nx_c = nx;
+    a.ny_c = ny;
+    a.n_patches = count;
+    a.cx = colour & 1;
+    a.cy = (colour >> 1) & 1;
+    a.cz = (colour >> 2) & 1;
+    a.n_batches = count;
+    a.zero_x = zero_x;
+    a.sy = l.sy;
+    a.sz = l.sz;
+    smoother3d_tc_kernel<K><<<tc_grid(static_cast<int>(ceil_div(count, C::U))), C::NT, C::BYTES, s>>>(
+        *reinterpret_cast<const CUtensorMap *>(maps->tx), *reinterpret_cast<const CUtensorMap *>(maps->tb),
+        static_cast<float *>(x), a, static_cast<float>(sc), static_cast<float>(omega / sc), err);
+    return cudaGetLastError();
+  }
+}
+
+cudaError_t encode_tc_maps(const VecLayout &l, void *x, const void *b, SmootherMaps *out)
+{
+  out->tc_valid = 0;
+  {
+    using C = Tc3<K>;
+    if ((l.sy * 4) % 16 || (l.sz * 4) % 16 || reinterpret_cast<uintptr_t>(x) % 16 ||
+        reinterpret_cast<uintptr_t>(b) % 16)
+      return cudaSuccess;
+    const uint64_t N = static_cast<uint64_t>(l.N1), NC = (N + 3) / 4;
+    const uint64_t sy = static_cast<uint64_t>(l.sy) * 4, sz = static_cast<uint64_t>(l.sz) * 4;
+    // x: (x%4, y, x/4, z), 8 rows of y per load -> [z][x/4][y%8][x%4] (K-major, K = x)
+    const uint64_t dx[4] = {4, N, NC, N}, stx[3] = {sy, 16, sz};
+    const uint32_t bx[4] = {4, 8, static_cast<uint32_t>(C::XC), static_cast<uint32_t>(C::N1)};
+    // b: plain [z][y][x] box of the patch interior (x from the aligned box start)
+    const uint64_t db[3] = {N, N, N}, stb[2] = {sy, sz};
+    const uint32_t bb[3] = {static_cast<uint32_t>(C::XW), static_cast<uint32_t>(C::M), static_cast<uint32_t>(C::M)};
+    cudaError_t e = encode_tiled(out->tx, false, x, 4, dx, stx, bx);
+    if (e == cudaSuccess) e = encode_tiled(out->tb, false, const_cast<void *>(b), 3, db, stb, bb);
+    if (e == cudaSuccess) out->tc_valid = 1;
+    return e;
+  }
+}
+
+#else
+cudaError_t encode_tc_maps(const VecLayout &, void *, const void *, SmootherMaps *out)
+{
+  out->tc_valid = 0;
+  return cudaSuccess;
+}
+#endif
 
 template <typename T>
 cudaError_t encode_maps(const VecLayout &l, void *x, const void *b, SmootherMaps *out)
@@ -368,6 +454,12 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
      {&deg_impl::kappa_smoother<3, double>, &deg_impl::kappa_smoother<3, float>}},
     {&deg_impl::mass<2>, &deg_impl::mass<3>},
     {&deg_impl::cell_energy<2>, &deg_impl::cell_energy<3>},
+#if TPS_DEGREE >= 2
+    &deg_impl::smoother_tc,
+#else
+    nullptr,
+#endif
+    &deg_impl::encode_tc_maps,
 };
 
 }  // namespace tps

@@ -33,20 +33,26 @@ EncodeFn encode_fn(cudaError_t &err)
 
 }  // namespace
 
-cudaError_t encode_tiled_3d(void *map_out, bool f64, void *base, const uint64_t dims[3],
-                            const uint64_t strides_bytes[2], const uint32_t box[3])
+cudaError_t encode_tiled(void *map_out, bool f64, void *base, int rank, const uint64_t *dims,
+                         const uint64_t *strides_bytes, const uint32_t *box)
 {
+  if (rank < 3 || rank > 5) return cudaErrorInvalidValue;
   cudaError_t e;
   EncodeFn fn = encode_fn(e);
   if (!fn) return e == cudaSuccess ? cudaErrorNotSupported : e;
-  const cuuint64_t gdim[3] = {dims[0], dims[1], dims[2]};
-  const cuuint64_t gstr[2] = {strides_bytes[0], strides_bytes[1]};
-  const cuuint32_t bdim[3] = {box[0], box[1], box[2]};
-  const cuuint32_t estr[3] = {1, 1, 1};
+  cuuint64_t gdim[5], gstr[4];
+  cuuint32_t bdim[5], estr[5];
+  for (int i = 0; i < rank; ++i) {
+    gdim[i] = dims[i];
+    bdim[i] = box[i];
+    estr[i] = 1;
+    if (i + 1 < rank) gstr[i] = strides_bytes[i];
+  }
   CUresult r = fn(reinterpret_cast<CUtensorMap *>(map_out),
-                  f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base,
-                  gdim, gstr, bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                  CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                  f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                  static_cast<cuuint32_t>(rank), base, gdim, gstr, bdim, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 

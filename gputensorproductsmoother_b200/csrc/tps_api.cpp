@@ -321,6 +321,8 @@ VcycleVectors &vcycle_vectors(tps_handle *h, int p)
     }
     if (h->dim == 3)
       TPS_CUDA(h->kt->encode_maps[p](lay, V.su[l]->p, V.d[l]->p, &V.maps[l]));
+    if (h->dim == 3 && p == 1)
+      TPS_CUDA(h->kt->encode_tc_maps(lay, V.su[l]->p, V.d[l]->p, &V.maps[l]));
   }
   if (h->dense_coarse) {
     const VecLayout &lc = V.layout[0];
@@ -348,10 +350,14 @@ VcycleVectors &vcycle_vectors(tps_handle *h, int p)
 }
 
 // one coloured sweep; x_zero declares x == 0 on entry (the first colour then
-// skips reading x); maps (may be null) select the TMA path
+// skips reading x); maps (may be null) select the TMA path; tc selects the
+// tensor-core kernel (3D, FP32 vectors, constant coefficient, TMA views)
 void smoother_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void *x, const void *b,
-                    bool reverse, bool x_zero, const SmootherMaps *maps, cudaStream_t s)
+                    bool reverse, bool x_zero, const SmootherMaps *maps, cudaStream_t s,
+                    bool tc = false)
 {
+  const bool use_tc = tc && p == 1 && h->dim == 3 && !h->has_kappa && maps && maps->tc_valid &&
+                      h->kt->smoother_tc;
   if (!h->err_flag.p) h->err_flag.alloc(sizeof(int));
   const int nc = 1 << h->dim;
   for (int i = 0; i < nc; ++i) {
@@ -359,6 +365,9 @@ void smoother_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void 
     if (h->has_kappa)
       TPS_CUDA(h->kt->kappa_smoother[h->dim - 2][p](h->lv[level], lay, x, b,
                                                     h->kappa_dev[p][level]->p, c, h->omega, s));
+    else if (use_tc)
+      TPS_CUDA(h->kt->smoother_tc(h->lv[level], lay, x, b, c, h->omega, (x_zero && i == 0) ? 1 : 0, maps,
+                                  h->err_flag.as<int>(), s));
     else
       TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], lay, x, b, c, h->omega,
                                               (x_zero && i == 0) ? 1 : 0, maps,
@@ -420,7 +429,7 @@ void set_kappa_levels(tps_handle *h, const double *kappa_fine)
   }
 }
 
-void coarse_solve(tps_handle *h, int p, cudaStream_t s)
+void coarse_solve(tps_handle *h, int p, cudaStream_t s, bool tc)
 {
   VcycleVectors &V = h->vc[p];
   const size_t es = p == 0 ? sizeof(double) : sizeof(float);
@@ -428,7 +437,7 @@ void coarse_solve(tps_handle *h, int p, cudaStream_t s)
   TPS_CUDA(cudaMemsetAsync(V.su[0]->p, 0, es * V.su[0]->bytes / es, s));
   if (!h->dense_coarse) {
     // one vertex patch covers every interior DoF: the smoother is an exact solve
-    smoother_sweep(h, 0, p, lay, V.su[0]->p, V.d[0]->p, false, true, &V.maps[0], s);
+    smoother_sweep(h, 0, p, lay, V.su[0]->p, V.d[0]->p, false, true, &V.maps[0], s, tc);
   } else {
     TPS_CUDA(launch_coarse_dense(V.coarse_inv.p, V.coarse_idx.as<int>(), h->n_int_coarse,
                                  V.su[0]->p, V.d[0]->p, static_cast<int>(es), s));
@@ -436,35 +445,37 @@ void coarse_solve(tps_handle *h, int p, cudaStream_t s)
 }
 
 // MultigridSolvers::v_cycle (include/solver.cuh:1952-2001) on precision p:
-// input d[level], output su[level]
-void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s)
+// input d[level], output su[level]; tc: FP32 3D sweeps on the tensor cores
+void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s, bool tc)
 {
   VcycleVectors &V = h->vc[p];
   if (level == 0) {
-    coarse_solve(h, p, s);
+    coarse_solve(h, p, s, tc);
     return;
   }
   const LevelGeomH &g = h->lv[level];
   const VecLayout &lay = V.layout[level], &lc = V.layout[level - 1];
   const int di = h->dim - 2;
   TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, V.su[level]->bytes, s));
-  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, true, &V.maps[level], s);
+  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, true, &V.maps[level], s, tc);
   level_laplace(h, level, p, lay, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s);
   TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], lc, lay, V.d[level - 1]->p, V.t[level]->p,
                                    V.tmp[level]->p, 0, s));
-  vcycle_rec(h, level - 1, p, symmetric, s);
+  vcycle_rec(h, level - 1, p, symmetric, s, tc);
   TPS_CUDA(h->kt->prolong[di][p](h->lv[level - 1], lc, lay, V.su[level]->p, V.su[level - 1]->p,
                                  V.tmp[level]->p, s));
   smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, symmetric, false,
-                 &V.maps[level], s);
+                 &V.maps[level], s, tc);
 }
 
 int vprec_index(int precision)
 {
-  if (precision < 0 || precision > 2) throw ApiError(TPS_ERR_INVALID, "bad V-cycle precision");
-  return precision == TPS_VCYCLE_F32 ? 1 : 0;
+  if (precision < 0 || precision > 3) throw ApiError(TPS_ERR_INVALID, "bad V-cycle precision");
+  return precision == TPS_VCYCLE_F32 || precision == TPS_VCYCLE_TF32 ? 1 : 0;
 }
-int input_kind(int precision) { return precision; }  // 0 f64, 1 f32, 2 f64-rounded
+// conversion of the FP64 input into the V-cycle vectors: 0 f64, 1 f32, 2 f64-rounded
+int input_kind(int precision) { return precision == TPS_VCYCLE_TF32 ? 1 : precision; }
+bool vprec_tc(int precision) { return precision == TPS_VCYCLE_TF32; }
 
 PadMap fine_padmap(tps_handle *h, int p)
 {
@@ -508,7 +519,7 @@ void cg_iteration_body(tps_handle *h, int prec, bool symmetric, double *x, cudaS
   const int zk = p == 1 ? 1 : 0;
   const PadMap pm = fine_padmap(h, p);
   const VecLayout lex = lex_layout(h, L);
-  vcycle_rec(h, L, p, symmetric, s);
+  vcycle_rec(h, L, p, symmetric, s, vprec_tc(prec));
   TPS_CUDA(launch_cg_beta(V.su[L]->p, zk, pm, h->q.as<double>(), h->r.as<double>(), N, part, sc, s));
   TPS_CUDA(launch_cg_update_p(h->p.as<double>(), V.su[L]->p, zk, pm, N, sc, s));
   level_laplace(h, L, 0, lex, h->q.p, h->p.p, nullptr, 0, s);
@@ -560,7 +571,7 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
   bool converged = res <= o.rel_tol;
   if (!converged && status == TPS_OK) {
     // first direction: z = V(r), p = z, rz; then q, alpha, x/r update
-    vcycle_rec(h, L, p, sym, s);
+    vcycle_rec(h, L, p, sym, s, vprec_tc(o.precision));
     TPS_CUDA(launch_cg_first_direction(h->p.as<double>(), V.su[L]->p, zk, pm, h->r.as<double>(), N,
                                        part, s));
     TPS_CUDA(launch_cg_finalize_rz(part, sc, s));
@@ -655,8 +666,35 @@ void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, c
   const int64_t N = h->fine().N;
   const PadMap pm = fine_padmap(h, p);
   TPS_CUDA(launch_to_vcycle(V.d[L]->p, input_kind(precision), pm, src, N, s));
-  vcycle_rec(h, L, p, symmetric, s);
+  vcycle_rec(h, L, p, symmetric, s, vprec_tc(precision));
   TPS_CUDA(launch_from_vcycle(dst, V.su[L]->p, p == 1 ? 1 : 0, pm, N, s));
+}
+
+// the tensor-core smoother exists for 3D, degree >= 2, constant coefficient
+void check_tc(tps_handle *h)
+{
+  if (h->dim != 3 || !h->kt->smoother_tc || h->has_kappa)
+    throw ApiError(TPS_ERR_UNSUPPORTED, "the tensor-core (TF32) smoother needs 3D, degree >= 2 and no kappa");
+}
+
+// tps_smoother_step with TPS_TF32 on caller vectors (FP32, lexicographic):
+// the sweep runs on the padded, TMA-addressable V-cycle vectors of the level
+void tc_smoother_step(tps_handle *h, int level, void *x, const void *b, bool zero_init, bool reverse,
+                      cudaStream_t s)
+{
+  check_tc(h);
+  VcycleVectors &V = vcycle_vectors(h, 1);
+  const VecLayout &l = V.layout[level];
+  const size_t row = sizeof(float) * l.N1, pitch = sizeof(float) * l.sy;
+  const size_t rows = static_cast<size_t>(l.N1) * l.N1;
+  void *px = V.su[level]->p, *pb = V.d[level]->p;
+  if (zero_init)
+    TPS_CUDA(cudaMemsetAsync(px, 0, V.su[level]->bytes, s));
+  else
+    TPS_CUDA(cudaMemcpy2DAsync(px, pitch, x, row, row, rows, cudaMemcpyDeviceToDevice, s));
+  TPS_CUDA(cudaMemcpy2DAsync(pb, pitch, b, row, row, rows, cudaMemcpyDeviceToDevice, s));
+  smoother_sweep(h, level, 1, l, px, pb, reverse, zero_init, &V.maps[level], s, true);
+  TPS_CUDA(cudaMemcpy2DAsync(x, row, px, pitch, row, rows, cudaMemcpyDeviceToDevice, s));
 }
 
 // deal.II SolverGMRES semantics (left preconditioning, MGS, Givens) as used by
@@ -885,11 +923,15 @@ int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *
 {
   return guarded(h, [&] {
     check_level(h, level);
-    const int p = dt_index(dtype);
     if (!x || !b) throw ApiError(TPS_ERR_INVALID, "null vector");
     if (x == b) throw ApiError(TPS_ERR_INVALID, "x and b must not alias");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const LevelGeomH &g = h->lv[level];
+    if (dtype == TPS_TF32) {
+      tc_smoother_step(h, level, x, b, zero_init != 0, reverse != 0, s);
+      return;
+    }
+    const int p = dt_index(dtype);
     if (zero_init) TPS_CUDA(cudaMemsetAsync(x, 0, (p == 0 ? 8 : 4) * g.N, s));
     smoother_sweep(h, level, p, lex_layout(h, level), x, b, reverse != 0, zero_init != 0, nullptr, s);
   });
@@ -1010,7 +1052,9 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
 {
   return guarded(h, [&] {
     check_level(h, level);
-    const int p = dt_index(dtype);
+    const bool tc = dtype == TPS_TF32;
+    if (tc) check_tc(h);
+    const int p = tc ? 1 : dt_index(dtype);
     if (sweeps < 1 || !ms_per_sweep) throw ApiError(TPS_ERR_INVALID, "sweeps >= 1 and an output are required");
     ensure_krylov(h);
     VcycleVectors &V = vcycle_vectors(h, p);
@@ -1018,7 +1062,7 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
     TPS_CUDA(cudaEventRecord(h->ev0, s));
     for (int i = 0; i < sweeps; ++i)
       smoother_sweep(h, level, p, V.layout[level], V.su[level]->p, V.d[level]->p, false, false,
-                     &V.maps[level], s);
+                     &V.maps[level], s, tc);
     TPS_CUDA(cudaEventRecord(h->ev1, s));
     TPS_CUDA(cudaEventSynchronize(h->ev1));
     float ms = 0.f;

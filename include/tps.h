@@ -31,7 +31,13 @@ typedef enum {
   TPS_ERR_UNSUPPORTED = 7   /* degree/dimension not compiled in */
 } tps_status;
 
-typedef enum { TPS_F64 = 0, TPS_F32 = 1 } tps_dtype;
+typedef enum {
+  TPS_F64 = 0,
+  TPS_F32 = 1,
+  TPS_TF32 = 2 /* FP32 vectors; the 3D patch solves run on the tensor cores (TF32
+                  operands, FP32 accumulation).  tps_smoother_step and
+                  tps_time_smoother only. */
+} tps_dtype;
 
 typedef struct tps_handle tps_handle;
 
@@ -85,8 +91,10 @@ int tps_restrict_add(tps_handle *h, int from_level, int dtype, void *coarse, con
 typedef enum {
   TPS_VCYCLE_F64 = 0,        /* FP64 V-cycle */
   TPS_VCYCLE_F32 = 1,        /* FP32 smoother/operator/transfer inside the V-cycle */
-  TPS_VCYCLE_F64_ROUNDED = 2 /* FP64 V-cycle fed with FP32-rounded input: the
+  TPS_VCYCLE_F64_ROUNDED = 2, /* FP64 V-cycle fed with FP32-rounded input: the
                                 reference's "double" V-cycle (include/solver.cuh:64-78) */
+  TPS_VCYCLE_TF32 = 3         /* as TPS_VCYCLE_F32, with the 3D patch solves on the tensor
+                                cores (TF32 operands, FP32 accumulation) */
 } tps_vcycle_precision;
 
 /* MultigridSolvers::vmult (include/solver.cuh:1915-1930): dst = V-cycle(src) on the
