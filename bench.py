@@ -41,9 +41,11 @@ def parse():
     ap.add_argument("--workload", default="poisson3d_q4_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--mode", default="solve", choices=["solve", "smoother", "operator"],
-                    help="smoother / operator: only time the finest-level FP32 smoother "
+                    help="smoother / operator: only time the finest-level smoother "
                          "sweeps / FP64 operator applications (small commands for kernel "
                          "profiling)")
+    ap.add_argument("--smoother", default="fp32", choices=["fp32", "tf32", "fp64"],
+                    help="--mode smoother: FP32 SIMT kernel, tensor-core (TF32) kernel or FP64")
     return ap.parse_args()
 
 
@@ -74,8 +76,8 @@ def run_operator_only(args):
 
 
 def run_smoother_only(args):
-    """Times --steps sweeps of the finest-level FP32 smoother (8 colour launches
-    each) after --warmup sweeps and prints one JSON line."""
+    """Times --steps sweeps of the finest-level smoother (8 colour launches
+    each, --smoother precision) after --warmup sweeps and prints one JSON line."""
     import torch
     import gputensorproductsmoother_b200 as tps
     from gputensorproductsmoother_b200 import _lib as L
@@ -86,14 +88,14 @@ def run_smoother_only(args):
     stream = torch.cuda.Stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
     ms = ctypes.c_double()
+    code = {"fp32": L.TPS_F32, "tf32": L.TPS_TF32, "fp64": L.TPS_F64}[args.smoother]
     if args.warmup > 0:
-        L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, args.warmup, ctypes.byref(ms), sp),
-                P.handle)
-    L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, max(args.steps, 1), ctypes.byref(ms), sp),
-            P.handle)
-    total, per = smoother_bytes(dim, k, n, 4)
-    print(json.dumps({"mode": "smoother", "workload": args.workload, "ms_per_sweep": ms.value,
-                      "algorithmic_GBps": total / (ms.value * 1e-3) / 1e9}), flush=True)
+        L.check(L.lib().tps_time_smoother(P.handle, lf, code, args.warmup, ctypes.byref(ms), sp), P.handle)
+    L.check(L.lib().tps_time_smoother(P.handle, lf, code, max(args.steps, 1), ctypes.byref(ms), sp), P.handle)
+    total, per = smoother_bytes(dim, k, n, 8 if args.smoother == "fp64" else 4)
+    print(json.dumps({"mode": "smoother", "smoother": args.smoother, "workload": args.workload,
+                      "ms_per_sweep": ms.value, "algorithmic_GBps": total / (ms.value * 1e-3) / 1e9}),
+          flush=True)
     P.close()
 
 
