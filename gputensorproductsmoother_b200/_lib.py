@@ -75,6 +75,12 @@ SIGNATURES = [
     ("tps_cell_energy", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     ("tps_restrict_add_noalloc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, _VP, _VP, _VP]),
+    ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
+    ("tps_batch_destroy", ctypes.c_int, [_VP]),
+    ("tps_batch_last_error", ctypes.c_char_p, [_VP]),
+    ("tps_batch_system", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(_VP)]),
+    ("tps_batch_solve", ctypes.c_int, [_VP, ctypes.POINTER(TpsSolveOpts), ctypes.POINTER(_VP),
+                                       ctypes.POINTER(_VP), ctypes.POINTER(TpsReport), _VP]),
 ]
 
 

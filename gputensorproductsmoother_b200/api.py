@@ -312,3 +312,74 @@ class MultigridSolvers:
         (non-convergence is reported, not raised, like the reference)."""
         return self._solve(L.DRIVER_GMRES, b, x, precision, False, max_iter, reduce, abs_tol,
                            False, raise_on_fail)
+
+
+class BatchSolver:
+    """Many independent Poisson systems solved together by one CUDA graph
+    launch (tps_batch_*): right-hand sides of one mesh and/or meshes of
+    different sizes.  ``systems`` is a list of (dim, degree, n_cells) or
+    (dim, degree, n_cells, n_coarse) tuples, one per system."""
+
+    def __init__(self, systems, relaxation: float = 1.0, device: int | None = None):
+        dev = torch.cuda.current_device() if device is None else device
+        self.shapes = []
+        arr = (L.TpsProblem * len(systems))()
+        for i, sysdef in enumerate(systems):
+            dim, degree, n_cells = sysdef[:3]
+            if len(sysdef) > 3:
+                n_coarse = sysdef[3]
+                q, n_levels = n_cells // n_coarse, 1
+                while q > 1:
+                    q //= 2
+                    n_levels += 1
+            else:
+                n_coarse, n_levels = split_cells(n_cells)
+            arr[i] = L.TpsProblem(dim, degree, n_coarse, n_levels, relaxation, None, dev)
+            self.shapes.append((dim, degree, n_cells))
+        h = ctypes.c_void_p()
+        st = L.lib().tps_batch_create(arr, len(systems), ctypes.byref(h))
+        if st != L.TPS_OK:
+            msg = L.lib().tps_batch_last_error(None)
+            raise L.TpsError(st, msg.decode() if msg else "")
+        self._h = h
+        self.device = dev
+
+    def __len__(self) -> int:
+        return len(self.shapes)
+
+    def n_dofs(self, i: int) -> int:
+        dim, degree, n = self.shapes[i]
+        return (n * degree + 1) ** dim
+
+    def solve(self, rhs, x=None, precision: str = "fp32", symmetric: bool = True, max_iter: int = 100,
+              rel_tol: float = 1e-10, raise_on_fail: bool = True):
+        """Solves every system; rhs (and x) are lists of CUDA float64 tensors.
+        Returns (x list, list of SolveReport)."""
+        n = len(self.shapes)
+        if len(rhs) != n:
+            raise ValueError(f"{n} right-hand sides are required")
+        for i, b in enumerate(rhs):
+            if not (b.is_cuda and b.dtype == torch.float64 and b.is_contiguous() and b.numel() == self.n_dofs(i)):
+                raise ValueError(f"rhs[{i}] must be a contiguous CUDA float64 tensor of {self.n_dofs(i)} entries")
+        xs = [torch.zeros_like(b) for b in rhs] if x is None else list(x)
+        bp = (ctypes.c_void_p * n)(*[b.data_ptr() for b in rhs])
+        xp = (ctypes.c_void_p * n)(*[v.data_ptr() for v in xs])
+        o = L.TpsSolveOpts(L.DRIVER_CG, _PRECISIONS[precision], int(symmetric), max_iter, rel_tol, 1e-300, 1)
+        reps = (L.TpsReport * n)()
+        st = L.lib().tps_batch_solve(self._h, ctypes.byref(o), bp, xp, reps, _stream())
+        if st != L.TPS_OK and (raise_on_fail or st != 4):
+            msg = L.lib().tps_batch_last_error(self._h)
+            raise L.TpsError(st, msg.decode() if msg else "")
+        return xs, [_report(reps[i]) for i in range(n)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            L.lib().tps_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

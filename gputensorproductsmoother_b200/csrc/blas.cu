@@ -445,4 +445,50 @@ cudaError_t launch_fill(void *dst, int elem_bytes, int64_t n, cudaStream_t s)
   return cudaMemsetAsync(dst, 0, static_cast<size_t>(n) * elem_bytes, s);
 }
 
+namespace {
+
+__global__ void batch_check_kernel(BatchLoop b, int first, cudaGraphConditionalHandle loop)
+{
+  __shared__ int any;
+  if (threadIdx.x == 0) any = 0;
+  __syncthreads();
+  for (int i = threadIdx.x; i < b.n; i += blockDim.x) {
+    const CGScalars &sc = *b.sc[i];
+    if (first) {
+      b.bnorm[i] = sc.bb > 0.0 ? sqrt(sc.bb) : 1.0;
+      b.iters[i] = 0;
+      b.active[i] = 1;
+    } else if (b.active[i]) {
+      b.iters[i] += 1;
+    }
+    if (b.active[i]) {
+      const double res = sqrt(sc.rr) / b.bnorm[i];
+      if (b.iters[i] < b.hist_len) b.hist[static_cast<int64_t>(i) * b.hist_len + b.iters[i]] = res;
+      b.active[i] = (sc.breakdown == 0 && isfinite(res) && res > b.rel_tol && b.iters[i] < b.max_iter) ? 1 : 0;
+    }
+    if (b.active[i]) atomicOr(&any, 1);
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) cudaGraphSetConditional(loop, any ? 1u : 0u);
+}
+
+__global__ void batch_select_kernel(const int *active, const __grid_constant__ BatchConds cond, int n)
+{
+  for (int i = threadIdx.x; i < n; i += blockDim.x) cudaGraphSetConditional(cond.h[i], active[i] ? 1u : 0u);
+}
+
+}  // namespace
+
+cudaError_t launch_batch_check(BatchLoop b, int first, cudaGraphConditionalHandle loop, cudaStream_t s)
+{
+  batch_check_kernel<<<1, 256, 0, s>>>(b, first, loop);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_select(const int *active, const BatchConds &cond, int n, cudaStream_t s)
+{
+  batch_select_kernel<<<1, 256, 0, s>>>(active, cond, n);
+  return cudaGetLastError();
+}
+
 }  // namespace tps

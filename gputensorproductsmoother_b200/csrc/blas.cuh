@@ -85,4 +85,27 @@ cudaError_t launch_from_vcycle(double *dst, const void *z, int z_kind, PadMap pm
                                cudaStream_t s);
 cudaError_t launch_fill(void *dst, int elem_bytes, int64_t n, cudaStream_t s);  // zero
 
+// --- batched solves: device-side control of one graph launch -------------
+// State of the batched CG loop (device memory, one entry per system).
+struct BatchLoop {
+  CGScalars *const *sc;  // per-system CG scalars
+  int *iters;            // iterations done
+  int *active;           // still iterating
+  double *bnorm;         // ||b|| (1 if b = 0)
+  double *hist;          // relative residual history, hist_len per system
+  int n, hist_len, max_iter;
+  double rel_tol;
+};
+// first = 1: after the initial residual (iteration 0); first = 0: after one
+// more iteration of every active system.  Updates the state and sets the
+// while-condition `loop` to "some system still active".
+cudaError_t launch_batch_check(BatchLoop b, int first, cudaGraphConditionalHandle loop, cudaStream_t s);
+// sets the if-condition of every system from its active flag (start of a loop
+// body); the handles are passed by value (kernel parameters), up to 256
+constexpr int kBatchMax = 256;
+struct BatchConds {
+  cudaGraphConditionalHandle h[kBatchMax];
+};
+cudaError_t launch_batch_select(const int *active, const BatchConds &cond, int n, cudaStream_t s);
+
 }  // namespace tps

@@ -16,6 +16,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -477,6 +478,14 @@ int vprec_index(int precision)
 int input_kind(int precision) { return precision == TPS_VCYCLE_TF32 ? 1 : precision; }
 bool vprec_tc(int precision) { return precision == TPS_VCYCLE_TF32; }
 
+// the tensor-core smoother exists for 3D, degree >= 2, constant coefficient
+void check_tc(tps_handle *h)
+{
+  if (h->dim != 3 || !h->kt->smoother_tc || h->has_kappa)
+    throw ApiError(TPS_ERR_UNSUPPORTED, "the tensor-core (TF32) smoother needs 3D, degree >= 2 and no kappa");
+}
+
+
 PadMap fine_padmap(tps_handle *h, int p)
 {
   const VecLayout &l = h->vc[p].layout.back();
@@ -539,6 +548,7 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
              cudaStream_t s)
 {
   const int p = vprec_index(o.precision);
+  if (vprec_tc(o.precision)) check_tc(h);
   vcycle_vectors(h, p);
   ensure_krylov(h);
   const int L = h->n_levels - 1;
@@ -661,6 +671,7 @@ void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, c
                     cudaStream_t s)
 {
   const int p = vprec_index(precision);
+  if (vprec_tc(precision)) check_tc(h);
   VcycleVectors &V = vcycle_vectors(h, p);
   const int L = h->n_levels - 1;
   const int64_t N = h->fine().N;
@@ -670,12 +681,6 @@ void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, c
   TPS_CUDA(launch_from_vcycle(dst, V.su[L]->p, p == 1 ? 1 : 0, pm, N, s));
 }
 
-// the tensor-core smoother exists for 3D, degree >= 2, constant coefficient
-void check_tc(tps_handle *h)
-{
-  if (h->dim != 3 || !h->kt->smoother_tc || h->has_kappa)
-    throw ApiError(TPS_ERR_UNSUPPORTED, "the tensor-core (TF32) smoother needs 3D, degree >= 2 and no kappa");
-}
 
 // tps_smoother_step with TPS_TF32 on caller vectors (FP32, lexicographic):
 // the sweep runs on the padded, TMA-addressable V-cycle vectors of the level
@@ -1102,6 +1107,340 @@ int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_ho
     }
   });
   return rc != TPS_OK ? rc : status;
+}
+
+}  // extern "C"
+
+// ---- batched solves ---------------------------------------------------------
+// n independent systems (own hierarchy and work vectors each) solved by one
+// CUDA graph: fork -> initial residual of every system -> join -> check ->
+// while (some system active) { select -> [if active_i: one CG iteration of
+// system i] on parallel branches -> check }.  The loop runs on the device;
+// the host waits once at the end.
+
+namespace {
+constexpr int kMaxBatch = kBatchMax;
+}  // namespace
+
+struct tps_batch {
+  std::vector<tps_handle *> sys;
+  int device = 0;
+  std::string err;
+  std::vector<cudaStream_t> fork, body;  // capture branches (init, loop body)
+  cudaStream_t aux = nullptr, own = nullptr;
+  std::vector<cudaEvent_t> ev;  // fork/join events
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  // what the instantiated graph was built for
+  int k_prec = -1, k_sym = -1, k_max = -1;
+  double k_tol = -1.0;
+  cudaStream_t k_stream = nullptr;
+  std::vector<const double *> k_b;
+  std::vector<double *> k_x;
+  DevBuf sc_ptrs, iters, active, bnorm, hist;
+
+  ~tps_batch()
+  {
+    if (exec) cudaGraphExecDestroy(exec);
+    for (cudaStream_t s : fork) cudaStreamDestroy(s);
+    for (cudaStream_t s : body) cudaStreamDestroy(s);
+    if (aux) cudaStreamDestroy(aux);
+    if (own) cudaStreamDestroy(own);
+    for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    if (t0) cudaEventDestroy(t0);
+    if (t1) cudaEventDestroy(t1);
+    for (tps_handle *h : sys) tps_destroy(h);
+  }
+};
+
+namespace tps {
+namespace {
+
+// x_b = b_b, r = b - A x, d = r in the V-cycle precision, rr and bb; p = q = 0
+// and zero scalars, so the first loop iteration is the first CG direction
+void batch_init_system(tps_handle *h, int prec, const double *b, double *x, cudaStream_t s)
+{
+  const int p = vprec_index(prec), L = h->n_levels - 1;
+  const int64_t N = h->fine().N;
+  VcycleVectors &V = h->vc[p];
+  CGScalars *sc = h->scalars.as<CGScalars>();
+  TPS_CUDA(cudaMemsetAsync(sc, 0, sizeof(CGScalars), s));
+  TPS_CUDA(cudaMemsetAsync(h->p.p, 0, sizeof(double) * N, s));
+  TPS_CUDA(cudaMemsetAsync(h->q.p, 0, sizeof(double) * N, s));
+  TPS_CUDA(cudaMemsetAsync(h->r.p, 0, sizeof(double) * N, s));
+  TPS_CUDA(launch_copy_boundary(x, b, h->dim, h->fine().N1, 8, s));
+  level_laplace(h, L, 0, lex_layout(h, L), h->r.p, x, b, 1, s);
+  TPS_CUDA(launch_cg_init(h->r.as<double>(), b, V.d[L]->p, input_kind(prec), fine_padmap(h, p), N,
+                          h->partial.as<double>(), s));
+  TPS_CUDA(launch_cg_finalize_init(h->partial.as<double>(), sc, s));
+}
+
+struct CaptureGuard {  // ends a capture left open by an exception
+  cudaStream_t s;
+  bool open = true;
+  ~CaptureGuard()
+  {
+    if (open) {
+      cudaGraph_t g = nullptr;
+      cudaStreamEndCapture(s, &g);
+      if (g) cudaGraphDestroy(g);
+    }
+  }
+};
+
+std::vector<cudaGraphNode_t> capture_deps(cudaStream_t s, cudaGraph_t *g)
+{
+  cudaStreamCaptureStatus st;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  TPS_CUDA(cudaStreamGetCaptureInfo(s, &st, nullptr, g, &deps, &nd));
+  if (st != cudaStreamCaptureStatusActive) throw ApiError(TPS_ERR_CUDA, "stream is not capturing");
+  return std::vector<cudaGraphNode_t>(deps, deps + nd);
+}
+
+void batch_build(tps_batch *B, const tps_solve_opts &o, const double *const *b, double *const *x, cudaStream_t s)
+{
+  const int n = static_cast<int>(B->sys.size());
+  const int p = vprec_index(o.precision);
+  const bool sym = o.symmetric != 0;
+  for (tps_handle *h : B->sys) {  // every allocation happens before the capture
+    vcycle_vectors(h, p);
+    ensure_krylov(h);
+  }
+  std::vector<CGScalars *> scp(n);
+  for (int i = 0; i < n; ++i) scp[i] = B->sys[i]->scalars.as<CGScalars>();
+  TPS_CUDA(cudaMemcpy(B->sc_ptrs.p, scp.data(), sizeof(CGScalars *) * n, cudaMemcpyHostToDevice));
+  BatchLoop bl{B->sc_ptrs.as<CGScalars *>(), B->iters.as<int>(), B->active.as<int>(), B->bnorm.as<double>(),
+               B->hist.as<double>(), n, TPS_MAX_HISTORY, o.max_iter, o.rel_tol};
+  if (B->exec) {
+    cudaGraphExecDestroy(B->exec);
+    B->exec = nullptr;
+  }
+  TPS_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  CaptureGuard top{s};
+  TPS_CUDA(cudaEventRecord(B->ev[n], s));
+  for (int i = 0; i < n; ++i) {
+    TPS_CUDA(cudaStreamWaitEvent(B->fork[i], B->ev[n], 0));
+    batch_init_system(B->sys[i], o.precision, b[i], x[i], B->fork[i]);
+    TPS_CUDA(cudaEventRecord(B->ev[i], B->fork[i]));
+    TPS_CUDA(cudaStreamWaitEvent(s, B->ev[i], 0));
+  }
+  cudaGraph_t cg = nullptr;
+  capture_deps(s, &cg);
+  cudaGraphConditionalHandle loop;
+  TPS_CUDA(cudaGraphConditionalHandleCreate(&loop, cg, 0, 0));
+  TPS_CUDA(launch_batch_check(bl, 1, loop, s));
+  std::vector<cudaGraphNode_t> deps = capture_deps(s, &cg);
+  cudaGraphNodeParams wp{};
+  wp.type = cudaGraphNodeTypeConditional;
+  wp.conditional.handle = loop;
+  wp.conditional.type = cudaGraphCondTypeWhile;
+  wp.conditional.size = 1;
+  cudaGraphNode_t wnode;
+  TPS_CUDA(cudaGraphAddNode(&wnode, cg, deps.data(), deps.size(), &wp));
+  cudaGraph_t bodyg = wp.conditional.phGraph_out[0];
+  {
+    TPS_CUDA(cudaStreamBeginCaptureToGraph(B->aux, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    CaptureGuard bg{B->aux};
+    BatchConds ca{};
+    for (int i = 0; i < n; ++i) TPS_CUDA(cudaGraphConditionalHandleCreate(&ca.h[i], bodyg, 0, 0));
+    TPS_CUDA(launch_batch_select(B->active.as<int>(), ca, n, B->aux));
+    cudaGraph_t bg_graph = nullptr;
+    std::vector<cudaGraphNode_t> sel = capture_deps(B->aux, &bg_graph);
+    std::vector<cudaGraphNode_t> ifn(n);
+    for (int i = 0; i < n; ++i) {
+      cudaGraphNodeParams ip{};
+      ip.type = cudaGraphNodeTypeConditional;
+      ip.conditional.handle = ca.h[i];
+      ip.conditional.type = cudaGraphCondTypeIf;
+      ip.conditional.size = 1;
+      TPS_CUDA(cudaGraphAddNode(&ifn[i], bg_graph, sel.data(), sel.size(), &ip));
+      TPS_CUDA(cudaStreamBeginCaptureToGraph(B->body[i], ip.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                             cudaStreamCaptureModeThreadLocal));
+      CaptureGuard ig{B->body[i]};
+      cg_iteration_body(B->sys[i], o.precision, sym, x[i], B->body[i]);
+      cudaGraph_t tmp = nullptr;
+      ig.open = false;
+      TPS_CUDA(cudaStreamEndCapture(B->body[i], &tmp));
+    }
+    TPS_CUDA(cudaStreamUpdateCaptureDependencies(B->aux, ifn.data(), ifn.size(), cudaStreamSetCaptureDependencies));
+    TPS_CUDA(launch_batch_check(bl, 0, loop, B->aux));
+    cudaGraph_t tmp = nullptr;
+    bg.open = false;
+    TPS_CUDA(cudaStreamEndCapture(B->aux, &tmp));
+  }
+  TPS_CUDA(cudaStreamUpdateCaptureDependencies(s, &wnode, 1, cudaStreamSetCaptureDependencies));
+  cudaGraph_t g = nullptr;
+  top.open = false;
+  TPS_CUDA(cudaStreamEndCapture(s, &g));
+  cudaError_t e = cudaGraphInstantiate(&B->exec, g, 0);
+  cudaGraphDestroy(g);
+  TPS_CUDA(e);
+  B->k_prec = o.precision;
+  B->k_sym = o.symmetric != 0;
+  B->k_max = o.max_iter;
+  B->k_tol = o.rel_tol;
+  B->k_stream = s;
+  B->k_b.assign(b, b + n);
+  B->k_x.assign(x, x + n);
+}
+
+template <typename F>
+int batch_guarded(tps_batch *B, F &&f)
+{
+  if (!B) return TPS_ERR_INVALID;
+  try {
+    cudaError_t e = cudaSetDevice(B->device);
+    if (e != cudaSuccess) throw ApiError(TPS_ERR_CUDA, cudaGetErrorString(e));
+    int st = f();
+    B->err.clear();
+    return st;
+  } catch (const ApiError &e) {
+    B->err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc &) {
+    B->err = "host allocation failed";
+    return TPS_ERR_ALLOC;
+  } catch (const std::exception &e) {
+    B->err = e.what();
+    return TPS_ERR_INVALID;
+  }
+}
+
+}  // namespace
+}  // namespace tps
+
+extern "C" {
+
+int tps_batch_create(const tps_problem *problems, int n_systems, tps_batch **out)
+{
+  if (!problems || !out || n_systems < 1 || n_systems > kMaxBatch) {
+    g_create_error = "tps_batch_create: 1..256 problems and an output pointer are required";
+    return TPS_ERR_INVALID;
+  }
+  *out = nullptr;
+  tps_batch *B = nullptr;
+  try {
+    B = new tps_batch;
+  } catch (const std::bad_alloc &) {
+    return TPS_ERR_ALLOC;
+  }
+  B->device = problems[0].device;
+  for (int i = 0; i < n_systems; ++i) {
+    if (problems[i].device != B->device) {
+      g_create_error = "tps_batch_create: all systems must be on one device";
+      delete B;
+      return TPS_ERR_INVALID;
+    }
+    tps_handle *h = nullptr;
+    const int st = tps_create(&problems[i], &h);
+    if (st != TPS_OK) {
+      delete B;
+      return st;
+    }
+    B->sys.push_back(h);
+  }
+  const int rc = batch_guarded(B, [&] {
+    const int n = n_systems;
+    B->fork.resize(n);
+    B->body.resize(n);
+    for (int i = 0; i < n; ++i) {
+      TPS_CUDA(cudaStreamCreateWithFlags(&B->fork[i], cudaStreamNonBlocking));
+      TPS_CUDA(cudaStreamCreateWithFlags(&B->body[i], cudaStreamNonBlocking));
+    }
+    TPS_CUDA(cudaStreamCreateWithFlags(&B->aux, cudaStreamNonBlocking));
+    B->ev.resize(n + 1);
+    for (auto &e : B->ev) TPS_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    TPS_CUDA(cudaEventCreate(&B->t0));
+    TPS_CUDA(cudaEventCreate(&B->t1));
+    B->sc_ptrs.alloc(sizeof(CGScalars *) * n);
+    B->iters.alloc(sizeof(int) * n);
+    B->active.alloc(sizeof(int) * n);
+    B->bnorm.alloc(sizeof(double) * n);
+    B->hist.alloc(sizeof(double) * n * TPS_MAX_HISTORY);
+    return TPS_OK;
+  });
+  if (rc != TPS_OK) {
+    g_create_error = B->err;
+    delete B;
+    return rc;
+  }
+  *out = B;
+  return TPS_OK;
+}
+
+int tps_batch_destroy(tps_batch *b)
+{
+  if (!b) return TPS_ERR_INVALID;
+  cudaSetDevice(b->device);
+  delete b;
+  return TPS_OK;
+}
+
+const char *tps_batch_last_error(const tps_batch *b) { return b ? b->err.c_str() : g_create_error.c_str(); }
+
+int tps_batch_system(tps_batch *b, int i, tps_handle **h)
+{
+  if (!b || !h || i < 0 || i >= static_cast<int>(b->sys.size())) return TPS_ERR_INVALID;
+  *h = b->sys[i];
+  return TPS_OK;
+}
+
+int tps_batch_solve(tps_batch *B, const tps_solve_opts *opts, const double *const *rhs, double *const *x,
+                    tps_report *reports, void *stream)
+{
+  return batch_guarded(B, [&]() -> int {
+    if (!opts || !rhs || !x || !reports) throw ApiError(TPS_ERR_INVALID, "null argument");
+    if (opts->driver != TPS_DRIVER_CG) throw ApiError(TPS_ERR_INVALID, "batched solves use the CG driver");
+    if (opts->max_iter < 1) throw ApiError(TPS_ERR_INVALID, "max_iter must be >= 1");
+    const int n = static_cast<int>(B->sys.size());
+    for (int i = 0; i < n; ++i) {
+      if (!rhs[i] || !x[i]) throw ApiError(TPS_ERR_INVALID, "null vector");
+      if (vprec_tc(opts->precision)) check_tc(B->sys[i]);
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (!s) {  // capture needs a non-default stream
+      if (!B->own) TPS_CUDA(cudaStreamCreateWithFlags(&B->own, cudaStreamNonBlocking));
+      s = B->own;
+    }
+    const bool same = B->exec && B->k_prec == opts->precision && B->k_sym == (opts->symmetric != 0) &&
+                      B->k_max == opts->max_iter && B->k_tol == opts->rel_tol && B->k_stream == s &&
+                      std::equal(B->k_b.begin(), B->k_b.end(), rhs) && std::equal(B->k_x.begin(), B->k_x.end(), x);
+    if (!same) batch_build(B, *opts, rhs, x, s);
+    TPS_CUDA(cudaEventRecord(B->t0, s));
+    TPS_CUDA(cudaGraphLaunch(B->exec, s));
+    TPS_CUDA(cudaEventRecord(B->t1, s));
+    TPS_CUDA(cudaEventSynchronize(B->t1));
+    float ms = 0.f;
+    TPS_CUDA(cudaEventElapsedTime(&ms, B->t0, B->t1));
+    std::vector<int> it(n), act(n);
+    std::vector<double> bn(n), hist(static_cast<size_t>(n) * TPS_MAX_HISTORY);
+    TPS_CUDA(cudaMemcpy(it.data(), B->iters.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    TPS_CUDA(cudaMemcpy(act.data(), B->active.p, sizeof(int) * n, cudaMemcpyDeviceToHost));
+    TPS_CUDA(cudaMemcpy(bn.data(), B->bnorm.p, sizeof(double) * n, cudaMemcpyDeviceToHost));
+    TPS_CUDA(cudaMemcpy(hist.data(), B->hist.p, sizeof(double) * hist.size(), cudaMemcpyDeviceToHost));
+    int status = TPS_OK;
+    for (int i = 0; i < n; ++i) {
+      CGScalars sc{};
+      TPS_CUDA(cudaMemcpy(&sc, B->sys[i]->scalars.p, sizeof(CGScalars), cudaMemcpyDeviceToHost));
+      tps_report &r = reports[i];
+      std::memset(&r, 0, sizeof(r));
+      const double *hi = hist.data() + static_cast<size_t>(i) * TPS_MAX_HISTORY;
+      const int nh = std::min(it[i] + 1, TPS_MAX_HISTORY);
+      for (int k = 0; k < nh; ++k) r.history[k] = hi[k];
+      r.iterations = it[i];
+      r.initial_residual = hi[0] * bn[i];
+      r.final_residual = std::sqrt(sc.rr) / bn[i];
+      r.converged = (sc.breakdown == 0 && r.final_residual <= opts->rel_tol) ? 1 : 0;
+      r.time_ms = ms;
+      int si = TPS_OK;
+      if (sc.breakdown) si = sc.breakdown == 2 ? TPS_ERR_NONFINITE : TPS_ERR_BREAKDOWN;
+      else if (!r.converged) si = TPS_ERR_NOT_CONVERGED;
+      if (si != TPS_OK && (status == TPS_OK || status == TPS_ERR_NOT_CONVERGED)) status = si;
+    }
+    (void)act;
+    return status;
+  });
 }
 
 }  // extern "C"

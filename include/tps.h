@@ -164,6 +164,29 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
                    double *x_host, tps_report *report);
 
+/* ---- batched solves (no reference counterpart) ----------------------------
+ * A batch owns n independent systems (1 <= n <= 256): right-hand sides of one
+ * mesh and/or meshes of different sizes; system i is built from problems[i]
+ * with its own hierarchy and work vectors.  tps_batch_solve runs the MG-CG of
+ * every system as ONE CUDA graph launch: the initial residuals on parallel
+ * branches, then a device-side while loop (a conditional graph node) whose body
+ * runs one CG iteration of every system that is still iterating (one
+ * conditional node per system, parallel branches) followed by a check kernel;
+ * the host waits once, when every system has converged or reached max_iter.
+ * The instantiated graph is reused while opts, stream and the vector pointers
+ * stay the same. */
+typedef struct tps_batch tps_batch;
+int tps_batch_create(const tps_problem *problems, int n_systems, tps_batch **out);
+int tps_batch_destroy(tps_batch *b);
+const char *tps_batch_last_error(const tps_batch *b);
+/* the handle of system i (owned by the batch): level operations, tps_level_info */
+int tps_batch_system(tps_batch *b, int i, tps_handle **h);
+/* rhs[i], x[i]: DEVICE FP64 vectors of system i (x[i] holds the initial guess);
+ * reports[i] per system (time_ms: the whole batch).  Driver must be TPS_DRIVER_CG;
+ * use_graph is implied.  Returns TPS_OK when every system converged. */
+int tps_batch_solve(tps_batch *b, const tps_solve_opts *opts, const double *const *rhs,
+                    double *const *x, tps_report *reports, void *stream);
+
 /* coarse += R fine, like tps_restrict_add, without a handle and without any
  * device allocation, for callers that must not allocate device memory (their
  * framework owns it all, e.g. a caching allocator or a pre-reserved arena).

@@ -1,0 +1,58 @@
+"""GPU tests of the batched solver (tps_batch_*): many right-hand sides and
+meshes of different sizes in one graph launch must give exactly the solves
+of the single-system driver (same iteration counts, same solutions)."""
+import numpy as np
+import pytest
+import torch
+
+import gputensorproductsmoother_b200 as tps
+
+pytestmark = pytest.mark.gpu
+
+
+def interior_random(dim, N1, seed):
+    rng = np.random.default_rng(seed)
+    v = rng.uniform(-1, 1, N1 ** dim)
+    idx = np.stack(np.unravel_index(np.arange(N1 ** dim), (N1,) * dim))
+    v[np.any((idx == 0) | (idx == N1 - 1), axis=0)] = 0.0
+    return torch.tensor(v, device="cuda")
+
+
+SYSTEMS = [(3, 3, 8)] * 3 + [(3, 3, 6), (3, 3, 12), (3, 2, 10), (2, 3, 16), (3, 4, 4)]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32", "tf32"])
+def test_batch_matches_single_solves(cuda, precision):
+    systems = SYSTEMS if precision != "tf32" else [s for s in SYSTEMS if s[0] == 3]
+    B = tps.BatchSolver(systems)
+    rhs = [interior_random(d, n * k + 1, 10 + i) for i, (d, k, n) in enumerate(systems)]
+    xs, reps = B.solve(rhs, precision=precision, rel_tol=1e-10)
+    for i, (d, k, n) in enumerate(systems):
+        P = tps.PoissonProblem(d, k, n)
+        x1, r1 = tps.MultigridSolvers(P).solve_cg(rhs[i], precision=precision, rel_tol=1e-10)
+        assert reps[i].converged and reps[i].final_residual <= 1e-10
+        assert reps[i].iterations == r1.iterations, (i, reps[i].iterations, r1.iterations)
+        np.testing.assert_allclose(reps[i].history, r1.history, rtol=1e-9, atol=0)
+        e = (xs[i] - x1).abs().max().item() / x1.abs().max().item()
+        assert e < 1e-12, (i, e)
+        P.close()
+    # a second launch reuses the instantiated graph and gives the same result
+    xs2, reps2 = B.solve(rhs, x=[torch.zeros_like(b) for b in rhs], precision=precision, rel_tol=1e-10)
+    for i in range(len(systems)):
+        assert reps2[i].iterations == reps[i].iterations
+        assert torch.equal(xs2[i], xs[i]) or (xs2[i] - xs[i]).abs().max().item() == 0.0
+    B.close()
+
+
+def test_batch_max_iter_and_zero_rhs(cuda):
+    systems = [(3, 3, 8), (3, 3, 8)]
+    B = tps.BatchSolver(systems)
+    rhs = [interior_random(3, 25, 1), torch.zeros(25 ** 3, dtype=torch.float64, device="cuda")]
+    xs, reps = B.solve(rhs, precision="fp32", rel_tol=1e-14, max_iter=2, raise_on_fail=False)
+    assert reps[0].iterations == 2 and not reps[0].converged
+    # b = 0: converged at iteration 0 with x = 0, never enters the loop body
+    assert reps[1].iterations == 0 and reps[1].converged
+    assert xs[1].abs().max().item() == 0.0
+    with pytest.raises(tps.TpsError):
+        B.solve(rhs, precision="fp32", rel_tol=1e-14, max_iter=2)
+    B.close()

@@ -58,7 +58,7 @@ def test_tc_vcycle_cg_reaches_fp64_solution(cuda, k, n):
     x64, r64 = MG.solve_cg(b, precision="fp64", rel_tol=1e-10)
     x32, r32 = MG.solve_cg(b, precision="fp32", rel_tol=1e-10)
     xtc, rtc = MG.solve_cg(b, precision="tf32", rel_tol=1e-10)
-    assert rtc.converged and rtc.final_residual <= 1e-10 * rtc.initial_residual
+    assert rtc.converged and rtc.final_residual <= 1e-10
     assert relerr(xtc.cpu().numpy(), x64.cpu().numpy()) < 1e-8
     # the TF32 V-cycle is a slightly weaker preconditioner than the FP32 one
     assert rtc.iterations <= r32.iterations + 2, (rtc.iterations, r32.iterations, r64.iterations)
