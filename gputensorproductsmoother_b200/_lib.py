@@ -75,6 +75,7 @@ SIGNATURES = [
     ("tps_cell_energy", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     ("tps_restrict_add_noalloc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, _VP, _VP, _VP]),
+    ("tps_autotune", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("tps_batch_destroy", ctypes.c_int, [_VP]),
     ("tps_batch_last_error", ctypes.c_char_p, [_VP]),

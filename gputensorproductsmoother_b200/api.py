@@ -103,6 +103,14 @@ class PoissonProblem:
                 self.handle)
         return ms.value
 
+    def autotune(self, dtype: str = "fp32") -> list[int]:
+        """Time the 3D smoother's patches-per-batch variants on every level and
+        keep the fastest; returns the chosen patches per batch per level."""
+        out = (ctypes.c_int * self.n_levels)()
+        L.check(L.lib().tps_autotune(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], out),
+                self.handle)
+        return list(out)
+
     def mass_vmult(self, dst: torch.Tensor, src: torch.Tensor) -> None:
         """dst = M src (finest level, all rows, FP64)."""
         lvl = self.n_levels - 1

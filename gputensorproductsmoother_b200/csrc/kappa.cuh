@@ -9,7 +9,11 @@
 //    fixed order (deterministic).
 //  * kappa_smoother_kernel: one patch per CTA, box residual b - A(kappa) x
 //    assembled cell by cell (the patch's 2^d cells), local solve by fast
-//    diagonalization of the unit-coefficient patch scaled by 1/mean(kappa),
+//    diagonalization of the unit-coefficient patch scaled by the
+//    patch-averaged coefficient per DoF, D^-1/2 FD^-1 D^-1/2 with D_i the
+//    mean kappa of the patch cells containing DoF i (exact on couplings
+//    inside one cell; one scalar mean per patch stagnates for strongly
+//    varying kappa),
 //    x_I <- x_I + omega * delta (the residual form is kept because the
 //    approximate local solve does not cancel x_I).
 //  * cell_energy_kernel: e_c = lambda_c^T (A_cell u_c) = int_c grad(lambda).grad(u)
@@ -282,13 +286,13 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
     R[l] = T(0);
   }
   __syncthreads();
-  T ksum = T(0);
+  T kpat[1 << DIM];
   for (int cc = 0; cc < (1 << DIM); ++cc) {
     const int ox = cc & 1, oy = (cc >> 1) & 1, oz = (cc >> 2) & 1;
     const int64_t cidx = int64_t(px + ox) + int64_t(py + oy) * n +
                          (DIM == 3 ? int64_t(pz + oz) * n * n : 0);
     const T kc = kappa[cidx];
-    ksum += kc;
+    kpat[cc] = kc;
     for (int l = threadIdx.x; l < S::CELL; l += NT) {
       const int lx = l % NP, ly = (l / NP) % NP, lz = DIM == 3 ? l / (NP * NP) : 0;
       cin[l] = X[(lx + ox * K) + (ly + oy * K) * N1 + (lz + oz * K) * N1 * N1];
@@ -301,11 +305,30 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
     }
     __syncthreads();
   }
-  const T kbar = ksum / T(1 << DIM);
-  // interior residual r = b_I - (A(kappa) x)_I into Q1 (lexicographic m^d)
+  // D^-1/2 of interior DoF l: mean kappa of the patch cells containing it
+  auto dinv_sqrt = [&](int l) -> T {
+    const int c3[3] = {l % M + 1, (l / M) % M + 1, DIM == 3 ? l / (M * M) + 1 : 0};
+    T acc = T(0);
+    int cnt = 0;
+#pragma unroll
+    for (int cc = 0; cc < (1 << DIM); ++cc) {
+      bool in = true;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const int o = (cc >> d) & 1;
+        in = in && !(o == 0 && c3[d] > K) && !(o == 1 && c3[d] < K);
+      }
+      if (in) {
+        acc += kpat[cc];
+        ++cnt;
+      }
+    }
+    return T(1) / sqrt(acc / T(cnt));
+  };
+  // interior residual r = D^-1/2 (b_I - (A(kappa) x)_I) into Q1 (lexicographic m^d)
   for (int l = threadIdx.x; l < S::INT; l += NT) {
     const int lx = l % M + 1, ly = (l / M) % M + 1, lz = DIM == 3 ? l / (M * M) + 1 : 0;
-    Q1[l] = b[first + lx + ly * sy + lz * sz] - R[lx + ly * N1 + lz * N1 * N1];
+    Q1[l] = (b[first + lx + ly * sy + lz * sz] - R[lx + ly * N1 + lz * N1 * N1]) * dinv_sqrt(l);
   }
   __syncthreads();
   // fast diagonalization: S^T along each direction, scale, S back (ping-pong Q1/Q2)
@@ -339,7 +362,7 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
           const int e = bidx + i * stride;
           const int mx = e % M, my = (e / M) % M, mz = DIM == 3 ? e / (M * M) : 0;
           const T lam = tb.eval[mx] + tb.eval[my] + (DIM == 3 ? tb.eval[mz] : T(0));
-          q[i] = q[i] * fd_scale / (lam * kbar);
+          q[i] = q[i] * fd_scale / lam;
         }
       }
 #pragma unroll
@@ -352,7 +375,7 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
   }
   for (int l = threadIdx.x; l < S::INT; l += NT) {
     const int lx = l % M + 1, ly = (l / M) % M + 1, lz = DIM == 3 ? l / (M * M) + 1 : 0;
-    x[first + lx + ly * sy + lz * sz] = omega * (X[lx + ly * N1 + lz * N1 * N1] + src[l]);
+    x[first + lx + ly * sy + lz * sz] = omega * (X[lx + ly * N1 + lz * N1 * N1] + src[l] * dinv_sqrt(l));
   }
 }
 

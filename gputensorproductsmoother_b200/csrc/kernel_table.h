@@ -37,6 +37,9 @@ struct SmootherMaps {
   int tc_valid = 0;
 };
 
+// compiled patches-per-batch variants of the 3D smoother (default, half, double)
+constexpr int kSmootherVariants = 3;
+
 struct KernelTable {
   int degree;
   // copy the 1D tables of this degree into constant memory of the current device
@@ -46,10 +49,12 @@ struct KernelTable {
   cudaError_t (*laplace[2][2])(const LevelGeomH &, const VecLayout &, void *dst, const void *src,
                                const void *rhs, int mode, cudaStream_t);
   // one colour of the patch sweep; maps (3D, TMA path) may be null; zero_x
-  // declares x == 0 on entry; err receives 1 if a bounded wait gave up
+  // declares x == 0 on entry; variant selects the 3D patches-per-batch
+  // (0 default, 1 half, 2 double; see smoother_ppb); err receives 1 if a
+  // bounded wait gave up
   cudaError_t (*smoother[2][2])(const LevelGeomH &, const VecLayout &, void *x, const void *b,
-                                int colour, double omega, int zero_x, const SmootherMaps *maps,
-                                int *err, cudaStream_t);
+                                int colour, double omega, int zero_x, int variant,
+                                const SmootherMaps *maps, int *err, cudaStream_t);
   // TMA descriptors of the 3D smoother for vectors x, b with layout l ([dtype])
   cudaError_t (*encode_maps[2])(const VecLayout &l, void *x, const void *b, SmootherMaps *out);
   // fine += P coarse (interior fine DoFs); geometry of the COARSE level
@@ -78,6 +83,8 @@ struct KernelTable {
                              double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t);
   // the rank-4 TMA views of FP32 x and b (sets tc_valid when the layout allows them)
   cudaError_t (*encode_tc_maps)(const VecLayout &l, void *x, const void *b, SmootherMaps *out);
+  // patches per CTA batch of smoother variant v (dtype 0 FP64, 1 FP32; 0 in 2D)
+  int (*smoother_ppb)(int dim, int dtype, int variant);
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda

@@ -90,8 +90,10 @@ cudaError_t set_attributes()
                            static_cast<int>(bytes));                                    \
   if (e != cudaSuccess) return e;
   TPS_SET((smoother_colour_kernel<2, K, T>), (smoother_smem<2, T>()));
-  TPS_SET((smoother3d_kernel<K, T, true>), (Sm3<K, T>::BYTES));
-  TPS_SET((smoother3d_kernel<K, T, false>), (Sm3<K, T>::BYTES));
+  TPS_SET((smoother3d_kernel<K, T, true, sm3_variant_ppb<K, T, 0>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 0>()>::BYTES));
+  TPS_SET((smoother3d_kernel<K, T, true, sm3_variant_ppb<K, T, 1>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 1>()>::BYTES));
+  TPS_SET((smoother3d_kernel<K, T, true, sm3_variant_ppb<K, T, 2>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 2>()>::BYTES));
+  TPS_SET((smoother3d_kernel<K, T, false, sm3_variant_ppb<K, T, 0>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 0>()>::BYTES));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Vmult>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Residual>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<3, K, T, OpMode::Vmult>), (laplace_smem<3, T>()));
@@ -135,7 +137,7 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
   return cudaGetLastError();
 }
 
-template <typename T, bool TMA>
+template <typename T, bool TMA, int PPB>
 int sm3_grid(int n_batches)
 {
   static int per_sm = -1, n_sm = 0;
@@ -143,8 +145,8 @@ int sm3_grid(int n_batches)
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_kernel<K, T, TMA>,
-                                                      Sm3<K, T>::NT, Sm3<K, T>::BYTES) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_kernel<K, T, TMA, PPB>,
+                                                      Sm3<K, T, PPB>::NT, Sm3<K, T, PPB>::BYTES) != cudaSuccess ||
         per_sm < 1)
       per_sm = 1;
   }
@@ -152,9 +154,43 @@ int sm3_grid(int n_batches)
   return n_batches < g ? n_batches : g;
 }
 
+// one colour of the 3D sweep with PPB patches per CTA batch (the plain-load
+// variant, for vectors without TMA views, always uses the default batch)
+template <typename T, int PPB>
+void smoother3d_launch(Sm3Args a, const SmootherMaps *maps, void *x, const void *b, T scale, T fd, int *err,
+                       cudaStream_t s)
+{
+  if (maps && maps->valid) {
+    using S = Sm3<K, T, PPB>;
+    a.n_batches = static_cast<int>(ceil_div(a.n_patches, S::PPB));
+    smoother3d_kernel<K, T, true, PPB><<<sm3_grid<T, true, PPB>(a.n_batches), S::NT, S::BYTES, s>>>(
+        *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),
+        static_cast<T *>(x), static_cast<const T *>(b), a, scale, fd, err);
+  } else {
+    constexpr int P0 = sm3_variant_ppb<K, T, 0>();
+    using S = Sm3<K, T, P0>;
+    a.n_batches = static_cast<int>(ceil_div(a.n_patches, S::PPB));
+    CUtensorMap none{};
+    smoother3d_kernel<K, T, false, P0><<<a.n_batches, S::NT, S::BYTES, s>>>(
+        none, none, static_cast<T *>(x), static_cast<const T *>(b), a, scale, fd, err);
+  }
+}
+
+// patches per batch of a 3D variant (0 in 2D: one fixed kernel shape)
+int smoother_ppb(int dim, int dtype, int variant)
+{
+  if (dim != 3) return 0;
+  auto pick = [&](auto tag) -> int {
+    using T = decltype(tag);
+    return variant == 1 ? sm3_variant_ppb<K, T, 1>() : variant == 2 ? sm3_variant_ppb<K, T, 2>()
+                                                                        : sm3_variant_ppb<K, T, 0>();
+  };
+  return dtype == 0 ? pick(double{}) : pick(float{});
+}
+
 template <int DIM, typename T>
 cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const void *b, int colour,
-                     double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t s)
+                     double omega, int zero_x, int variant, const SmootherMaps *maps, int *err, cudaStream_t s)
 {
   int nx, ny, nz, count;
   colour_lattice(DIM, g.n, colour, nx, ny, nz, count);
@@ -170,7 +206,6 @@ cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const voi
         static_cast<T *>(x), static_cast<const T *>(b), l.sy, l.sz, nx, ny, count, cx, cy, cz,
         static_cast<T>(sc), static_cast<T>(1.0 / sc), static_cast<T>(omega));
   } else {
-    using S = Sm3<K, T>;
     Sm3Args a;
     a.nx_c = nx;
     a.ny_c = ny;
@@ -178,21 +213,16 @@ cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const voi
     a.cx = cx;
     a.cy = cy;
     a.cz = cz;
-    a.n_batches = static_cast<int>(ceil_div(count, S::PPB));
     a.zero_x = zero_x;
     a.sy = l.sy;
     a.sz = l.sz;
     const T scale = static_cast<T>(sc), fd = static_cast<T>(omega / sc);
-    if (maps && maps->valid) {
-      smoother3d_kernel<K, T, true><<<sm3_grid<T, true>(a.n_batches), S::NT, S::BYTES, s>>>(
-          *reinterpret_cast<const CUtensorMap *>(maps->x),
-          *reinterpret_cast<const CUtensorMap *>(maps->b), static_cast<T *>(x),
-          static_cast<const T *>(b), a, scale, fd, err);
-    } else {
-      CUtensorMap none{};
-      smoother3d_kernel<K, T, false><<<a.n_batches, S::NT, S::BYTES, s>>>(
-          none, none, static_cast<T *>(x), static_cast<const T *>(b), a, scale, fd, err);
-    }
+    if (variant == 1)
+      smoother3d_launch<T, sm3_variant_ppb<K, T, 1>()>(a, maps, x, b, scale, fd, err, s);
+    else if (variant == 2)
+      smoother3d_launch<T, sm3_variant_ppb<K, T, 2>()>(a, maps, x, b, scale, fd, err, s);
+    else
+      smoother3d_launch<T, sm3_variant_ppb<K, T, 0>()>(a, maps, x, b, scale, fd, err, s);
   }
   return cudaGetLastError();
 }
@@ -460,6 +490,7 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
     nullptr,
 #endif
     &deg_impl::encode_tc_maps,
+    &deg_impl::smoother_ppb,
 };
 
 }  // namespace tps

@@ -40,7 +40,15 @@
 
 namespace tps {
 
+// default patches per CTA batch: enough lines per stage, two to three CTAs per SM
 template <int K, typename T>
+constexpr int sm3_default_ppb()
+{
+  return sizeof(T) == 4 ? (K == 1 ? 32 : K == 2 ? 16 : K == 3 ? 8 : K == 4 ? 4 : K <= 6 ? 2 : 1)
+                        : (K == 1 ? 16 : K == 2 ? 8 : K == 3 ? 4 : K == 4 ? 2 : 1);
+}
+
+template <int K, typename T, int PPB_ = 0>
 struct Sm3 {
   static constexpr int N1 = 2 * K + 1, M = 2 * K - 1;
   static constexpr int A = 16 / static_cast<int>(sizeof(T));  // TMA x-alignment (elements)
@@ -57,9 +65,8 @@ struct Sm3 {
   static constexpr int STAGE = (BOFF + BBOX + ALIGN - 1) / ALIGN * ALIGN;  // per patch
   static constexpr int RING = N1 * N1 - M * M;  // boundary lines of a z-face
   static constexpr int IPAIR = (M * M + 1) / 2;  // interior z-lines, two per task
-  // patches per batch: enough lines per stage, two to three CTAs per SM
-  static constexpr int PPB = sizeof(T) == 4 ? (K == 1 ? 32 : K == 2 ? 16 : K == 3 ? 8 : K == 4 ? 4 : K <= 6 ? 2 : 1)
-                                            : (K == 1 ? 16 : K == 2 ? 8 : K == 3 ? 4 : K == 4 ? 2 : 1);
+  // patches per batch (PPB_ = 0: the default; the autotuner picks among variants)
+  static constexpr int PPB = PPB_ > 0 ? PPB_ : sm3_default_ppb<K, T>();
   // threads = widest stage (y lines), rounded to warps
   static constexpr int NT_RAW = (PPB * M * N1 + 31) / 32 * 32;
   static constexpr int NT = NT_RAW < 128 ? 128 : NT_RAW;
@@ -151,6 +158,17 @@ __device__ __forceinline__ void apply_evec2(const T (&in)[2 * K - 1], T (&out)[2
   }
 }
 
+// patches per batch of autotuner variant v: 0 the default P, 1 P/2, 2 2P
+// (variants that would not fit in shared memory fall back to P)
+template <int K, typename T, int V>
+constexpr int sm3_variant_ppb()
+{
+  constexpr int P = sm3_default_ppb<K, T>();
+  if constexpr (V == 1) return P > 1 ? P / 2 : P;
+  else if constexpr (V == 2) return Sm3<K, T, 2 * P>::BYTES <= 232448 ? 2 * P : P;
+  else return P;
+}
+
 struct Sm3Args {
   int nx_c, ny_c, n_patches;  // patch lattice of the colour
   int cx, cy, cz;             // colour parities
@@ -159,14 +177,14 @@ struct Sm3Args {
   int64_t sy, sz;             // vector pitches (elements)
 };
 
-template <int K, typename T, bool USE_TMA>
-__global__ void __launch_bounds__(Sm3<K, T>::NT)
+template <int K, typename T, bool USE_TMA, int PPB_ = 0>
+__global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
     smoother3d_kernel(const __grid_constant__ CUtensorMap map_x,
                       const __grid_constant__ CUtensorMap map_b, T *__restrict__ x,
                       const T *__restrict__ b, const Sm3Args a, T scale, T fd_scale,
                       int *__restrict__ err)
 {
-  using S = Sm3<K, T>;
+  using S = Sm3<K, T, PPB_>;
   using P2 = typename Pair<T>::type;
   constexpr int N1 = S::N1, M = S::M, W = S::W, PPB = S::PPB, NT = S::NT, AL = S::A;
   const DegreeTables<K, T> &tb = c_tables<K, T>;

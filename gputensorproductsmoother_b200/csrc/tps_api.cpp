@@ -132,6 +132,7 @@ struct tps_handle {
   std::vector<double> coarse_inv_host;  // n_int^2, FP64
   std::vector<int> coarse_coord;        // (x, y, z) of each interior coarse DoF
   VcycleVectors vc[2];  // [0] FP64, [1] FP32
+  std::vector<int> sm_variant[2];  // per level: 3D smoother patches-per-batch variant (autotuned)
   DevBuf err_flag;      // set by a kernel whose bounded wait gave up
   // variable coefficient: per-level per-cell kappa (fine given, coarse = mean of children)
   bool has_kappa = false;
@@ -359,6 +360,7 @@ void smoother_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void 
 {
   const bool use_tc = tc && p == 1 && h->dim == 3 && !h->has_kappa && maps && maps->tc_valid &&
                       h->kt->smoother_tc;
+  const int variant = level < static_cast<int>(h->sm_variant[p].size()) ? h->sm_variant[p][level] : 0;
   if (!h->err_flag.p) h->err_flag.alloc(sizeof(int));
   const int nc = 1 << h->dim;
   for (int i = 0; i < nc; ++i) {
@@ -371,7 +373,7 @@ void smoother_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void 
                                   h->err_flag.as<int>(), s));
     else
       TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], lay, x, b, c, h->omega,
-                                              (x_zero && i == 0) ? 1 : 0, maps,
+                                              (x_zero && i == 0) ? 1 : 0, variant, maps,
                                               h->err_flag.as<int>(), s));
   }
 }
@@ -681,6 +683,42 @@ void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, c
   TPS_CUDA(launch_from_vcycle(dst, V.su[L]->p, p == 1 ? 1 : 0, pm, N, s));
 }
 
+
+// Patches-per-batch autotuner of the 3D smoother: every level of precision p
+// times each compiled variant on the V-cycle work vectors (one warm-up sweep,
+// then the best of three timed sweeps) and keeps the fastest.
+void autotune_levels(tps_handle *h, int p, cudaStream_t s)
+{
+  VcycleVectors &V = vcycle_vectors(h, p);
+  ensure_krylov(h);
+  h->sm_variant[p].assign(h->n_levels, 0);
+  if (h->dim != 3 || h->has_kappa) return;
+  for (int l = 0; l < h->n_levels; ++l) {
+    float best = 1e30f;
+    int bv = 0;
+    for (int v = 0; v < kSmootherVariants; ++v) {
+      if (v > 0 && h->kt->smoother_ppb(3, p == 0 ? 0 : 1, v) == h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 0)) continue;
+      h->sm_variant[p][l] = v;
+      smoother_sweep(h, l, p, V.layout[l], V.su[l]->p, V.d[l]->p, false, false, &V.maps[l], s);
+      float t = 1e30f;
+      for (int r = 0; r < 3; ++r) {
+        TPS_CUDA(cudaEventRecord(h->ev0, s));
+        smoother_sweep(h, l, p, V.layout[l], V.su[l]->p, V.d[l]->p, false, false, &V.maps[l], s);
+        TPS_CUDA(cudaEventRecord(h->ev1, s));
+        TPS_CUDA(cudaEventSynchronize(h->ev1));
+        float ms = 0.f;
+        TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        t = ms < t ? ms : t;
+      }
+      if (t < best) {
+        best = t;
+        bv = v;
+      }
+    }
+    h->sm_variant[p][l] = bv;
+  }
+  TPS_CUDA(cudaMemsetAsync(V.su.back()->p, 0, V.su.back()->bytes, s));
+}
 
 // tps_smoother_step with TPS_TF32 on caller vectors (FP32, lexicographic):
 // the sweep runs on the padded, TMA-addressable V-cycle vectors of the level
@@ -1052,6 +1090,19 @@ int tps_cell_energy(tps_handle *h, const double *u, const double *lam, double *e
   });
 }
 
+int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level)
+{
+  return guarded(h, [&] {
+    const int p = dt_index(dtype);
+    if (!h->own_stream) TPS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    autotune_levels(h, p, h->own_stream);
+    TPS_CUDA(cudaStreamSynchronize(h->own_stream));
+    if (ppb_per_level)
+      for (int l = 0; l < h->n_levels; ++l)
+        ppb_per_level[l] = h->kt->smoother_ppb(h->dim, p == 0 ? 0 : 1, h->sm_variant[p][l]);
+  });
+}
+
 int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *ms_per_sweep,
                       void *stream)
 {
@@ -1206,6 +1257,22 @@ void batch_build(tps_batch *B, const tps_solve_opts &o, const double *const *b, 
   for (tps_handle *h : B->sys) {  // every allocation happens before the capture
     vcycle_vectors(h, p);
     ensure_krylov(h);
+  }
+  // patches-per-batch autotuning, once per distinct hierarchy of the batch
+  for (int i = 0; i < n; ++i) {
+    tps_handle *h = B->sys[i];
+    if (static_cast<int>(h->sm_variant[p].size()) == h->n_levels) continue;
+    int j = 0;
+    for (; j < i; ++j) {
+      const tps_handle *o2 = B->sys[j];
+      if (o2->dim == h->dim && o2->k == h->k && o2->n_coarse == h->n_coarse && o2->n_levels == h->n_levels &&
+          static_cast<int>(o2->sm_variant[p].size()) == o2->n_levels)
+        break;
+    }
+    if (j < i)
+      h->sm_variant[p] = B->sys[j]->sm_variant[p];
+    else
+      autotune_levels(h, p, s);
   }
   std::vector<CGScalars *> scp(n);
   for (int i = 0; i < n; ++i) scp[i] = B->sys[i]->scalars.as<CGScalars>();

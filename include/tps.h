@@ -164,6 +164,14 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
                    double *x_host, tps_report *report);
 
+/* Patches-per-batch autotuner of the 3D smoother (the reference's
+ * AdditionalData::patch_per_block, include/patch_smoother.cuh:101-118, chosen
+ * by timing): every level of the dtype's V-cycle times each compiled variant
+ * and keeps the fastest for later sweeps and V-cycles of this handle.
+ * ppb_per_level (n_levels entries, may be null) receives the chosen values
+ * (0 in 2D).  Batched solves tune their systems automatically. */
+int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
+
 /* ---- batched solves (no reference counterpart) ----------------------------
  * A batch owns n independent systems (1 <= n <= 256): right-hand sides of one
  * mesh and/or meshes of different sizes; system i is built from problems[i]

@@ -56,3 +56,24 @@ def test_batch_max_iter_and_zero_rhs(cuda):
     with pytest.raises(tps.TpsError):
         B.solve(rhs, precision="fp32", rel_tol=1e-14, max_iter=2)
     B.close()
+
+
+def test_autotune_keeps_results(cuda):
+    """The patches-per-batch variants only regroup independent patches of a
+    colour: the autotuned sweep is bit-identical to the default one."""
+    P = tps.PoissonProblem(3, 3, 16)
+    N1 = 49
+    x0, b = interior_random(3, N1, 1).float(), interior_random(3, N1, 2).float()
+    x_def = x0.clone()
+    tps.PatchSmoother(P).step(x_def, b)
+    ppb = P.autotune("fp32")
+    assert len(ppb) == P.n_levels and all(v >= 1 for v in ppb)
+    x_tuned = x0.clone()
+    tps.PatchSmoother(P).step(x_tuned, b)
+    torch.cuda.synchronize()
+    assert torch.equal(x_tuned, x_def)
+    MG = tps.MultigridSolvers(P)
+    bb = interior_random(3, N1, 3)
+    x, rep = MG.solve_cg(bb, precision="fp32", rel_tol=1e-10)
+    assert rep.converged
+    assert P.autotune("fp64")[0] >= 1

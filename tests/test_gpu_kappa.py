@@ -61,8 +61,7 @@ def test_kappa_vcycle_and_cg(cuda, oracle, dim, k, n):
     xr, itr, _ = H.solve_cg(b, precision=0, symmetric=True, rel_tol=1e-10)
     x, rep = tps.MultigridSolvers(P).solve_cg(torch.tensor(b, device="cuda"), precision="fp64",
                                               rel_tol=1e-10)
-    # the patch-mean-kappa local solve makes the smoother weak for strongly
-    # varying kappa; in slowly converging runs rounding can shift the count
+    # rounding can shift the count of a longer run by one
     assert rep.converged and abs(rep.iterations - itr) <= 1 + itr // 20
     assert relerr(x.cpu().numpy(), xr) < 1e-8
     x32, rep32 = tps.MultigridSolvers(P).solve_cg(torch.tensor(b, device="cuda"), precision="fp32",
@@ -129,3 +128,35 @@ def test_adjoint_gradients_match_finite_differences(cuda):
         ad_f, ad_k = (gf * df).sum(), (gk * dk).sum()
         assert abs(ad_f - fd_f) <= 1e-6 * abs(fd_f), (d, ad_f.item(), fd_f.item())
         assert abs(ad_k - fd_k) <= 1e-6 * abs(fd_k), (d, ad_k.item(), fd_k.item())
+
+
+def test_adjoint_48cubed_q4(cuda):
+    """The adjoint configuration itself (Q4, 48^3 cells, coarse 3^3, kappa =
+    exp(N(0, 0.5^2))): forward and adjoint MG-CG converge and two random
+    directions agree with central differences (h = 1e-6) to 1e-6."""
+    dim, k, n = 3, 4, 48
+    rng = np.random.default_rng(0)
+    kap = torch.tensor(np.exp(rng.normal(0.0, 0.5, n ** dim)), device="cuda")
+    P = tps.PoissonProblem(dim, k, n, kappa=kap)
+    N = P.n_dofs()
+    f = torch.tensor(rng.uniform(-1, 1, N), device="cuda")
+    with torch.no_grad():
+        u0 = tps.autograd.solve(P, f, kap, rel_tol=1e-13)
+    ut = u0 * torch.tensor(1.0 + 0.3 * rng.standard_normal(N), device="cuda")
+
+    def J(f_, k_):
+        u = tps.autograd.solve(P, f_, k_, rel_tol=1e-13)
+        return 0.5 * ((u - ut) ** 2).sum()
+
+    fv, kv = f.clone().requires_grad_(True), kap.clone().requires_grad_(True)
+    J(fv, kv).backward()
+    h = 1e-6
+    for _ in range(2):
+        df = torch.tensor(rng.standard_normal(N), device="cuda")
+        dk = torch.tensor(rng.standard_normal(n ** dim), device="cuda") * kap
+        with torch.no_grad():
+            fd_f = (J(f + h * df, kap) - J(f - h * df, kap)) / (2 * h)
+            fd_k = (J(f, kap + h * dk) - J(f, kap - h * dk)) / (2 * h)
+        assert abs((fv.grad * df).sum() - fd_f) <= 1e-6 * abs(fd_f)
+        assert abs((kv.grad * dk).sum() - fd_k) <= 1e-6 * abs(fd_k)
+    P.close()
