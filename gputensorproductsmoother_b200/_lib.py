@@ -75,6 +75,8 @@ SIGNATURES = [
     ("tps_cell_energy", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     ("tps_restrict_add_noalloc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, _VP, _VP, _VP]),
+    ("tps_fmg", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP), ctypes.POINTER(_VP), _VP,
+                               ctypes.POINTER(TpsReport), _VP]),
     ("tps_autotune", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("tps_batch_destroy", ctypes.c_int, [_VP]),

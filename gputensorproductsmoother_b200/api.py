@@ -306,6 +306,27 @@ class MultigridSolvers:
             L.check(st, p.handle)
         return x, _report(rep)
 
+    def solve_fmg(self, rhs_levels, bnd_levels=None, precision: str = "fp32", n_cycles: int = 1):
+        """MultigridSolvers::solve: one full-multigrid pass.  rhs_levels[l]: the
+        right-hand side of level l (float64 CUDA tensors, lifting of the
+        Dirichlet data included); bnd_levels[l] (optional): Dirichlet values on
+        the boundary DoFs of level l.  Returns (x, SolveReport)."""
+        p = self.problem
+        n = p.n_levels
+        if len(rhs_levels) != n or (bnd_levels is not None and len(bnd_levels) != n):
+            raise ValueError(f"one vector per level ({n}) is required")
+        for l in range(n):
+            p._check_vec(rhs_levels[l], l, torch.float64)
+            if bnd_levels is not None:
+                p._check_vec(bnd_levels[l], l, torch.float64)
+        x = p.new_vector()
+        rp = (ctypes.c_void_p * n)(*[r.data_ptr() for r in rhs_levels])
+        bp = None if bnd_levels is None else (ctypes.c_void_p * n)(*[b.data_ptr() for b in bnd_levels])
+        rep = L.TpsReport()
+        L.check(L.lib().tps_fmg(p.handle, _PRECISIONS[precision], n_cycles, rp, bp, x.data_ptr(),
+                                ctypes.byref(rep), _stream()), p.handle)
+        return x, _report(rep)
+
     def solve_cg(self, b: torch.Tensor, x: torch.Tensor | None = None, precision: str = "fp32",
                  symmetric: bool = True, max_iter: int = 100, rel_tol: float = 1e-10,
                  use_graph: bool = True, raise_on_fail: bool = True):

@@ -85,6 +85,9 @@ struct KernelTable {
   cudaError_t (*encode_tc_maps)(const VecLayout &l, void *x, const void *b, SmootherMaps *out);
   // patches per CTA batch of smoother variant v (dtype 0 FP64, 1 FP32; 0 in 2D)
   int (*smoother_ppb)(int dim, int dtype, int variant);
+  // FP64 fine += P coarse with the coarse boundary values used ([dim - 2])
+  cudaError_t (*prolong_nb[2])(const LevelGeomH &coarse, const VecLayout &lc, const VecLayout &lf,
+                               void *fine, const void *coarse_v, void *tmp, cudaStream_t);
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda

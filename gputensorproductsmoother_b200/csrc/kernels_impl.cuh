@@ -328,27 +328,43 @@ cudaError_t encode_maps(const VecLayout &l, void *x, const void *b, SmootherMaps
   return e;
 }
 
-template <int DIM, typename T>
-cudaError_t prolong(const LevelGeomH &gc, const VecLayout &lc, const VecLayout &lf, void *fine,
-                    const void *coarse, void *tmp, cudaStream_t s)
+template <int DIM, typename T, bool MASK>
+cudaError_t prolong_impl(const LevelGeomH &gc, const VecLayout &lc, const VecLayout &lf, void *fine,
+                         const void *coarse, void *tmp, cudaStream_t s)
 {
   constexpr int C = XYTile<K>::C;
   const int N1c = gc.N1, N1f = 2 * gc.n * K + 1;
   const unsigned gxy = ceil_div(gc.n, C);
   if constexpr (DIM == 2) {
     prolong_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, 1), XYTile<K>::NT, 0, s>>>(
-        static_cast<T *>(fine), static_cast<const T *>(coarse), N1c, N1f, lc.sy, 0, lf.sy, 0, 0, 1);
+        static_cast<T *>(fine), static_cast<const T *>(coarse), N1c, N1f, lc.sy, 0, lf.sy, 0, 0, MASK ? 1 : 0);
   } else {
     const int64_t P = static_cast<int64_t>(N1c) * N1c;
-    prolong_z_kernel<K, T><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
+    prolong_z_kernel<K, T, MASK><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
         static_cast<T *>(tmp), static_cast<const T *>(coarse), N1c, N1f, gc.n, lc.sy, lc.sz);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // fine interior planes 1..N1f-2 from tmp planes 1..N1f-2
     prolong_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, N1f - 2), XYTile<K>::NT, 0, s>>>(
-        static_cast<T *>(fine), static_cast<const T *>(tmp), N1c, N1f, N1c, P, lf.sy, lf.sz, 1, 0);
+        static_cast<T *>(fine), static_cast<const T *>(tmp), N1c, N1f, N1c, P, lf.sy, lf.sz, 1, MASK ? 1 : 0);
   }
   return cudaGetLastError();
+}
+
+template <int DIM, typename T>
+cudaError_t prolong(const LevelGeomH &gc, const VecLayout &lc, const VecLayout &lf, void *fine,
+                    const void *coarse, void *tmp, cudaStream_t s)
+{
+  return prolong_impl<DIM, T, true>(gc, lc, lf, fine, coarse, tmp, s);
+}
+
+// FP64 prolongation that reads the coarse boundary values (the FMG
+// prolongation of the solution); fine interior DoFs += P coarse
+template <int DIM>
+cudaError_t prolong_nb(const LevelGeomH &gc, const VecLayout &lc, const VecLayout &lf, void *fine,
+                       const void *coarse, void *tmp, cudaStream_t s)
+{
+  return prolong_impl<DIM, double, false>(gc, lc, lf, fine, coarse, tmp, s);
 }
 
 template <int DIM, typename T>
@@ -491,6 +507,7 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
 #endif
     &deg_impl::encode_tc_maps,
     &deg_impl::smoother_ppb,
+    {&deg_impl::prolong_nb<2>, &deg_impl::prolong_nb<3>},
 };
 
 }  // namespace tps

@@ -147,6 +147,9 @@ struct tps_handle {
   cudaStream_t graph_stream = nullptr;
   const double *graph_x = nullptr;  // the captured graph updates this solution vector
   cudaStream_t own_stream = nullptr;  // used by tps_solve_host
+  DevBuf host_b, host_x;              // device staging of tps_solve_host (kept, so its graph stays valid)
+  std::vector<std::unique_ptr<DevBuf>> fmg_sol, fmg_res;  // FMG: FP64 per level (lexicographic)
+  DevBuf fmg_tmp;                                        // FMG: FP64 transfer scratch
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   ~tps_handle()
@@ -448,8 +451,11 @@ void coarse_solve(tps_handle *h, int p, cudaStream_t s, bool tc)
 }
 
 // MultigridSolvers::v_cycle (include/solver.cuh:1952-2001) on precision p:
-// input d[level], output su[level]; tc: FP32 3D sweeps on the tensor cores
-void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s, bool tc)
+// input d[level], output su[level]; tc: FP32 3D sweeps on the tensor cores;
+// zero_init = false continues from the current su[level] (a further cycle of
+// v_cycle(level, n_cycles), include/solver.cuh:798-805)
+void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s, bool tc,
+                bool zero_init = true)
 {
   VcycleVectors &V = h->vc[p];
   if (level == 0) {
@@ -459,8 +465,8 @@ void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s,
   const LevelGeomH &g = h->lv[level];
   const VecLayout &lay = V.layout[level], &lc = V.layout[level - 1];
   const int di = h->dim - 2;
-  TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, V.su[level]->bytes, s));
-  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, true, &V.maps[level], s, tc);
+  if (zero_init) TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, V.su[level]->bytes, s));
+  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, zero_init, &V.maps[level], s, tc);
   level_laplace(h, level, p, lay, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s);
   TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], lc, lay, V.d[level - 1]->p, V.t[level]->p,
                                    V.tmp[level]->p, 0, s));
@@ -740,6 +746,79 @@ void tc_smoother_step(tps_handle *h, int level, void *x, const void *b, bool zer
   TPS_CUDA(cudaMemcpy2DAsync(x, row, px, pitch, row, rows, cudaMemcpyDeviceToDevice, s));
 }
 
+// MultigridSolvers::solve (include/solver.cuh:1784-1860), see tps_fmg
+void fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, const double *const *bnd,
+         double *x, tps_report *rep, cudaStream_t s)
+{
+  const int p = vprec_index(precision), L = h->n_levels - 1, dim = h->dim;
+  const bool tc = vprec_tc(precision);
+  if (tc) check_tc(h);
+  VcycleVectors &V = vcycle_vectors(h, p);
+  ensure_krylov(h);
+  if (h->fmg_sol.size() != static_cast<size_t>(h->n_levels)) {
+    h->fmg_sol.clear();
+    h->fmg_res.clear();
+    size_t tmp = 0;
+    for (int l = 0; l <= L; ++l) {
+      h->fmg_sol.emplace_back(new DevBuf);
+      h->fmg_res.emplace_back(new DevBuf);
+      if (l < L) h->fmg_sol[l]->alloc(sizeof(double) * h->lv[l].N);
+      h->fmg_res[l]->alloc(sizeof(double) * h->lv[l].N);
+      if (l > 0 && dim == 3)
+        tmp = std::max(tmp, sizeof(double) * static_cast<size_t>(h->lv[l].N1) * h->lv[l - 1].N1 * h->lv[l - 1].N1);
+    }
+    if (tmp) h->fmg_tmp.alloc(tmp);
+  }
+  auto padmap = [&](int l) { return PadMap{V.layout[l].N1, V.layout[l].sy}; };
+  const int zk = p == 1 ? 1 : 0;
+  TPS_CUDA(cudaEventRecord(h->ev0, s));
+  // coarse level: coarse solve, then one more smoother step
+  TPS_CUDA(launch_to_vcycle(V.d[0]->p, input_kind(precision), padmap(0), rhs[0], h->lv[0].N, s));
+  coarse_solve(h, p, s, tc);
+  smoother_sweep(h, 0, p, V.layout[0], V.su[0]->p, V.d[0]->p, false, false, &V.maps[0], s, tc);
+  double *sol0 = L == 0 ? x : h->fmg_sol[0]->as<double>();
+  TPS_CUDA(launch_from_vcycle(sol0, V.su[0]->p, zk, padmap(0), h->lv[0].N, s));
+  for (int l = 1; l <= L; ++l) {
+    const LevelGeomH &g = h->lv[l], &gc = h->lv[l - 1];
+    double *solc = h->fmg_sol[l - 1]->as<double>();
+    double *sol = l == L ? x : h->fmg_sol[l]->as<double>();
+    double *res = h->fmg_res[l]->as<double>();
+    if (bnd && bnd[l - 1]) TPS_CUDA(launch_copy_boundary(solc, bnd[l - 1], dim, gc.N1, 8, s));
+    TPS_CUDA(cudaMemsetAsync(sol, 0, sizeof(double) * g.N, s));
+    TPS_CUDA(h->kt->prolong_nb[dim - 2](gc, lex_layout(h, l - 1), lex_layout(h, l), sol, solc, h->fmg_tmp.p, s));
+    TPS_CUDA(cudaMemsetAsync(res, 0, sizeof(double) * g.N, s));
+    level_laplace(h, l, 0, lex_layout(h, l), res, sol, rhs[l], 1, s);
+    TPS_CUDA(launch_to_vcycle(V.d[l]->p, input_kind(precision), padmap(l), res, g.N, s));
+    for (int c = 0; c < n_cycles; ++c) vcycle_rec(h, l, p, false, s, tc, c == 0);
+    TPS_CUDA(launch_from_vcycle(res, V.su[l]->p, zk, padmap(l), g.N, s));
+    TPS_CUDA(launch_axpy_f64(sol, 1.0, res, g.N, s));
+  }
+  // final relative residual of the homogeneous part, then the Dirichlet data
+  double *r = h->fmg_res[L]->as<double>();
+  TPS_CUDA(cudaMemsetAsync(r, 0, sizeof(double) * h->fine().N, s));
+  level_laplace(h, L, 0, lex_layout(h, L), r, x, rhs[L], 1, s);
+  const double rr = dev_dot(h, r, r, s);
+  // ||b|| on the interior rows: r = rhs - A 0 writes exactly those rows
+  TPS_CUDA(cudaMemsetAsync(h->q.p, 0, sizeof(double) * h->fine().N, s));
+  TPS_CUDA(cudaMemsetAsync(h->r.p, 0, sizeof(double) * h->fine().N, s));
+  level_laplace(h, L, 0, lex_layout(h, L), h->r.p, h->q.p, rhs[L], 1, s);
+  const double bb = dev_dot(h, h->r.as<double>(), h->r.as<double>(), s);
+  if (bnd && bnd[L]) TPS_CUDA(launch_copy_boundary(x, bnd[L], dim, h->fine().N1, 8, s));
+  TPS_CUDA(cudaEventRecord(h->ev1, s));
+  TPS_CUDA(cudaEventSynchronize(h->ev1));
+  float ms = 0.f;
+  TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+  if (rep) {
+    std::memset(rep, 0, sizeof(*rep));
+    rep->iterations = n_cycles;
+    rep->initial_residual = std::sqrt(bb);
+    rep->final_residual = std::sqrt(rr) / (bb > 0 ? std::sqrt(bb) : 1.0);
+    rep->history[0] = 1.0;
+    rep->converged = std::isfinite(rep->final_residual) ? 1 : 0;
+    rep->time_ms = ms;
+  }
+}
+
 // deal.II SolverGMRES semantics (left preconditioning, MGS, Givens) as used by
 // MultigridSolvers::solve_gmres (include/solver.cuh:1865-1910)
 int solve_gmres(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
@@ -1010,6 +1089,18 @@ int tps_restrict_add(tps_handle *h, int from_level, int dtype, void *coarse, con
   });
 }
 
+int tps_fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, const double *const *bnd,
+            double *x, tps_report *report, void *stream)
+{
+  return guarded(h, [&] {
+    if (!rhs || !x) throw ApiError(TPS_ERR_INVALID, "null argument");
+    if (n_cycles < 1) throw ApiError(TPS_ERR_INVALID, "n_cycles must be >= 1");
+    for (int l = 0; l < h->n_levels; ++l)
+      if (!rhs[l] || (bnd && !bnd[l])) throw ApiError(TPS_ERR_INVALID, "a right-hand side (or Dirichlet vector) per level is required");
+    fmg(h, precision, n_cycles, rhs, bnd, x, report, static_cast<cudaStream_t>(stream));
+  });
+}
+
 int tps_vcycle(tps_handle *h, int precision, int symmetric, double *dst, const double *src,
                void *stream)
 {
@@ -1140,21 +1231,16 @@ int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_ho
     const int64_t N = h->fine().N;
     if (!h->own_stream) TPS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     cudaStream_t s = h->own_stream;
-    DevBuf db, dx;
-    db.alloc(sizeof(double) * N);
-    dx.alloc(sizeof(double) * N);
-    TPS_CUDA(cudaMemcpyAsync(db.p, b_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    TPS_CUDA(cudaMemcpyAsync(dx.p, x_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    status = tps_solve(h, opts, db.as<double>(), dx.as<double>(), report, s);
-    if (status == TPS_OK || status == TPS_ERR_NOT_CONVERGED) {
-      TPS_CUDA(cudaMemcpyAsync(x_host, dx.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
-      TPS_CUDA(cudaStreamSynchronize(s));
+    if (!h->host_b.p) {
+      h->host_b.alloc(sizeof(double) * N);
+      h->host_x.alloc(sizeof(double) * N);
     }
-    // the cached graph refers to dx, which is freed on return
-    if (h->graph_x == dx.as<double>()) {
-      cudaGraphExecDestroy(h->graph);
-      h->graph = nullptr;
-      h->graph_x = nullptr;
+    TPS_CUDA(cudaMemcpyAsync(h->host_b.p, b_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    TPS_CUDA(cudaMemcpyAsync(h->host_x.p, x_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    status = tps_solve(h, opts, h->host_b.as<double>(), h->host_x.as<double>(), report, s);
+    if (status == TPS_OK || status == TPS_ERR_NOT_CONVERGED) {
+      TPS_CUDA(cudaMemcpyAsync(x_host, h->host_x.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));
+      TPS_CUDA(cudaStreamSynchronize(s));
     }
   });
   return rc != TPS_OK ? rc : status;

@@ -197,8 +197,9 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
 
 // ---------------------------------------------------------------------------
 // z pass, prolongation: coarse (N1c planes of P entries) -> tmp (N1f planes of
-// P entries), P = N1c^2.  Input entries on the coarse boundary read as zero.
-template <int K, typename T>
+// P entries), P = N1c^2.  Input entries on the coarse boundary read as zero
+// (MASK) or as they are (the FMG prolongation of the solution).
+template <int K, typename T, bool MASK = true>
 __global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coarse, int N1c,
                                  int N1f, int n_cells_c, int64_t c_sy, int64_t c_sz)
 {
@@ -212,12 +213,12 @@ __global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coar
 #pragma unroll
   for (int b = 0; b <= K; ++b) {
     const int gz = c * K + b;
-    v[b] = (bxy || gz == 0 || gz == N1c - 1) ? T(0) : __ldg(&coarse[gz * c_sz + gy * c_sy + gx]);
+    v[b] = (MASK && (bxy || gz == 0 || gz == N1c - 1)) ? T(0) : __ldg(&coarse[gz * c_sz + gy * c_sy + gx]);
   }
   prol_cell<K, T>(v, o);
 #pragma unroll
   for (int f = 0; f < 2 * K; ++f) tmp[(2 * K * c + f) * P + idx] = o[f];
-  if (c == n_cells_c - 1) tmp[(N1f - 1) * P + idx] = T(0);
+  if (c == n_cells_c - 1) tmp[(N1f - 1) * P + idx] = MASK ? T(0) : v[K];
 }
 
 // z pass, restriction: tmp (N1f planes of P = N1c^2 entries) -> coarse.

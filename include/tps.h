@@ -135,6 +135,22 @@ void tps_solve_opts_default(tps_solve_opts *opts);
 int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double *x,
               tps_report *report, void *stream);
 
+/* MultigridSolvers::solve (include/solver.cuh:1784-1860): one full-multigrid
+ * pass.  rhs[l] (level l = 0..n_levels-1, FP64 device vectors, lexicographic):
+ * the right-hand side of every level, with the lifting of the Dirichlet data
+ * already subtracted, as the reference assembles it on every level; bnd (may
+ * be null): per level the Dirichlet values on the boundary DoFs (other entries
+ * ignored).  Coarse solve plus one smoother step; then per level the coarse
+ * solution with its Dirichlet data is prolongated without boundary
+ * constraints (FP64), the fine boundary set to zero, the FP64 residual formed
+ * and n_cycles V-cycles (precision: tps_vcycle_precision, reference colour
+ * order) add the correction.  x (finest level) receives the solution with the
+ * Dirichlet data on its boundary.  report (may be null): final_residual =
+ * ||rhs - A x_0||/||rhs|| on the interior rows (x_0: x with zero boundary),
+ * iterations = n_cycles, time_ms. */
+int tps_fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs,
+            const double *const *bnd, double *x, tps_report *report, void *stream);
+
 /* Variable coefficient -div(kappa grad u) (no reference counterpart; the
  * reference's operator has kappa = 1).  A handle created with a kappa array can
  * change it: the finest-level values are replaced, the coarser levels take the
@@ -160,7 +176,8 @@ int tps_cell_energy(tps_handle *h, const double *u, const double *lam, double *e
 int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *ms_per_sweep,
                       void *stream);
 
-/* Same solve with HOST buffers; the host<->device copies are part of the call. */
+/* Same solve with HOST buffers; the host<->device copies are part of the call.
+ * The handle keeps two device staging vectors (16 N bytes) between calls. */
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
                    double *x_host, tps_report *report);
 

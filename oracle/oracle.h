@@ -32,6 +32,7 @@ int orc_patch_eigen(int k, double h, double *S, double *lam);
                               const REAL *b, int zero_init, int reverse,               \
                               const double *kappa);                                    \
   void orc_prolongate_add##SUF(int dim, int k, int nc, REAL *fine, const REAL *coarse); \
+  void orc_prolongate_add_nb##SUF(int dim, int k, int nc, REAL *fine, const REAL *coarse); \
   void orc_restrict_add##SUF(int dim, int k, int nc, REAL *coarse, const REAL *fine);
 ORC_LEVEL_DECL(_d, double)
 ORC_LEVEL_DECL(_f, float)
@@ -58,6 +59,10 @@ int orc_solve_gmres(orc_hier *H, int precision, const double *b, double *x, doub
                     double abs_tol, int max_it, int basis_size, double *history);
 /* coarse direct solve of the hierarchy (interior DoFs, dense Cholesky) */
 void orc_coarse_solve(orc_hier *H, double *dst, const double *src);
+/* full multigrid pass (MultigridSolvers::solve): per-level right-hand sides,
+ * optional per-level Dirichlet data (boundary entries used), finest solution */
+void orc_fmg(orc_hier *H, int precision, int n_cycles, const double *const *rhs,
+             const double *const *bnd, double *x);
 
 #ifdef __cplusplus
 }

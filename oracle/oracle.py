@@ -64,6 +64,11 @@ def lib():
         L.orc_solve_cg.restype = ctypes.c_int
         L.orc_solve_cg.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp,
                                    ctypes.c_double, ctypes.c_int, _dp]
+        L.orc_fmg.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp),
+                              ctypes.POINTER(_dp), _dp]
+        for suf, ptr in (("_d", _dp), ("_f", _fp)):
+            getattr(L, "orc_prolongate_add_nb" + suf).argtypes = [
+                ctypes.c_int, ctypes.c_int, ctypes.c_int, ptr, ptr]
         L.orc_solve_gmres.restype = ctypes.c_int
         L.orc_solve_gmres.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, _dp, ctypes.c_double,
                                       ctypes.c_double, ctypes.c_int, ctypes.c_int, _dp]
@@ -196,6 +201,20 @@ class Hierarchy:
         it = lib().orc_solve_cg(self.h, precision, int(symmetric), _p(b), _p(x), rel_tol, max_it,
                                 _p(hist))
         return x, it, hist[: it + 1]
+
+    def fmg(self, rhs_levels, bnd_levels=None, precision=1, n_cycles=1):
+        """Full multigrid pass (MultigridSolvers::solve): rhs_levels[l] per level,
+        bnd_levels[l] Dirichlet data (boundary entries used) or None."""
+        L = self.n_levels
+        rh = [np.ascontiguousarray(r, dtype=np.float64) for r in rhs_levels]
+        rp = (_dp * L)(*[_p(r) for r in rh])
+        bp = None
+        if bnd_levels is not None:
+            bd = [np.ascontiguousarray(b, dtype=np.float64) for b in bnd_levels]
+            bp = (_dp * L)(*[_p(b) for b in bd])
+        x = np.zeros_like(rh[-1])
+        lib().orc_fmg(self.h, precision, n_cycles, rp, bp, _p(x))
+        return x
 
     def solve_gmres(self, b, precision=2, reduce=1e-9, abs_tol=1e-16, max_it=20, basis=28):
         b = np.ascontiguousarray(b, dtype=np.float64)

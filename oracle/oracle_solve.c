@@ -188,7 +188,7 @@ void orc_coarse_solve(orc_hier *H, double *dst, const double *src)
 }
 
 #define DEFINE_VCYCLE(SUF, REAL, D, SU, T)                                                \
-  static void vcycle_rec##SUF(orc_hier *H, int symmetric, int l)                         \
+  static void vcycle_rec##SUF(orc_hier *H, int symmetric, int l, int zero_init)          \
   {                                                                                       \
     const int dim = H->dim, k = H->k;                                                     \
     if (l == 0) {                                                                         \
@@ -196,8 +196,8 @@ void orc_coarse_solve(orc_hier *H, double *dst, const double *src)
         orc_smoother_step##SUF(dim, k, H->n[0], 1.0, H->SU[0], H->D[0], 1, 0, H->kappa[0]); \
       } else {                                                                            \
         long N0 = H->N[0];                                                                \
-        double *s = (double *)calloc(N0, sizeof(double));                                \
-        double *o = (double *)malloc(sizeof(double) * N0);                                \
+        double *s = (double *)calloc((size_t)(N0 > 0 ? N0 : 1), sizeof(double));          \
+        double *o = (double *)malloc(sizeof(double) * (size_t)(N0 > 0 ? N0 : 1));         \
         for (long i = 0; i < N0; ++i) s[i] = H->D[0][i];                                  \
         orc_coarse_solve(H, o, s);                                                        \
         for (long i = 0; i < N0; ++i) H->SU[0][i] = (REAL)o[i];                           \
@@ -208,12 +208,12 @@ void orc_coarse_solve(orc_hier *H, double *dst, const double *src)
     }                                                                                     \
     const int n = H->n[l];                                                                \
     const long N = H->N[l];                                                               \
-    orc_smoother_step##SUF(dim, k, n, 1.0, H->SU[l], H->D[l], 1, 0, H->kappa[l]);         \
+    orc_smoother_step##SUF(dim, k, n, 1.0, H->SU[l], H->D[l], zero_init, 0, H->kappa[l]); \
     orc_laplace_vmult##SUF(dim, k, n, H->T[l], H->SU[l], H->kappa[l]);                    \
     for (long i = 0; i < N; ++i) H->T[l][i] = H->D[l][i] - H->T[l][i];                    \
     memset(H->D[l - 1], 0, sizeof(REAL) * H->N[l - 1]);                                   \
     orc_restrict_add##SUF(dim, k, H->n[l - 1], H->D[l - 1], H->T[l]);                     \
-    vcycle_rec##SUF(H, symmetric, l - 1);                                                 \
+    vcycle_rec##SUF(H, symmetric, l - 1, 1);                                              \
     orc_prolongate_add##SUF(dim, k, H->n[l - 1], H->SU[l], H->SU[l - 1]);                 \
     orc_smoother_step##SUF(dim, k, n, 1.0, H->SU[l], H->D[l], 0, symmetric, H->kappa[l]); \
   }
@@ -227,12 +227,12 @@ void orc_vcycle_level(orc_hier *H, int precision, int symmetric, int level, doub
   const long N = H->N[level];
   if (precision == 1) {
     for (long i = 0; i < N; ++i) H->df[level][i] = (float)src[i];
-    vcycle_rec_f(H, symmetric, level);
+    vcycle_rec_f(H, symmetric, level, 1);
     for (long i = 0; i < N; ++i) dst[i] = (double)H->suf[level][i];
   } else {
     for (long i = 0; i < N; ++i)
       H->dd[level][i] = precision == 2 ? (double)(float)src[i] : src[i];
-    vcycle_rec_d(H, symmetric, level);
+    vcycle_rec_d(H, symmetric, level, 1);
     memcpy(dst, H->sud[level], sizeof(double) * N);
   }
 }
@@ -240,6 +240,72 @@ void orc_vcycle_level(orc_hier *H, int precision, int symmetric, int level, doub
 void orc_vcycle(orc_hier *H, int precision, int symmetric, double *dst, const double *src)
 {
   orc_vcycle_level(H, precision, symmetric, H->n_levels - 1, dst, src);
+}
+
+/* MultigridSolvers::solve (include/solver.cuh:1784-1860): coarse solve plus
+ * one smoother step, then per finer level: Dirichlet data on the coarse
+ * solution, prolongation without boundary constraints (FP64), fine boundary
+ * set to zero, FP64 residual, n_cycles V-cycles in the V-cycle precision
+ * (v_cycle(level, n_cycles): the first pre-smoothing starts from zero, later
+ * ones continue), correction added.  The solution is kept with zero boundary
+ * entries (the Dirichlet data enter through the lifting in rhs) and the data
+ * are written into the boundary of x at the end (get_solution, :1776-1781). */
+void orc_fmg(orc_hier *H, int precision, int n_cycles, const double *const *rhs,
+             const double *const *bnd, double *x)
+{
+  const int L = H->n_levels - 1, dim = H->dim, k = H->k;
+  double **sol = (double **)calloc(L + 1, sizeof(double *));
+  for (int l = 0; l < L; ++l) sol[l] = (double *)calloc(H->N[l], sizeof(double));
+  sol[L] = x;
+  double *res = (double *)malloc(sizeof(double) * H->N[L]);
+  /* coarse level: coarse solve, then one more smoother step */
+  {
+    const long N0 = H->N[0];
+    if (precision == 1) {
+      for (long i = 0; i < N0; ++i) H->df[0][i] = (float)rhs[0][i];
+      vcycle_rec_f(H, 0, 0, 1);
+      orc_smoother_step_f(dim, k, H->n[0], 1.0, H->suf[0], H->df[0], 0, 0, H->kappa[0]);
+      for (long i = 0; i < N0; ++i) sol[0][i] = (double)H->suf[0][i];
+    } else {
+      for (long i = 0; i < N0; ++i) H->dd[0][i] = rhs[0][i];
+      vcycle_rec_d(H, 0, 0, 1);
+      orc_smoother_step_d(dim, k, H->n[0], 1.0, H->sud[0], H->dd[0], 0, 0, H->kappa[0]);
+      memcpy(sol[0], H->sud[0], sizeof(double) * N0);
+    }
+  }
+  for (int l = 1; l <= L; ++l) {
+    const long Nc = H->N[l - 1], N = H->N[l];
+    const int N1c = H->n[l - 1] * k + 1, N1 = H->n[l] * k + 1;
+    if (bnd && bnd[l - 1])
+      for (long i = 0; i < Nc; ++i)
+        if (is_boundary(dim, N1c, i)) sol[l - 1][i] = bnd[l - 1][i];
+    memset(sol[l], 0, sizeof(double) * N);
+    orc_prolongate_add_nb_d(dim, k, H->n[l - 1], sol[l], sol[l - 1]);
+    if (bnd && bnd[l - 1])
+      for (long i = 0; i < Nc; ++i)
+        if (is_boundary(dim, N1c, i)) sol[l - 1][i] = 0.0;
+    orc_laplace_vmult_d(dim, k, H->n[l], res, sol[l], H->kappa[l]);
+    for (long i = 0; i < N; ++i) res[i] = is_boundary(dim, N1, i) ? 0.0 : rhs[l][i] - res[i];
+    for (int c = 0; c < n_cycles; ++c) {
+      if (precision == 1) {
+        for (long i = 0; i < N; ++i) H->df[l][i] = (float)res[i];
+        vcycle_rec_f(H, 0, l, c == 0);
+      } else {
+        for (long i = 0; i < N; ++i) H->dd[l][i] = res[i];
+        vcycle_rec_d(H, 0, l, c == 0);
+      }
+    }
+    if (precision == 1)
+      for (long i = 0; i < N; ++i) sol[l][i] += (double)H->suf[l][i];
+    else
+      for (long i = 0; i < N; ++i) sol[l][i] += H->sud[l][i];
+  }
+  if (bnd && bnd[L])
+    for (long i = 0; i < H->N[L]; ++i)
+      if (is_boundary(dim, H->n[L] * k + 1, i)) x[i] = bnd[L][i];
+  for (int l = 0; l < L; ++l) free(sol[l]);
+  free(sol);
+  free(res);
 }
 
 void orc_fine_vmult(orc_hier *H, double *dst, const double *src)
