@@ -40,7 +40,8 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson3d_q4_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--mode", default="solve", choices=["solve", "smoother", "operator", "batch", "adjoint"],
+    ap.add_argument("--mode", default="solve",
+                    choices=["solve", "smoother", "operator", "batch", "adjoint", "micro"],
                     help="smoother / operator: only time the finest-level smoother "
                          "sweeps / FP64 operator applications (small commands for kernel "
                          "profiling)")
@@ -259,6 +260,74 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_micro(args):
+    """Micro-benchmarks of the level operations (the reference's
+    apps/benchmark_mg.cu:238-503): operator FP64/FP32, transfers FP64/FP32
+    between the two finest levels, and the finest-level smoother for every
+    compiled patches-per-block variant (FP64, FP32) and the tensor-core
+    variant.  Best of 5 repetitions of 10 calls, CUDA events; one JSON line."""
+    import torch
+    import gputensorproductsmoother_b200 as tps
+    from gputensorproductsmoother_b200 import _lib as L
+    from gputensorproductsmoother_b200 import problems
+    dim, k, n, _ = problems.WORKLOADS[args.workload]
+    P = tps.PoissonProblem(dim, k, n)
+    lf = P.n_levels - 1
+    N, Nc = P.n_dofs(lf), P.n_dofs(lf - 1)
+    rows = []
+
+    def best(fn, calls=10, reps=5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        fn()
+        t = 1e30
+        for _ in range(reps):
+            e0.record()
+            for _ in range(calls):
+                fn()
+            e1.record()
+            torch.cuda.synchronize()
+            t = min(t, e0.elapsed_time(e1) / calls)
+        return t
+
+    for dt, name in ((torch.float64, "DP"), (torch.float32, "SP")):
+        src = problems.make_rhs(args.workload).to(dt)
+        dst = torch.empty_like(src)
+        A = tps.LaplaceOperator(P)
+        ms = best(lambda: A.vmult(dst, src))
+        rows.append({"name": f"Mat-vec {name}", "ms": ms, "dof_per_s": N / (ms * 1e-3),
+                     "GBps": 2 * src.element_size() * N / (ms * 1e-3) / 1e9})
+        T = tps.MGTransferCUDA(P)
+        fine = torch.ones(N, dtype=dt, device="cuda")
+        coarse = torch.ones(Nc, dtype=dt, device="cuda")
+        ms = best(lambda: T.prolongate_and_add(lf, fine, coarse))
+        rows.append({"name": f"Prolongation {name}", "ms": ms, "dof_per_s": N / (ms * 1e-3)})
+        ms = best(lambda: T.restrict_and_add(lf, coarse, fine))
+        rows.append({"name": f"Restriction {name}", "ms": ms, "dof_per_s": N / (ms * 1e-3)})
+    for dtname, code in (("DP", L.TPS_F64), ("SP", L.TPS_F32)):
+        ppb = (ctypes.c_int * 3)()
+        L.check(L.lib().tps_smoother_variants(P.handle, code, ppb), P.handle)
+        seen = set()
+        for v in range(3):
+            if ppb[v] in seen:
+                continue
+            seen.add(ppb[v])
+            L.check(L.lib().tps_set_smoother_variant(P.handle, code, lf, v), P.handle)
+            P.time_smoother(dtype="fp64" if code == L.TPS_F64 else "fp32", sweeps=2)
+            ms = P.time_smoother(dtype="fp64" if code == L.TPS_F64 else "fp32", sweeps=10)
+            total, _ = smoother_bytes(dim, k, n, 8 if code == L.TPS_F64 else 4)
+            rows.append({"name": f"Smooth {dtname} ppb={ppb[v]}", "ms": ms, "dof_per_s": N / (ms * 1e-3),
+                         "GBps": total / (ms * 1e-3) / 1e9})
+        L.check(L.lib().tps_set_smoother_variant(P.handle, code, lf, 0), P.handle)
+    if dim == 3 and k >= 2:
+        P.time_smoother(dtype="tf32", sweeps=2)
+        ms = P.time_smoother(dtype="tf32", sweeps=10)
+        total, _ = smoother_bytes(dim, k, n, 4)
+        rows.append({"name": "Smooth TF32 tensor cores", "ms": ms, "dof_per_s": N / (ms * 1e-3),
+                     "GBps": total / (ms * 1e-3) / 1e9})
+    print(json.dumps({"mode": "micro", "workload": args.workload, "dofs": N, "rows": rows}), flush=True)
+    P.close()
+
+
 def batch_systems(seed: int = 0):
     """Batched workload: 32 right-hand sides on one 32^3 Q3 mesh plus 12
     independent Q3 meshes with 8..48 cells per direction drawn from the seed
@@ -388,6 +457,9 @@ def main():
         return
     if args.mode == "batch":
         run_batch(args)
+        return
+    if args.mode == "micro":
+        run_micro(args)
         return
     if args.mode == "adjoint":
         run_adjoint(args)

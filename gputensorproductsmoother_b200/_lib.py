@@ -78,6 +78,8 @@ SIGNATURES = [
     ("tps_fmg", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP), ctypes.POINTER(_VP), _VP,
                                ctypes.POINTER(TpsReport), _VP]),
     ("tps_autotune", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("tps_smoother_variants", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("tps_set_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("tps_batch_destroy", ctypes.c_int, [_VP]),
     ("tps_batch_last_error", ctypes.c_char_p, [_VP]),

@@ -72,19 +72,39 @@ __global__ void copy_d_kernel(double *dst, const double *src, int64_t n, int rou
 template <typename T>
 __global__ void copy_boundary_kernel(T *dst, const T *src, int dim, int N1)
 {
-  // one thread per row (y, z) of N1 entries
-  const int64_t rows = dim == 3 ? static_cast<int64_t>(N1) * N1 : N1;
-  const int64_t r = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
-  if (r >= rows) return;
-  const int y = static_cast<int>(r % N1), z = dim == 3 ? static_cast<int>(r / N1) : 0;
-  const bool full = y == 0 || y == N1 - 1 || (dim == 3 && (z == 0 || z == N1 - 1));
-  const int64_t base = r * N1;
-  if (full) {
-    for (int x = 0; x < N1; ++x) dst[base + x] = src[base + x];
+  // one thread per boundary entry, in three coalesced groups (3D): the z = 0
+  // and z = N1-1 planes, the y = 0 and y = N1-1 rows of the other planes, and
+  // the x = 0 and x = N1-1 ends of the remaining rows (2D: the y rows, then
+  // the x ends)
+  const int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
+  const int64_t n1 = N1, m = N1 - 2;
+  int64_t idx;
+  if (dim == 3) {
+    const int64_t g0 = 2 * n1 * n1, g1 = 2 * m * n1, g2 = 2 * m * m;
+    if (i < g0) {
+      const int64_t f = i / (n1 * n1), r = i % (n1 * n1);
+      idx = (f ? (n1 - 1) * n1 * n1 : 0) + r;
+    } else if (i < g0 + g1) {
+      const int64_t j = i - g0, z = 1 + j / (2 * n1), r = j % (2 * n1);
+      idx = z * n1 * n1 + (r / n1 ? (n1 - 1) * n1 : 0) + r % n1;
+    } else if (i < g0 + g1 + g2) {
+      const int64_t j = i - g0 - g1, z = 1 + j / (2 * m), r = j % (2 * m);
+      idx = z * n1 * n1 + (1 + r / 2) * n1 + (r & 1 ? n1 - 1 : 0);
+    } else {
+      return;
+    }
   } else {
-    dst[base] = src[base];
-    dst[base + N1 - 1] = src[base + N1 - 1];
+    const int64_t g0 = 2 * n1, g1 = 2 * m;
+    if (i < g0) {
+      idx = (i / n1 ? (n1 - 1) * n1 : 0) + i % n1;
+    } else if (i < g0 + g1) {
+      const int64_t j = i - g0;
+      idx = (1 + j / 2) * n1 + (j & 1 ? n1 - 1 : 0);
+    } else {
+      return;
+    }
   }
+  dst[idx] = src[idx];
 }
 
 __global__ void __launch_bounds__(kRedThreads)
@@ -323,8 +343,9 @@ cudaError_t launch_copy_f64(double *dst, const double *src, int64_t n, int round
 cudaError_t launch_copy_boundary(void *dst, const void *src, int dim, int N1, int elem_bytes,
                                  cudaStream_t s)
 {
-  const int64_t rows = dim == 3 ? static_cast<int64_t>(N1) * N1 : N1;
-  const unsigned g = static_cast<unsigned>((rows + 255) / 256);
+  const int64_t n1 = N1, m = N1 - 2;
+  const int64_t count = dim == 3 ? 2 * n1 * n1 + 2 * m * n1 + 2 * m * m : 2 * n1 + 2 * m;
+  const unsigned g = static_cast<unsigned>((count + 255) / 256);
   if (elem_bytes == 8)
     copy_boundary_kernel<double><<<g, 256, 0, s>>>(static_cast<double *>(dst),
                                                    static_cast<const double *>(src), dim, N1);

@@ -96,8 +96,15 @@ cudaError_t set_attributes()
   TPS_SET((smoother3d_kernel<K, T, false, sm3_variant_ppb<K, T, 0>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 0>()>::BYTES));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Vmult>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Residual>), (laplace_smem<2, T>()));
-  TPS_SET((laplace_kernel<3, K, T, OpMode::Vmult>), (laplace_smem<3, T>()));
-  TPS_SET((laplace_kernel<3, K, T, OpMode::Residual>), (laplace_smem<3, T>()));
+  TPS_SET((laplace3d_stream_kernel<K, T, OpMode::Vmult>), (sizeof(T) * OpStream<K, T>::ELEMS));
+  TPS_SET((laplace3d_stream_kernel<K, T, OpMode::Residual>), (sizeof(T) * OpStream<K, T>::ELEMS));
+  // the streaming operator is shared-memory heavy: prefer the largest carveout
+  e = cudaFuncSetAttribute(laplace3d_stream_kernel<K, T, OpMode::Vmult>,
+                           cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(laplace3d_stream_kernel<K, T, OpMode::Residual>,
+                           cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+  if (e != cudaSuccess) return e;
   TPS_SET((restrict_xy_kernel<K, T, XYOut::AddInterior>), (restrict_smem<T>()));
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetInterior>), (restrict_smem<T>()));
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetAll>), (restrict_smem<T>()));
@@ -123,17 +130,30 @@ template <int DIM, typename T>
 cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const void *src,
                     const void *rhs, int mode, cudaStream_t s)
 {
-  using Tl = OpTile<DIM, K>;
-  const dim3 grid(ceil_div(g.n, Tl::CX), ceil_div(g.n, Tl::CY), DIM == 3 ? ceil_div(g.n, Tl::CZ) : 1);
   const T scale = static_cast<T>(stiffness_scale(DIM, g.h));
-  const size_t smem = laplace_smem<DIM, T>();
-  if (mode == 0)
-    laplace_kernel<DIM, K, T, OpMode::Vmult><<<grid, Tl::NT, smem, s>>>(
-        static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, l.sy, l.sz, scale);
-  else
-    laplace_kernel<DIM, K, T, OpMode::Residual><<<grid, Tl::NT, smem, s>>>(
-        static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1,
-        l.sy, l.sz, scale);
+  if constexpr (DIM == 3) {
+    using Sz = OpStream<K, T>;
+    const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, Sz::CZ));
+    const size_t smem = sizeof(T) * Sz::ELEMS;
+    if (mode == 0)
+      laplace3d_stream_kernel<K, T, OpMode::Vmult><<<grid, Sz::NT, smem, s>>>(
+          static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, l.sy, l.sz, scale);
+    else
+      laplace3d_stream_kernel<K, T, OpMode::Residual><<<grid, Sz::NT, smem, s>>>(
+          static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1, g.n, l.sy,
+          l.sz, scale);
+  } else {
+    using Tl = OpTile<DIM, K>;
+    const dim3 grid(ceil_div(g.n, Tl::CX), ceil_div(g.n, Tl::CY), 1);
+    const size_t smem = laplace_smem<DIM, T>();
+    if (mode == 0)
+      laplace_kernel<DIM, K, T, OpMode::Vmult><<<grid, Tl::NT, smem, s>>>(
+          static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, l.sy, l.sz, scale);
+    else
+      laplace_kernel<DIM, K, T, OpMode::Residual><<<grid, Tl::NT, smem, s>>>(
+          static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1,
+          l.sy, l.sz, scale);
+  }
   return cudaGetLastError();
 }
 

@@ -1181,6 +1181,26 @@ int tps_cell_energy(tps_handle *h, const double *u, const double *lam, double *e
   });
 }
 
+int tps_smoother_variants(tps_handle *h, int dtype, int *ppb)
+{
+  return guarded(h, [&] {
+    const int p = dt_index(dtype);
+    if (!ppb) throw ApiError(TPS_ERR_INVALID, "null output");
+    for (int v = 0; v < kSmootherVariants; ++v) ppb[v] = h->kt->smoother_ppb(h->dim, p == 0 ? 0 : 1, v);
+  });
+}
+
+int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant)
+{
+  return guarded(h, [&] {
+    const int p = dt_index(dtype);
+    check_level(h, level);
+    if (variant < 0 || variant >= kSmootherVariants) throw ApiError(TPS_ERR_INVALID, "variant out of range");
+    if (static_cast<int>(h->sm_variant[p].size()) != h->n_levels) h->sm_variant[p].assign(h->n_levels, 0);
+    h->sm_variant[p][level] = variant;
+  });
+}
+
 int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level)
 {
   return guarded(h, [&] {

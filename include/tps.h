@@ -188,6 +188,10 @@ int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_ho
  * ppb_per_level (n_levels entries, may be null) receives the chosen values
  * (0 in 2D).  Batched solves tune their systems automatically. */
 int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
+/* The compiled patches-per-block variants of the 3D smoother (3 entries; 0 in
+ * 2D) and the explicit choice of one for a level (what tps_autotune sets). */
+int tps_smoother_variants(tps_handle *h, int dtype, int *ppb);
+int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant);
 
 /* ---- batched solves (no reference counterpart) ----------------------------
  * A batch owns n independent systems (1 <= n <= 256): right-hand sides of one
