@@ -21,10 +21,11 @@
 //  * contractions: z (M, L) -> y (3 products) -> x (2 products) + S^T_x ->
 //    S^T_y -> S^T_z, scale, S_z -> S_x -> S_y + store.  Every contraction keeps
 //    one 1D line per thread in registers and applies the centro-symmetric 1D
-//    matrices in even/odd folded form; the even and odd partial sums of an
-//    output pair travel together through one packed FP32x2 FMA (__ffma2_rn),
-//    so a folded contraction costs about a quarter of the dense FMA
-//    instructions; coefficients are constant-bank data;
+//    matrices in even/odd folded form (about half the dense multiply-adds)
+//    with scalar FMAs whose coefficients are constant-bank operands.  A
+//    packed FP32x2 form (__ffma2_rn on (even, odd) pairs, TPS_SM3_PACKED=1)
+//    halves the FMA count but needs a constant load per coefficient pair; it
+//    measured within 1.5 % of the scalar form, which is the default;
 //  * per-batch patch offsets are computed once into shared memory; the
 //    thread count matches the widest stage (the y stage), and the cheap
 //    interior z-lines are processed two per thread;
@@ -116,6 +117,30 @@ __device__ __forceinline__ void fold_rows2(const typename Pair<T>::type *fp, con
   out[K - 1] = sc;
 }
 
+// The same rows with scalar FMAs: every coefficient is a constant-bank
+// operand of its FMA (the packed pairs above need a constant load per pair).
+template <int K, typename T>
+__device__ __forceinline__ void fold_rows_s(const T *fe, const T *fo, const typename Pair<T>::type (&eo)[K > 1 ? K : 1],
+                                            const T ec, T (&out)[2 * K - 1])
+{
+  constexpr int M = 2 * K - 1;
+#pragma unroll
+  for (int r = 0; r < K - 1; ++r) {
+    T e = fe[r * (K + 1) + K] * ec, o = T(0);
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      e += fe[r * (K + 1) + j] * eo[j].x;
+      o += fo[r * K + j] * eo[j].y;
+    }
+    out[r] = e + o;
+    out[M - 1 - r] = e - o;
+  }
+  T sc = fe[(K - 1) * (K + 1) + K] * ec;
+#pragma unroll
+  for (int j = 0; j < K; ++j) sc += fe[(K - 1) * (K + 1) + j] * eo[j].x;
+  out[K - 1] = sc;
+}
+
 // Fast-diagonalization factor S (eigenvectors as columns; modes 0..k-1 even,
 // k..2k-2 odd) or its transpose applied to a line of 2k-1 values, with packed
 // (even, odd) pairs.
@@ -167,6 +192,80 @@ constexpr int sm3_variant_ppb()
   if constexpr (V == 1) return P > 1 ? P / 2 : P;
   else if constexpr (V == 2) return Sm3<K, T, 2 * P>::BYTES <= 232448 ? 2 * P : P;
   else return P;
+}
+
+// S or S^T with scalar FMAs (constant-bank coefficients)
+template <int K, typename T, bool TRANSPOSE>
+__device__ __forceinline__ void apply_evec_s(const T (&in)[2 * K - 1], T (&out)[2 * K - 1])
+{
+  constexpr int M = 2 * K - 1, C = K - 1;
+  const DegreeTables<K, T> &tb = c_tables<K, T>;
+  if constexpr (TRANSPOSE) {
+    T ev[C > 0 ? C : 1], od[C > 0 ? C : 1];
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+      ev[j] = in[j] + in[M - 1 - j];
+      od[j] = in[j] - in[M - 1 - j];
+    }
+    const T ec = in[C];
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      T e = tb.evec[C * M + q] * ec, o = T(0);
+#pragma unroll
+      for (int j = 0; j < C; ++j) {
+        e += tb.evec[j * M + q] * ev[j];
+        o += tb.evec[j * M + C + 1 + q] * od[j];
+      }
+      out[q] = e;
+      out[C + 1 + q] = o;
+    }
+    T sc = tb.evec[C * M + C] * ec;
+#pragma unroll
+    for (int j = 0; j < C; ++j) sc += tb.evec[j * M + C] * ev[j];
+    out[C] = sc;
+  } else {
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+      T e = tb.evec[i * M + C] * in[C], o = T(0);
+#pragma unroll
+      for (int q = 0; q < C; ++q) {
+        e += tb.evec[i * M + q] * in[q];
+        o += tb.evec[i * M + C + 1 + q] * in[C + 1 + q];
+      }
+      out[i] = e + o;
+      out[M - 1 - i] = e - o;
+    }
+    T sc = T(0);
+#pragma unroll
+    for (int q = 0; q <= C; ++q) sc += tb.evec[C * M + q] * in[q];
+    out[C] = sc;
+  }
+}
+
+#ifndef TPS_SM3_PACKED
+#define TPS_SM3_PACKED 0
+#endif
+template <int K, typename T>
+__device__ __forceinline__ void rows_mass(const typename Pair<T>::type (&eo)[K > 1 ? K : 1], const T ec,
+                                          T (&out)[2 * K - 1])
+{
+  const DegreeTables<K, T> &tb = c_tables<K, T>;
+  if constexpr (TPS_SM3_PACKED) rows_mass<K, T>(eo, ec, out);
+  else fold_rows_s<K, T>(tb.pmass_fe, tb.pmass_fo, eo, ec, out);
+}
+template <int K, typename T>
+__device__ __forceinline__ void rows_lap(const typename Pair<T>::type (&eo)[K > 1 ? K : 1], const T ec,
+                                         T (&out)[2 * K - 1])
+{
+  const DegreeTables<K, T> &tb = c_tables<K, T>;
+  if constexpr (TPS_SM3_PACKED) rows_lap<K, T>(eo, ec, out);
+  else fold_rows_s<K, T>(tb.plap_fe, tb.plap_fo, eo, ec, out);
+}
+template <int K, typename T, bool TRANSPOSE>
+__device__ __forceinline__ void evec_apply(const T (&in)[2 * K - 1], T (&out)[2 * K - 1])
+{
+  if constexpr (TPS_SM3_PACKED) apply_evec2<K, T, TRANSPOSE>(in, out);
+  else apply_evec_s<K, T, TRANSPOSE>(in, out);
 }
 
 struct Sm3Args {
@@ -350,8 +449,8 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
 #pragma unroll
           for (int z = 0; z < N1; ++z) v[z] = src[z * N1 * W];
           fold_pairs<K, T>(v, eo, ec);
-          fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo, ec, r1);
-          fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo, ec, r2);
+          rows_mass<K, T>(eo, ec, r1);
+          rows_lap<K, T>(eo, ec, r2);
           T *d1 = Z1 + lp * S::ZSZ + y * N1 + xx, *d2 = Z2 + lp * S::ZSZ + y * N1 + xx;
 #pragma unroll
           for (int i = 0; i < M; ++i) {
@@ -393,9 +492,9 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
         for (int j = 0; j < N1; ++j) v[j] = s2[j * N1];
         fold_pairs<K, T>(v, eo2, ec2);
         T ra[M], rb[M], rc[M];
-        fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo2, ec2, ra);
-        fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo1, ec1, rb);
-        fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo1, ec1, rc);
+        rows_mass<K, T>(eo2, ec2, ra);
+        rows_lap<K, T>(eo1, ec1, rb);
+        rows_mass<K, T>(eo1, ec1, rc);
         T *d1 = V1 + lp * VST + zi * M * N1 + xx, *d2 = V2 + lp * VST + zi * M * N1 + xx;
 #pragma unroll
         for (int i = 0; i < M; ++i) {
@@ -421,8 +520,8 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
         for (int j = 0; j < N1; ++j) v[j] = s2[j];
         fold_pairs<K, T>(v, eo2, ec2);
         T ra[M], rb[M];
-        fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo1, ec1, ra);
-        fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo2, ec2, rb);
+        rows_mass<K, T>(eo1, ec1, ra);
+        rows_lap<K, T>(eo2, ec2, rb);
 #pragma unroll
         for (int i = 0; i < M; ++i) res[i] = bb[i] - scale * (ra[i] + rb[i]);
       } else {
@@ -430,7 +529,7 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
         for (int i = 0; i < M; ++i) res[i] = bb[i];
       }
       T q[M];
-      apply_evec2<K, T, true>(res, q);
+      evec_apply<K, T, true>(res, q);
       T *d = Q1 + lp * S::QSZ + r * M;
 #pragma unroll
       for (int i = 0; i < M; ++i) d[i] = q[i];
@@ -444,7 +543,7 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j * M];
-      apply_evec2<K, T, true>(v, q);
+      evec_apply<K, T, true>(v, q);
       T *d = Q2 + lp * S::QSZ + zi * M * M + qx;
 #pragma unroll
       for (int j = 0; j < M; ++j) d[j * M] = q[j];
@@ -457,10 +556,10 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j * M * M];
-      apply_evec2<K, T, true>(v, q);
+      evec_apply<K, T, true>(v, q);
 #pragma unroll
       for (int j = 0; j < M; ++j) q[j] *= RL[j * M * M + r];
-      apply_evec2<K, T, false>(q, v);
+      evec_apply<K, T, false>(q, v);
       T *d = Q1 + lp * S::QSZ + r;
 #pragma unroll
       for (int j = 0; j < M; ++j) d[j * M * M] = v[j];
@@ -473,7 +572,7 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j];
-      apply_evec2<K, T, false>(v, q);
+      evec_apply<K, T, false>(v, q);
       T *d = Q2 + lp * S::QSZ + r * M;
 #pragma unroll
       for (int j = 0; j < M; ++j) d[j] = q[j];
@@ -487,7 +586,7 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
       T v[M], q[M];
 #pragma unroll
       for (int j = 0; j < M; ++j) v[j] = s[j * M];
-      apply_evec2<K, T, false>(v, q);
+      evec_apply<K, T, false>(v, q);
       const int64_t base = s_base[lp];
       if (base >= 0) {
         T *dst = x + base + xx + z * a.sz;
