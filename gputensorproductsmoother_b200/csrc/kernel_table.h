@@ -37,7 +37,7 @@ struct SmootherMaps {
   int tc_valid = 0;
 };
 
-// compiled patches-per-batch variants of the 3D smoother (default, half, double)
+// compiled patches-per-batch variants of the 3D smoother (default, half, quarter)
 constexpr int kSmootherVariants = 3;
 
 struct KernelTable {
@@ -50,7 +50,7 @@ struct KernelTable {
                                const void *rhs, int mode, cudaStream_t);
   // one colour of the patch sweep; maps (3D, TMA path) may be null; zero_x
   // declares x == 0 on entry; variant selects the 3D patches-per-batch
-  // (0 default, 1 half, 2 double; see smoother_ppb); err receives 1 if a
+  // (0 default, 1 half, 2 quarter; see smoother_ppb); err receives 1 if a
   // bounded wait gave up
   cudaError_t (*smoother[2][2])(const LevelGeomH &, const VecLayout &, void *x, const void *b,
                                 int colour, double omega, int zero_x, int variant,

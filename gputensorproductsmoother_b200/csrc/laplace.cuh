@@ -220,6 +220,9 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT, 2)
 // three directions.  The next layer's k input planes are loaded into
 // registers while the current layer is contracted; each thread's staged xy
 // offsets are computed once, so a prefetched entry costs one add and a load.
+#ifndef TPS_OPSTREAM_MINB
+#define TPS_OPSTREAM_MINB(K) 1  // a register cap for more CTAs per SM measured slower (spills)
+#endif
 template <int K, typename T>
 struct OpStream {
   static constexpr int TX = K == 1 ? 16 : K == 2 ? 8 : K <= 4 ? 4 : K == 5 ? 3 : 2, TY = TX;  // cells per CTA in x, y
@@ -235,10 +238,11 @@ struct OpStream {
   static constexpr int OFF_T2 = OFF_T1 + (K + 1) * TS;
   static constexpr int ELEMS = OFF_T2 + (K + 1) * TS;
   static constexpr int EPT = (PL + NT - 1) / NT;      // staged xy entries per thread and plane
+  static constexpr int MINB = TPS_OPSTREAM_MINB(K);    // CTAs per SM the registers must allow
 };
 
 template <int K, typename T, OpMode MODE>
-__global__ void __launch_bounds__(OpStream<K, T>::NT)
+__global__ void __launch_bounds__(OpStream<K, T>::NT, OpStream<K, T>::MINB)
     laplace3d_stream_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs,
                             int N1g, int n_cells, int64_t sy, int64_t sz, T scale)
 {

@@ -70,7 +70,7 @@ struct Sm3 {
   static constexpr int PPB = PPB_ > 0 ? PPB_ : sm3_default_ppb<K, T>();
   // threads = widest stage (y lines), rounded to warps
   static constexpr int NT_RAW = (PPB * M * N1 + 31) / 32 * 32;
-  static constexpr int NT = NT_RAW < 128 ? 128 : NT_RAW;
+  static constexpr int NT = NT_RAW < 64 ? 64 : NT_RAW;
   // shared memory layout (elements of T): 2 stages | Z1 | Z2 | 1/(lambda sums)
   static constexpr int OFF_Z1 = 2 * PPB * STAGE;
   static constexpr int OFF_Z2 = OFF_Z1 + PPB * ZSZ;
@@ -183,14 +183,14 @@ __device__ __forceinline__ void apply_evec2(const T (&in)[2 * K - 1], T (&out)[2
   }
 }
 
-// patches per batch of autotuner variant v: 0 the default P, 1 P/2, 2 2P
-// (variants that would not fit in shared memory fall back to P)
+// patches per batch of autotuner variant v: 0 the default P, 1 P/2, 2 P/4
+// (at least one patch; larger batches than P measured slower everywhere)
 template <int K, typename T, int V>
 constexpr int sm3_variant_ppb()
 {
   constexpr int P = sm3_default_ppb<K, T>();
   if constexpr (V == 1) return P > 1 ? P / 2 : P;
-  else if constexpr (V == 2) return Sm3<K, T, 2 * P>::BYTES <= 232448 ? 2 * P : P;
+  else if constexpr (V == 2) return P > 3 ? P / 4 : P;
   else return P;
 }
 
