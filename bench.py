@@ -328,6 +328,23 @@ def run_micro(args):
     P.close()
 
 
+def max_over_ranks(values, world: int, device: str = "cuda"):
+    """Element-wise maximum of per-rank timings over the process group (the
+    whole job is as slow as its slowest rank); identity for one rank."""
+    import torch
+    t = torch.tensor(list(values), dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return t.tolist()
+
+
+def job_throughput(world: int, units_per_rank: float, ms: float) -> float:
+    """Whole-job units per second: every rank solves its own instance of
+    `units_per_rank` units, the job takes the slowest rank's `ms`."""
+    return world * units_per_rank / (ms * 1e-3)
+
+
 def batch_systems(seed: int = 0):
     """Batched workload: 32 right-hand sides on one 32^3 Q3 mesh plus 12
     independent Q3 meshes with 8..48 cells per direction drawn from the seed
@@ -559,10 +576,7 @@ def main():
         torch.cuda.synchronize()
         e2e_ms = 1000 * (time.perf_counter() - t0) / ne2e
 
-    t = torch.tensor([ms, ms64, e2e_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms, ms64, e2e_ms = t.tolist()
+    ms, ms64, e2e_ms = max_over_ranks([ms, ms64, e2e_ms], world)
     peaks = {}
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -572,7 +586,7 @@ def main():
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
     line = {
-        "metric": METRIC, "value": world * nint / (ms * 1e-3), "unit": "DoF/s", "n_gpus": world,
+        "metric": METRIC, "value": job_throughput(world, nint, ms), "unit": "DoF/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 V-cycle / f64 CG",
         "data": "synthetic (seeded sin-mode RHS per rank)",
@@ -581,14 +595,19 @@ def main():
                    "rel_tol": 1e-10, "parallelism": f"replicas x{world}",
                    "l2": "vectors (136 MB FP64) larger than L2; no flush"},
         "iterations": rep.iterations, "final_rel_residual": resid_check,
-        "fp64": {"ms_per_step": ms64, "value": world * nint / (ms64 * 1e-3),
+        "fp64": {"ms_per_step": ms64, "value": job_throughput(world, nint, ms64),
                  "iterations": rep64.iterations},
         "mixed_speedup_vs_fp64": ms64 / ms,
         "error_vs_fp64_solve": err,
-        "e2e": {"value": world * nint / (e2e_ms * 1e-3), "unit": "DoF/s",
+        "e2e": {"value": job_throughput(world, nint, e2e_ms), "unit": "DoF/s",
                 "h2d_bytes_per_step": 2 * 8 * P.n_dofs(), "d2h_bytes_per_step": 8 * P.n_dofs()},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                     "frac": achieved / hbm_peak, "traffic": None,
+                     "frac": achieved / hbm_peak,
+                     # DRAM bytes of one launch from the ncu capture of the colour-0 launch
+                     # (dram__bytes_read + write = 136.6 MB for 167.5 MB algorithmic),
+                     # scaled to the average launch by its algorithmic bytes
+                     "traffic": (136.6e6 * launch_bytes / 167.5e6) if args.workload == "poisson3d_q4_64" else None,
+                     "traffic_unit": "bytes per launch",
                      "kernel": "smoother3d_kernel<4,float,TMA>",
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": launch_bytes, "launch_ms": launch_ms},
