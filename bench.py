@@ -45,6 +45,9 @@ def parse():
                     help="smoother / operator: only time the finest-level smoother "
                          "sweeps / FP64 operator applications (small commands for kernel "
                          "profiling)")
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="--mode smoother: 3D smoother variant (0-2 CTA batches P, P/2, P/4; 3 one warp "
+                         "per patch; -1 the library default)")
     ap.add_argument("--smoother", default="fp32", choices=["fp32", "tf32", "fp64"],
                     help="--mode smoother: FP32 SIMT kernel, tensor-core (TF32) kernel or FP64")
     ap.add_argument("--directions", type=int, default=64,
@@ -92,12 +95,15 @@ def run_smoother_only(args):
     sp = ctypes.c_void_p(stream.cuda_stream)
     ms = ctypes.c_double()
     code = {"fp32": L.TPS_F32, "tf32": L.TPS_TF32, "fp64": L.TPS_F64}[args.smoother]
+    if args.variant >= 0 and args.smoother != "tf32":
+        P.set_smoother_variant(args.variant, args.smoother, lf)
     if args.warmup > 0:
         L.check(L.lib().tps_time_smoother(P.handle, lf, code, args.warmup, ctypes.byref(ms), sp), P.handle)
     L.check(L.lib().tps_time_smoother(P.handle, lf, code, max(args.steps, 1), ctypes.byref(ms), sp), P.handle)
     total, per = smoother_bytes(dim, k, n, 8 if args.smoother == "fp64" else 4)
+    variant = P.smoother_variant(lf, args.smoother) if args.smoother != "tf32" else None
     print(json.dumps({"mode": "smoother", "smoother": args.smoother, "workload": args.workload,
-                      "ms_per_sweep": ms.value, "algorithmic_GBps": total / (ms.value * 1e-3) / 1e9}),
+                      "variant": variant, "ms_per_sweep": ms.value, "algorithmic_GBps": total / (ms.value * 1e-3) / 1e9}),
           flush=True)
     P.close()
 
@@ -304,10 +310,10 @@ def run_micro(args):
         ms = best(lambda: T.restrict_and_add(lf, coarse, fine))
         rows.append({"name": f"Restriction {name}", "ms": ms, "dof_per_s": N / (ms * 1e-3)})
     for dtname, code in (("DP", L.TPS_F64), ("SP", L.TPS_F32)):
-        ppb = (ctypes.c_int * 3)()
+        ppb = (ctypes.c_int * L.SMOOTHER_VARIANTS)()
         L.check(L.lib().tps_smoother_variants(P.handle, code, ppb), P.handle)
         seen = set()
-        for v in range(3):
+        for v in range(L.SMOOTHER_VARIANTS):
             if ppb[v] in seen:
                 continue
             seen.add(ppb[v])
@@ -315,7 +321,8 @@ def run_micro(args):
             P.time_smoother(dtype="fp64" if code == L.TPS_F64 else "fp32", sweeps=2)
             ms = P.time_smoother(dtype="fp64" if code == L.TPS_F64 else "fp32", sweeps=10)
             total, _ = smoother_bytes(dim, k, n, 8 if code == L.TPS_F64 else 4)
-            rows.append({"name": f"Smooth {dtname} ppb={ppb[v]}", "ms": ms, "dof_per_s": N / (ms * 1e-3),
+            label = "warp/patch" if ppb[v] == -1 else f"ppb={ppb[v]}"
+            rows.append({"name": f"Smooth {dtname} {label}", "ms": ms, "dof_per_s": N / (ms * 1e-3),
                          "GBps": total / (ms * 1e-3) / 1e9})
         L.check(L.lib().tps_set_smoother_variant(P.handle, code, lf, 0), P.handle)
     if dim == 3 and k >= 2:
@@ -551,6 +558,8 @@ def main():
         L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, 3, ctypes.byref(msw), sp), P.handle)
         L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, 20, ctypes.byref(msw), sp), P.handle)
         sweep_ms = msw.value
+        kernel_name = (f"smoother3d_warp_kernel<{k},float>" if P.smoother_variant(lf, "fp32") == 3
+                       else f"smoother3d_kernel<{k},float,TMA>")
         bytes_sweep, per_colour = smoother_bytes(dim, k, n, 4)
         colours = sum(1 for c in per_colour if c > 0)
         launch_ms = sweep_ms / colours
@@ -608,7 +617,7 @@ def main():
                      # scaled to the average launch by its algorithmic bytes
                      "traffic": (136.6e6 * launch_bytes / 167.5e6) if args.workload == "poisson3d_q4_64" else None,
                      "traffic_unit": "bytes per launch",
-                     "kernel": "smoother3d_kernel<4,float,TMA>",
+                     "kernel": kernel_name,
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": launch_bytes, "launch_ms": launch_ms},
         "gpu_launches": args.steps * launches_per_solve(dim, P.n_levels, rep.iterations),

@@ -20,6 +20,7 @@ STATUS_NAMES = {
 TPS_F64, TPS_F32, TPS_TF32 = 0, 1, 2
 VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32 = 0, 1, 2, 3
 DRIVER_CG, DRIVER_GMRES = 0, 1
+SMOOTHER_VARIANTS = 4  # TPS_SMOOTHER_VARIANTS
 MAX_HISTORY = 256
 
 
@@ -80,6 +81,7 @@ SIGNATURES = [
     ("tps_autotune", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_smoother_variants", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_set_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("tps_get_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("tps_batch_destroy", ctypes.c_int, [_VP]),
     ("tps_batch_last_error", ctypes.c_char_p, [_VP]),

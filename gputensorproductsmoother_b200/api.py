@@ -104,12 +104,36 @@ class PoissonProblem:
         return ms.value
 
     def autotune(self, dtype: str = "fp32") -> list[int]:
-        """Time the 3D smoother's patches-per-batch variants on every level and
-        keep the fastest; returns the chosen patches per batch per level."""
+        """Time the 3D smoother's kernel variants on every level and keep the
+        fastest; returns the chosen patches per batch per level (-1: the
+        one-warp-per-patch kernel)."""
         out = (ctypes.c_int * self.n_levels)()
         L.check(L.lib().tps_autotune(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], out),
                 self.handle)
         return list(out)
+
+    def smoother_variants(self, dtype: str = "fp32") -> list[int]:
+        """Patches per batch of each compiled 3D smoother variant (index =
+        variant; -1: one warp per patch; 0 in 2D)."""
+        out = (ctypes.c_int * L.SMOOTHER_VARIANTS)()
+        L.check(L.lib().tps_smoother_variants(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], out),
+                self.handle)
+        return list(out)
+
+    def smoother_variant(self, level: int | None = None, dtype: str = "fp32") -> int:
+        """The 3D smoother variant the level's sweeps use now (set, autotuned
+        or the library default)."""
+        v = ctypes.c_int()
+        lv = self.n_levels - 1 if level is None else level
+        L.check(L.lib().tps_get_smoother_variant(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], lv,
+                                                 ctypes.byref(v)), self.handle)
+        return v.value
+
+    def set_smoother_variant(self, variant: int, dtype: str = "fp32", level: int | None = None) -> None:
+        """Use smoother variant `variant` on one level (all levels if None)."""
+        code = {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype]
+        for lv in range(self.n_levels) if level is None else [level]:
+            L.check(L.lib().tps_set_smoother_variant(self.handle, code, lv, variant), self.handle)
 
     def mass_vmult(self, dst: torch.Tensor, src: torch.Tensor) -> None:
         """dst = M src (finest level, all rows, FP64)."""

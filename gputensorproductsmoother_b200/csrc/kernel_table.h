@@ -37,8 +37,9 @@ struct SmootherMaps {
   int tc_valid = 0;
 };
 
-// compiled patches-per-batch variants of the 3D smoother (default, half, quarter)
-constexpr int kSmootherVariants = 3;
+// compiled variants of the 3D smoother: patches per CTA batch default, half,
+// quarter, and one warp per patch
+constexpr int kSmootherVariants = 4;
 
 struct KernelTable {
   int degree;
@@ -49,8 +50,9 @@ struct KernelTable {
   cudaError_t (*laplace[2][2])(const LevelGeomH &, const VecLayout &, void *dst, const void *src,
                                const void *rhs, int mode, cudaStream_t);
   // one colour of the patch sweep; maps (3D, TMA path) may be null; zero_x
-  // declares x == 0 on entry; variant selects the 3D patches-per-batch
-  // (0 default, 1 half, 2 quarter; see smoother_ppb); err receives 1 if a
+  // declares x == 0 on entry; variant selects the 3D kernel shape
+  // (0 default, 1 half, 2 quarter batch, 3 one warp per patch; see
+  // smoother_ppb); err receives 1 if a
   // bounded wait gave up
   cudaError_t (*smoother[2][2])(const LevelGeomH &, const VecLayout &, void *x, const void *b,
                                 int colour, double omega, int zero_x, int variant,
@@ -83,7 +85,8 @@ struct KernelTable {
                              double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t);
   // the rank-4 TMA views of FP32 x and b (sets tc_valid when the layout allows them)
   cudaError_t (*encode_tc_maps)(const VecLayout &l, void *x, const void *b, SmootherMaps *out);
-  // patches per CTA batch of smoother variant v (dtype 0 FP64, 1 FP32; 0 in 2D)
+  // patches per CTA batch of smoother variant v (dtype 0 FP64, 1 FP32; 0 in
+  // 2D; -1 for the one-warp-per-patch kernel)
   int (*smoother_ppb)(int dim, int dtype, int variant);
   // FP64 fine += P coarse with the coarse boundary values used ([dim - 2])
   cudaError_t (*prolong_nb[2])(const LevelGeomH &coarse, const VecLayout &lc, const VecLayout &lf,

@@ -11,6 +11,7 @@
 #include "smoother.cuh"
 #include "smoother3d.cuh"
 #include "smoother3d_tc.cuh"
+#include "smoother3d_warp.cuh"
 #include "transfer.cuh"
 
 namespace tps {
@@ -94,6 +95,8 @@ cudaError_t set_attributes()
   TPS_SET((smoother3d_kernel<K, T, true, sm3_variant_ppb<K, T, 1>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 1>()>::BYTES));
   TPS_SET((smoother3d_kernel<K, T, true, sm3_variant_ppb<K, T, 2>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 2>()>::BYTES));
   TPS_SET((smoother3d_kernel<K, T, false, sm3_variant_ppb<K, T, 0>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 0>()>::BYTES));
+  if constexpr (wp3_enabled<K, T>())
+    TPS_SET((smoother3d_warp_kernel<K, T, wp3_warps<K, T>()>), (Wp3<K, T, wp3_warps<K, T>()>::BYTES));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Vmult>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Residual>), (laplace_smem<2, T>()));
   TPS_SET((laplace3d_stream_kernel<K, T, OpMode::Vmult>), (sizeof(T) * OpStream<K, T>::ELEMS));
@@ -196,12 +199,41 @@ void smoother3d_launch(Sm3Args a, const SmootherMaps *maps, void *x, const void 
   }
 }
 
-// patches per batch of a 3D variant (0 in 2D: one fixed kernel shape)
+// one colour with one warp per patch (TMA views required): a persistent grid
+// of the CTAs resident per SM x SMs, capped by the patch count
+template <typename T>
+void smoother3d_warp_launch(const Sm3Args &a, const SmootherMaps *maps, void *x, T scale, T fd, int *err,
+                            cudaStream_t s)
+{
+  if constexpr (wp3_enabled<K, T>()) {
+    constexpr int WA = wp3_warps<K, T>();
+    using S = Wp3<K, T, WA>;
+    static int per_sm = -1, n_sm = 0;
+    if (per_sm < 0) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_warp_kernel<K, T, WA>, S::NT,
+                                                        S::BYTES) != cudaSuccess ||
+          per_sm < 1)
+        per_sm = 1;
+    }
+    const int need = static_cast<int>(ceil_div(a.n_patches, WA));
+    const int grid = need < per_sm * n_sm ? need : per_sm * n_sm;
+    smoother3d_warp_kernel<K, T, WA><<<grid, S::NT, S::BYTES, s>>>(
+        *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),
+        static_cast<T *>(x), a, scale, fd, err);
+  }
+}
+
+// patches per batch of a 3D variant (0 in 2D: one fixed kernel shape; -1:
+// the one-warp-per-patch kernel, variant 3, where it is compiled)
 int smoother_ppb(int dim, int dtype, int variant)
 {
   if (dim != 3) return 0;
   auto pick = [&](auto tag) -> int {
     using T = decltype(tag);
+    if (variant == 3) return wp3_enabled<K, T>() ? -1 : sm3_variant_ppb<K, T, 0>();
     return variant == 1 ? sm3_variant_ppb<K, T, 1>() : variant == 2 ? sm3_variant_ppb<K, T, 2>()
                                                                         : sm3_variant_ppb<K, T, 0>();
   };
@@ -236,8 +268,12 @@ cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const voi
     a.zero_x = zero_x;
     a.sy = l.sy;
     a.sz = l.sz;
+    magic_div(static_cast<uint32_t>(nx), a.mx, a.sx);
+    magic_div(static_cast<uint32_t>(nx) * static_cast<uint32_t>(ny), a.mxy, a.sxy);
     const T scale = static_cast<T>(sc), fd = static_cast<T>(omega / sc);
-    if (variant == 1)
+    if (variant == 3 && wp3_enabled<K, T>() && maps && maps->valid)
+      smoother3d_warp_launch<T>(a, maps, x, scale, fd, err, s);
+    else if (variant == 1)
       smoother3d_launch<T, sm3_variant_ppb<K, T, 1>()>(a, maps, x, b, scale, fd, err, s);
     else if (variant == 2)
       smoother3d_launch<T, sm3_variant_ppb<K, T, 2>()>(a, maps, x, b, scale, fd, err, s);
@@ -291,6 +327,8 @@ cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const 
     a.zero_x = zero_x;
     a.sy = l.sy;
     a.sz = l.sz;
+    magic_div(static_cast<uint32_t>(nx), a.mx, a.sx);
+    magic_div(static_cast<uint32_t>(nx) * static_cast<uint32_t>(ny), a.mxy, a.sxy);
     smoother3d_tc_kernel<K><<<tc_grid(static_cast<int>(ceil_div(count, C::U))), C::NT, C::BYTES, s>>>(
         *reinterpret_cast<const CUtensorMap *>(maps->tx), *reinterpret_cast<const CUtensorMap *>(maps->tb),
         static_cast<float *>(x), a, static_cast<float>(sc), static_cast<float>(omega / sc), err);

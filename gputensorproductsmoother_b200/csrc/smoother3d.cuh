@@ -25,7 +25,10 @@
 //    with scalar FMAs whose coefficients are constant-bank operands.  A
 //    packed FP32x2 form (__ffma2_rn on (even, odd) pairs, TPS_SM3_PACKED=1)
 //    halves the FMA count but needs a constant load per coefficient pair; it
-//    measured within 1.5 % of the scalar form, which is the default;
+//    measured within 1.5 % of the scalar form, which is the default.  The
+//    sums of two products (M_y Z2 + L_y Z1, M_x V1 + L_x V2) run as one
+//    accumulation chain, and every kernel variant uses the same chains, so
+//    the variants give bit-identical sweeps;
 //  * per-batch patch offsets are computed once into shared memory; the
 //    thread count matches the widest stage (the y stage), and the cheap
 //    interior z-lines are processed two per thread;
@@ -141,6 +144,72 @@ __device__ __forceinline__ void fold_rows_s(const T *fe, const T *fo, const type
   out[K - 1] = sc;
 }
 
+// interior rows of A u + B v for two centro-symmetric patch matrices from
+// folded inputs: one accumulation chain per even/odd partial sum, so the sum
+// costs no more combining adds than a single product
+template <int K, typename T>
+__device__ __forceinline__ void fold_rows_sum_s(const T *fea, const T *foa,
+                                                const typename Pair<T>::type (&eoa)[K > 1 ? K : 1], const T eca,
+                                                const T *feb, const T *fob,
+                                                const typename Pair<T>::type (&eob)[K > 1 ? K : 1], const T ecb,
+                                                T (&out)[2 * K - 1])
+{
+  constexpr int M = 2 * K - 1;
+#pragma unroll
+  for (int r = 0; r < K - 1; ++r) {
+    T e = fea[r * (K + 1) + K] * eca, o = T(0);
+    e += feb[r * (K + 1) + K] * ecb;
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      e += fea[r * (K + 1) + j] * eoa[j].x;
+      o += foa[r * K + j] * eoa[j].y;
+      e += feb[r * (K + 1) + j] * eob[j].x;
+      o += fob[r * K + j] * eob[j].y;
+    }
+    out[r] = e + o;
+    out[M - 1 - r] = e - o;
+  }
+  T sc = fea[(K - 1) * (K + 1) + K] * eca;
+  sc += feb[(K - 1) * (K + 1) + K] * ecb;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    sc += fea[(K - 1) * (K + 1) + j] * eoa[j].x;
+    sc += feb[(K - 1) * (K + 1) + j] * eob[j].x;
+  }
+  out[K - 1] = sc;
+}
+
+// A u + B v with packed (even, odd) accumulators
+template <int K, typename T>
+__device__ __forceinline__ void fold_rows_sum2(const typename Pair<T>::type *fpa, const T *fea,
+                                               const typename Pair<T>::type (&eoa)[K > 1 ? K : 1], const T eca,
+                                               const typename Pair<T>::type *fpb, const T *feb,
+                                               const typename Pair<T>::type (&eob)[K > 1 ? K : 1], const T ecb,
+                                               T (&out)[2 * K - 1])
+{
+  using P = Pair<T>;
+  constexpr int M = 2 * K - 1;
+#pragma unroll
+  for (int r = 0; r < K - 1; ++r) {
+    typename P::type acc = P::make(fea[r * (K + 1) + K] * eca + feb[r * (K + 1) + K] * ecb, T(0));
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      acc = P::fma(fpa[r * K + j], eoa[j], acc);
+      acc = P::fma(fpb[r * K + j], eob[j], acc);
+    }
+    out[r] = acc.x + acc.y;
+    out[M - 1 - r] = acc.x - acc.y;
+  }
+  T sc = fea[(K - 1) * (K + 1) + K] * eca;
+  sc += feb[(K - 1) * (K + 1) + K] * ecb;
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    sc += fea[(K - 1) * (K + 1) + j] * eoa[j].x;
+    sc += feb[(K - 1) * (K + 1) + j] * eob[j].x;
+  }
+  out[K - 1] = sc;
+}
+
 // Fast-diagonalization factor S (eigenvectors as columns; modes 0..k-1 even,
 // k..2k-2 odd) or its transpose applied to a line of 2k-1 values, with packed
 // (even, odd) pairs.
@@ -250,7 +319,7 @@ __device__ __forceinline__ void rows_mass(const typename Pair<T>::type (&eo)[K >
                                           T (&out)[2 * K - 1])
 {
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  if constexpr (TPS_SM3_PACKED) rows_mass<K, T>(eo, ec, out);
+  if constexpr (TPS_SM3_PACKED) fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo, ec, out);
   else fold_rows_s<K, T>(tb.pmass_fe, tb.pmass_fo, eo, ec, out);
 }
 template <int K, typename T>
@@ -258,8 +327,20 @@ __device__ __forceinline__ void rows_lap(const typename Pair<T>::type (&eo)[K > 
                                          T (&out)[2 * K - 1])
 {
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  if constexpr (TPS_SM3_PACKED) rows_lap<K, T>(eo, ec, out);
+  if constexpr (TPS_SM3_PACKED) fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo, ec, out);
   else fold_rows_s<K, T>(tb.plap_fe, tb.plap_fo, eo, ec, out);
+}
+// interior rows of M u + L v (patch mass and stiffness)
+template <int K, typename T>
+__device__ __forceinline__ void rows_mass_lap(const typename Pair<T>::type (&eou)[K > 1 ? K : 1], const T ecu,
+                                              const typename Pair<T>::type (&eov)[K > 1 ? K : 1], const T ecv,
+                                              T (&out)[2 * K - 1])
+{
+  const DegreeTables<K, T> &tb = c_tables<K, T>;
+  if constexpr (TPS_SM3_PACKED)
+    fold_rows_sum2<K, T>(tb.pmass_fp, tb.pmass_fe, eou, ecu, tb.plap_fp, tb.plap_fe, eov, ecv, out);
+  else
+    fold_rows_sum_s<K, T>(tb.pmass_fe, tb.pmass_fo, eou, ecu, tb.plap_fe, tb.plap_fo, eov, ecv, out);
 }
 template <int K, typename T, bool TRANSPOSE>
 __device__ __forceinline__ void evec_apply(const T (&in)[2 * K - 1], T (&out)[2 * K - 1])
@@ -274,7 +355,28 @@ struct Sm3Args {
   int n_batches;
   int zero_x;                 // x == 0 on entry (first colour of a zero-initialised sweep)
   int64_t sy, sz;             // vector pitches (elements)
+  // n / nx_c == (n * mx) >> sx and n / (nx_c ny_c) == (n * mxy) >> sxy for
+  // 0 <= n < 2^31 (see magic_div)
+  uint32_t mx, sx, mxy, sxy;
 };
+
+// Division by an invariant d > 0 as a multiply and shift (the round-up method
+// of Granlund & Montgomery, "Division by invariant integers using
+// multiplication", PLDI 1994, Thm. 4.2 with N = 31): with l = ceil(log2 d),
+// s = 31 + l and m = ceil(2^s / d) < 2^32, floor(n m / 2^s) = floor(n / d) for
+// every 0 <= n < 2^31.
+inline void magic_div(uint32_t d, uint32_t &m, uint32_t &s)
+{
+  uint32_t l = 0;
+  while ((uint64_t(1) << l) < d) ++l;
+  s = 31 + l;
+  m = static_cast<uint32_t>(((uint64_t(1) << s) + d - 1) / d);
+}
+
+__device__ __forceinline__ int fast_div(int n, uint32_t m, uint32_t s)
+{
+  return static_cast<int>((static_cast<uint64_t>(static_cast<uint32_t>(n)) * m) >> s);
+}
 
 template <int K, typename T, bool USE_TMA, int PPB_ = 0>
 __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
@@ -297,7 +399,8 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
 
   // patch j of the colour -> first DoF coordinates of its box
   auto patch_xyz = [&](int j, int &fx, int &fy, int &fz) {
-    const int jx = j % a.nx_c, jy = (j / a.nx_c) % a.ny_c, jz = j / (a.nx_c * a.ny_c);
+    const int jz = fast_div(j, a.mxy, a.sxy), rz = j - jz * (a.nx_c * a.ny_c);
+    const int jy = fast_div(rz, a.mx, a.sx), jx = rz - jy * a.nx_c;
     fx = (a.cx + 2 * jx) * K;
     fy = (a.cy + 2 * jy) * K;
     fz = (a.cz + 2 * jz) * K;
@@ -491,14 +594,13 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
 #pragma unroll
         for (int j = 0; j < N1; ++j) v[j] = s2[j * N1];
         fold_pairs<K, T>(v, eo2, ec2);
-        T ra[M], rb[M], rc[M];
-        rows_mass<K, T>(eo2, ec2, ra);
-        rows_lap<K, T>(eo1, ec1, rb);
+        T ra[M], rc[M];
+        rows_mass_lap<K, T>(eo2, ec2, eo1, ec1, ra);
         rows_mass<K, T>(eo1, ec1, rc);
         T *d1 = V1 + lp * VST + zi * M * N1 + xx, *d2 = V2 + lp * VST + zi * M * N1 + xx;
 #pragma unroll
         for (int i = 0; i < M; ++i) {
-          d1[i * N1] = ra[i] + rb[i];
+          d1[i * N1] = ra[i];
           d2[i * N1] = rc[i];
         }
       }
@@ -519,11 +621,10 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
 #pragma unroll
         for (int j = 0; j < N1; ++j) v[j] = s2[j];
         fold_pairs<K, T>(v, eo2, ec2);
-        T ra[M], rb[M];
-        rows_mass<K, T>(eo1, ec1, ra);
-        rows_lap<K, T>(eo2, ec2, rb);
+        T ra[M];
+        rows_mass_lap<K, T>(eo1, ec1, eo2, ec2, ra);
 #pragma unroll
-        for (int i = 0; i < M; ++i) res[i] = bb[i] - scale * (ra[i] + rb[i]);
+        for (int i = 0; i < M; ++i) res[i] = bb[i] - scale * ra[i];
       } else {
 #pragma unroll
         for (int i = 0; i < M; ++i) res[i] = bb[i];

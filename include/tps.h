@@ -186,12 +186,19 @@ int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_ho
  * by timing): every level of the dtype's V-cycle times each compiled variant
  * and keeps the fastest for later sweeps and V-cycles of this handle.
  * ppb_per_level (n_levels entries, may be null) receives the chosen values
- * (0 in 2D).  Batched solves tune their systems automatically. */
+ * (0 in 2D, -1 for the one-warp-per-patch kernel).  Batched solves tune their systems automatically. */
 int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
-/* The compiled patches-per-block variants of the 3D smoother (3 entries; 0 in
- * 2D) and the explicit choice of one for a level (what tps_autotune sets). */
+/* The compiled variants of the 3D smoother, TPS_SMOOTHER_VARIANTS entries:
+ * patches per CTA batch 0 default, 1 half, 2 quarter, and 3 one warp per
+ * patch (reported as -1 where it is compiled, else as variant 0's value; 0 in
+ * 2D), and the explicit choice of one for a level (what tps_autotune sets). */
+#define TPS_SMOOTHER_VARIANTS 4
 int tps_smoother_variants(tps_handle *h, int dtype, int *ppb);
 int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant);
+/* The variant a level's sweeps use now: the one set or autotuned, else the
+ * library default (one warp per patch where compiled and a colour holds at
+ * least 8192 patches, else the default CTA batch). */
+int tps_get_smoother_variant(tps_handle *h, int dtype, int level, int *variant);
 
 /* ---- batched solves (no reference counterpart) ----------------------------
  * A batch owns n independent systems (1 <= n <= 256): right-hand sides of one

@@ -59,15 +59,15 @@ def test_batch_max_iter_and_zero_rhs(cuda):
 
 
 def test_autotune_keeps_results(cuda):
-    """The patches-per-batch variants only regroup independent patches of a
-    colour: the autotuned sweep is bit-identical to the default one."""
+    """The kernel variants only regroup independent patches of a colour: the
+    autotuned sweep is bit-identical to the default one."""
     P = tps.PoissonProblem(3, 3, 16)
     N1 = 49
     x0, b = interior_random(3, N1, 1).float(), interior_random(3, N1, 2).float()
     x_def = x0.clone()
     tps.PatchSmoother(P).step(x_def, b)
     ppb = P.autotune("fp32")
-    assert len(ppb) == P.n_levels and all(v >= 1 for v in ppb)
+    assert len(ppb) == P.n_levels and all(v >= 1 or v == -1 for v in ppb)
     x_tuned = x0.clone()
     tps.PatchSmoother(P).step(x_tuned, b)
     torch.cuda.synchronize()
@@ -76,4 +76,4 @@ def test_autotune_keeps_results(cuda):
     bb = interior_random(3, N1, 3)
     x, rep = MG.solve_cg(bb, precision="fp32", rel_tol=1e-10)
     assert rep.converged
-    assert P.autotune("fp64")[0] >= 1
+    assert P.autotune("fp64")[0] in (-1, 1, 2, 4, 8, 16)

@@ -111,6 +111,35 @@ def test_vcycle(cuda, oracle, dim, k, n, precision, oprec, tol, symmetric):
     assert relerr(dst.cpu().numpy(), ref) < tol
 
 
+@pytest.mark.parametrize("k,n", [(2, 8), (3, 8), (4, 8), (5, 4), (6, 4), (7, 4)])
+@pytest.mark.parametrize("precision,oprec,tol", [("fp64", 0, TOL64), ("fp32", 1, 1e-4)])
+def test_vcycle_smoother_variants(cuda, oracle, k, n, precision, oprec, tol):
+    """Every compiled 3D smoother variant (patches per CTA batch P, P/2, P/4,
+    one warp per patch) gives the oracle's V-cycle; the variants only regroup
+    the independent patches of a colour with the same per-patch arithmetic,
+    so their V-cycles are bit-identical."""
+    P = tps.PoissonProblem(3, k, n)
+    H = oracle.Hierarchy(3, k, P.n_coarse, P.n_levels)
+    rng = np.random.default_rng(450 + k)
+    src = rng.uniform(-1, 1, P.n_dofs())
+    ref = H.vcycle(src, precision=oprec, symmetric=True)
+    dt = "fp64" if precision == "fp64" else "fp32"
+    variants = P.smoother_variants(dt)
+    assert len(variants) == 4
+    outs = []
+    for v in range(len(variants)):
+        P.set_smoother_variant(v, dt)
+        assert P.smoother_variant(0, dt) == v
+        dst = P.new_vector()
+        tps.MultigridSolvers(P).vmult(dst, dev(src, torch.float64), precision=precision, symmetric=True)
+        torch.cuda.synchronize()
+        assert relerr(dst.cpu().numpy(), ref) < tol, (v, variants[v])
+        outs.append(dst.cpu().numpy())
+    for v in range(1, len(outs)):
+        assert np.array_equal(outs[v], outs[0]), (v, variants[v], relerr(outs[v], outs[0]))
+    P.close()
+
+
 def _rhs(dim, N1, seed):
     rng = np.random.default_rng(seed)
     b = rng.uniform(-1, 1, N1 ** dim)
