@@ -355,15 +355,18 @@ VcycleVectors &vcycle_vectors(tps_handle *h, int p)
 }
 
 // smoother variant of a level that was neither autotuned nor set: the
-// one-warp-per-patch kernel (variant 3) where it is compiled and a colour
-// holds at least 8192 patches (several per resident warp; it measured 17-21 %
-// faster than the CTA batches on 64^3 Q4 in FP32, 12 % in FP64), else the
-// default CTA batch
+// one-warp-per-patch kernel (variant 3) for degrees 3 and 4 when a colour
+// holds at least 4096 patches, else the default CTA batch.  Measured on B200
+// (us per sweep, best CTA batch vs one warp per patch): Q4 64^3 FP32 738 vs
+// 584, FP64 1166 vs 1052; Q4 32^3 FP32 132 vs 115; Q3 32^3 FP64 114 vs 105;
+// on 16^3 and coarser levels (latency-bound launches) and for degrees 2 and 5
+// (3x3 patch interiors leave lanes idle, 9^3 patches leave few warps per SM)
+// the CTA batches are as fast or faster.
 int default_variant(const tps_handle *h, int level, int p)
 {
-  if (h->dim != 3 || h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 3) != -1) return 0;
+  if (h->dim != 3 || (h->k != 3 && h->k != 4) || h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 3) != -1) return 0;
   const int64_t c = h->lv[level].n / 2;  // patches per direction of colour 0
-  return c * c * c >= 8192 ? 3 : 0;
+  return c * c * c >= 4096 ? 3 : 0;
 }
 
 // one coloured sweep; x_zero declares x == 0 on entry (the first colour then

@@ -196,8 +196,8 @@ int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
 int tps_smoother_variants(tps_handle *h, int dtype, int *ppb);
 int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant);
 /* The variant a level's sweeps use now: the one set or autotuned, else the
- * library default (one warp per patch where compiled and a colour holds at
- * least 8192 patches, else the default CTA batch). */
+ * library default (one warp per patch for degrees 3 and 4 when a colour
+ * holds at least 4096 patches, else the default CTA batch). */
 int tps_get_smoother_variant(tps_handle *h, int dtype, int level, int *variant);
 
 /* ---- batched solves (no reference counterpart) ----------------------------
