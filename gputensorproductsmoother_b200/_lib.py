@@ -21,6 +21,7 @@ TPS_F64, TPS_F32, TPS_TF32 = 0, 1, 2
 VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32 = 0, 1, 2, 3
 DRIVER_CG, DRIVER_GMRES = 0, 1
 SMOOTHER_VARIANTS = 4  # TPS_SMOOTHER_VARIANTS
+SMOOTHER_FUSED, SMOOTHER_SEPARATE, SMOOTHER_GLOBAL, SMOOTHER_EXACT = 0, 1, 2, 3
 MAX_HISTORY = 256
 
 
@@ -61,6 +62,8 @@ SIGNATURES = [
     ("tps_laplace_vmult", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
     ("tps_smoother_step", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, ctypes.c_int,
                                          ctypes.c_int, _VP]),
+    ("tps_smoother_step_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, ctypes.c_int,
+                                                 ctypes.c_int, ctypes.c_int, _VP]),
     ("tps_prolongate_add", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
     ("tps_restrict_add", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),
     ("tps_vcycle", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, _VP, _VP, _VP]),

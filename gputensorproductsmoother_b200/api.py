@@ -223,12 +223,26 @@ class PatchSmoother:
     """PatchSmoother (PreconditionRelaxation over the coloured vertex-patch
     sweep): vmult zeroes dst and sweeps once, step sweeps once in place.
     tensor_cores=True runs the 3D patch solves of FP32 vectors on the tensor
-    cores (TF32 operands, FP32 accumulation)."""
+    cores (TF32 operands, FP32 accumulation).  variant selects the
+    reference's SmootherVariant (include/patch_base.cuh:28-90): "fused" (the
+    default kernels), or the separate-kernel cross-checks "separate" (patch
+    residual kernel + fast-diagonalisation kernel), "global" (level operator
+    residual + fast diagonalisation) and "exact" (patch residual + dense
+    inverse of the interior patch matrix)."""
 
-    def __init__(self, problem: PoissonProblem, level: int | None = None, tensor_cores: bool = False):
+    VARIANTS = {"fused": L.SMOOTHER_FUSED, "separate": L.SMOOTHER_SEPARATE, "global": L.SMOOTHER_GLOBAL,
+                "exact": L.SMOOTHER_EXACT}
+
+    def __init__(self, problem: PoissonProblem, level: int | None = None, tensor_cores: bool = False,
+                 variant: str = "fused"):
         self.problem = problem
         self.level = problem.n_levels - 1 if level is None else level
         self.tensor_cores = tensor_cores
+        if variant not in self.VARIANTS:
+            raise ValueError(f"unknown smoother variant {variant!r}")
+        if tensor_cores and variant != "fused":
+            raise ValueError("the tensor-core smoother is a fused kernel")
+        self.variant = variant
 
     def _sweep(self, dst, src, zero_init: bool, reverse: bool):
         p = self.problem
@@ -238,8 +252,13 @@ class PatchSmoother:
             if dst.dtype != torch.float32:
                 raise TypeError("the tensor-core smoother works on float32 vectors")
             dt = L.TPS_TF32
-        L.check(L.lib().tps_smoother_step(p.handle, self.level, dt, dst.data_ptr(), src.data_ptr(),
-                                          int(zero_init), int(reverse), _stream()), p.handle)
+        if self.variant == "fused":
+            L.check(L.lib().tps_smoother_step(p.handle, self.level, dt, dst.data_ptr(), src.data_ptr(),
+                                              int(zero_init), int(reverse), _stream()), p.handle)
+        else:
+            L.check(L.lib().tps_smoother_step_variant(p.handle, self.level, dt, dst.data_ptr(), src.data_ptr(),
+                                                      int(zero_init), int(reverse), self.VARIANTS[self.variant],
+                                                      _stream()), p.handle)
 
     def vmult(self, dst: torch.Tensor, src: torch.Tensor, reverse: bool = False) -> None:
         self._sweep(dst, src, True, reverse)

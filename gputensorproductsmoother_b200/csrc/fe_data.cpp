@@ -285,4 +285,61 @@ DegreeData make_degree_data(int k)
   return D;
 }
 
+std::vector<double> dense_patch_inverse(const DegreeData &D, int dim)
+{
+  const int k = D.k, n1 = 2 * k + 1, m = 2 * k - 1;
+  int n = 1;
+  for (int d = 0; d < dim; ++d) n *= m;
+  auto Mi = [&](int i, int j) { return D.pmass[(i + 1) * n1 + j + 1]; };
+  auto Li = [&](int i, int j) { return D.plap[(i + 1) * n1 + j + 1]; };
+  const size_t nn = static_cast<size_t>(n);
+  std::vector<double> A(nn * nn);
+  for (int e = 0; e < n; ++e) {
+    const int ex = e % m, ey = (e / m) % m, ez = dim == 3 ? e / (m * m) : 0;
+    for (int f = 0; f < n; ++f) {
+      const int fx = f % m, fy = (f / m) % m, fz = dim == 3 ? f / (m * m) : 0;
+      double v;
+      if (dim == 3)
+        v = Li(ex, fx) * Mi(ey, fy) * Mi(ez, fz) + Mi(ex, fx) * Li(ey, fy) * Mi(ez, fz) +
+            Mi(ex, fx) * Mi(ey, fy) * Li(ez, fz);
+      else
+        v = Li(ex, fx) * Mi(ey, fy) + Mi(ex, fx) * Li(ey, fy);
+      A[e * nn + f] = v;
+    }
+  }
+  // A = L L^T (lower triangle of A, row-major)
+  for (size_t j = 0; j < nn; ++j) {
+    double s = A[j * nn + j];
+    for (size_t p = 0; p < j; ++p) s -= A[j * nn + p] * A[j * nn + p];
+    if (!(s > 0.0)) throw std::runtime_error("interior patch matrix is not positive definite");
+    const double d = std::sqrt(s);
+    A[j * nn + j] = d;
+    for (size_t i = j + 1; i < nn; ++i) {
+      double t = A[i * nn + j];
+      for (size_t p = 0; p < j; ++p) t -= A[i * nn + p] * A[j * nn + p];
+      A[i * nn + j] = t / d;
+    }
+  }
+  // WT[c][p] = (L^{-1})[p][c] for p >= c
+  std::vector<double> WT(nn * nn, 0.0);
+  for (size_t c = 0; c < nn; ++c) {
+    WT[c * nn + c] = 1.0 / A[c * nn + c];
+    for (size_t i = c + 1; i < nn; ++i) {
+      double t = 0.0;
+      for (size_t p = c; p < i; ++p) t += A[i * nn + p] * WT[c * nn + p];
+      WT[c * nn + i] = -t / A[i * nn + i];
+    }
+  }
+  // A^{-1} = L^{-T} L^{-1}: inv[i][j] = sum over p >= max(i, j) of W[p][i] W[p][j]
+  std::vector<double> inv(nn * nn);
+  for (size_t i = 0; i < nn; ++i)
+    for (size_t j = i; j < nn; ++j) {
+      double t = 0.0;
+      for (size_t p = j; p < nn; ++p) t += WT[i * nn + p] * WT[j * nn + p];
+      inv[i * nn + j] = t;
+      inv[j * nn + i] = t;
+    }
+  return inv;
+}
+
 }  // namespace tps

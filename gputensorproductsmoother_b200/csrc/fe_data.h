@@ -31,6 +31,14 @@ struct DegreeData {
 // Builds every table above for degree k (1 <= k <= kMaxDegree).
 DegreeData make_degree_data(int k);
 
+// Inverse of the reference-cell interior patch matrix (the Exact local
+// solver, include/loop_kernel.cuh:241-327): A_II = sum over the dim
+// directions of the interior patch stiffness in that direction times the
+// interior patch mass in the others, assembled densely (x fastest,
+// (2k-1)^dim rows) and inverted by Cholesky factorisation in FP64.  Returns
+// the full symmetric inverse, row-major.
+std::vector<double> dense_patch_inverse(const DegreeData &D, int dim);
+
 // Symmetric-definite generalized eigenproblem A v = lambda B v (FP64,
 // Cholesky + cyclic Jacobi); V column-major-as-rows like DegreeData::evec.
 void generalized_eigen(int m, const double *A, const double *B, double *V, double *lambda);

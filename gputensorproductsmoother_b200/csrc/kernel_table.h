@@ -91,6 +91,14 @@ struct KernelTable {
   // FP64 fine += P coarse with the coarse boundary values used ([dim - 2])
   cudaError_t (*prolong_nb[2])(const LevelGeomH &coarse, const VecLayout &lc, const VecLayout &lf,
                                void *fine, const void *coarse_v, void *tmp, cudaStream_t);
+  // separate-kernel smoother variants (cross-checks of the fused kernels), per
+  // colour: r_I = (b - A x)_I on the interiors of the colour's patches, and
+  // x_I <- omega (x_I + A_II^{-1} r_I) with the fast diagonalisation (inv
+  // null) or the dense reference-cell inverse inv (interior^2, symmetric)
+  cudaError_t (*patch_residual[2][2])(const LevelGeomH &, const VecLayout &, const void *x, const void *b,
+                                      void *r, int colour, cudaStream_t);
+  cudaError_t (*patch_solve[2][2])(const LevelGeomH &, const VecLayout &, void *x, const void *r,
+                                   const void *inv, int colour, double omega, cudaStream_t);
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda

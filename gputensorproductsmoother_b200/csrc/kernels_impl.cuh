@@ -12,6 +12,7 @@
 #include "smoother3d.cuh"
 #include "smoother3d_tc.cuh"
 #include "smoother3d_warp.cuh"
+#include "smoother_variants.cuh"
 #include "transfer.cuh"
 
 namespace tps {
@@ -112,6 +113,10 @@ cudaError_t set_attributes()
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetInterior>), (restrict_smem<T>()));
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetAll>), (restrict_smem<T>()));
   TPS_SET((kappa_smoother_kernel<2, K, T>), (sizeof(T) * KSm<2, K, T>::ELEMS));
+  TPS_SET((patch_residual_kernel<2, K, T>), (sizeof(T) * PVar<2, K>::RES_ELEMS));
+  TPS_SET((patch_residual_kernel<3, K, T>), (sizeof(T) * PVar<3, K>::RES_ELEMS));
+  TPS_SET((patch_solve_kernel<2, K, T>), (sizeof(T) * PVar<2, K>::SOLVE_ELEMS));
+  TPS_SET((patch_solve_kernel<3, K, T>), (sizeof(T) * PVar<3, K>::SOLVE_ELEMS));
   TPS_SET((kappa_smoother_kernel<3, K, T>), (sizeof(T) * KSm<3, K, T>::ELEMS));
 #if TPS_DEGREE >= 2
   if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_tc_kernel<K>), (Tc3<K>::BYTES));
@@ -534,6 +539,47 @@ cudaError_t cell_energy(const LevelGeomH &g, const VecLayout &l, double *e, cons
   return cudaGetLastError();
 }
 
+// patches of colour `colour` of a level with layout l
+template <int DIM>
+PatchColour patch_colour(const LevelGeomH &g, const VecLayout &l, int colour)
+{
+  PatchColour c;
+  int nz = 1;
+  colour_lattice(DIM, g.n, colour, c.nx, c.ny, nz, c.count);
+  c.cx = colour & 1;
+  c.cy = (colour >> 1) & 1;
+  c.cz = (colour >> 2) & 1;
+  c.sy = l.sy;
+  c.sz = l.sz;
+  return c;
+}
+
+template <int DIM, typename T>
+cudaError_t patch_residual(const LevelGeomH &g, const VecLayout &l, const void *x, const void *b, void *r,
+                           int colour, cudaStream_t s)
+{
+  const PatchColour c = patch_colour<DIM>(g, l, colour);
+  if (c.count == 0) return cudaSuccess;
+  using S = PVar<DIM, K>;
+  patch_residual_kernel<DIM, K, T><<<c.count, S::NT, sizeof(T) * S::RES_ELEMS, s>>>(
+      static_cast<const T *>(x), static_cast<const T *>(b), static_cast<T *>(r), c,
+      static_cast<T>(stiffness_scale(DIM, g.h)));
+  return cudaGetLastError();
+}
+
+template <int DIM, typename T>
+cudaError_t patch_solve(const LevelGeomH &g, const VecLayout &l, void *x, const void *r, const void *inv,
+                        int colour, double omega, cudaStream_t s)
+{
+  const PatchColour c = patch_colour<DIM>(g, l, colour);
+  if (c.count == 0) return cudaSuccess;
+  using S = PVar<DIM, K>;
+  patch_solve_kernel<DIM, K, T><<<c.count, S::NT, sizeof(T) * S::SOLVE_ELEMS, s>>>(
+      static_cast<T *>(x), static_cast<const T *>(r), static_cast<const T *>(inv), c, static_cast<T>(omega),
+      static_cast<T>(1.0 / stiffness_scale(DIM, g.h)));
+  return cudaGetLastError();
+}
+
 }  // namespace deg_impl
 }  // namespace
 
@@ -566,6 +612,10 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
     &deg_impl::encode_tc_maps,
     &deg_impl::smoother_ppb,
     {&deg_impl::prolong_nb<2>, &deg_impl::prolong_nb<3>},
+    {{&deg_impl::patch_residual<2, double>, &deg_impl::patch_residual<2, float>},
+     {&deg_impl::patch_residual<3, double>, &deg_impl::patch_residual<3, float>}},
+    {{&deg_impl::patch_solve<2, double>, &deg_impl::patch_solve<2, float>},
+     {&deg_impl::patch_solve<3, double>, &deg_impl::patch_solve<3, float>}},
 };
 
 }  // namespace tps

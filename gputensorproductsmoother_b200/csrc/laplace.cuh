@@ -220,9 +220,21 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT, 2)
 // three directions.  The next layer's k input planes are loaded into
 // registers while the current layer is contracted; each thread's staged xy
 // offsets are computed once, so a prefetched entry costs one add and a load.
-#ifndef TPS_OPSTREAM_MINB
-#define TPS_OPSTREAM_MINB(K) 1  // a register cap for more CTAs per SM measured slower (spills)
+// CTAs per SM the register budget must allow: two (at most 128 registers for
+// 256 threads), which doubles the resident warps of this latency-bound kernel
+// (measured on B200, ms per apply, one CTA vs two: Q4 64^3 FP64 0.255 vs
+// 0.198, FP32 0.136 vs 0.131; Q3 32^3 FP64 0.038 vs 0.024; Q7 32^3 FP64 0.321
+// vs 0.296), except Q7 FP32, which spills 444 bytes under the cap (0.169 vs
+// 0.388 ms) and keeps one
+template <int K, typename T>
+constexpr int opstream_minb()
+{
+#ifdef TPS_OPSTREAM_MINB
+  return TPS_OPSTREAM_MINB(K);
+#else
+  return (K == 7 && sizeof(T) == 4) ? 1 : 2;
 #endif
+}
 template <int K, typename T>
 struct OpStream {
   static constexpr int TX = K == 1 ? 16 : K == 2 ? 8 : K <= 4 ? 4 : K == 5 ? 3 : 2, TY = TX;  // cells per CTA in x, y
@@ -238,7 +250,7 @@ struct OpStream {
   static constexpr int OFF_T2 = OFF_T1 + (K + 1) * TS;
   static constexpr int ELEMS = OFF_T2 + (K + 1) * TS;
   static constexpr int EPT = (PL + NT - 1) / NT;      // staged xy entries per thread and plane
-  static constexpr int MINB = TPS_OPSTREAM_MINB(K);    // CTAs per SM the registers must allow
+  static constexpr int MINB = opstream_minb<K, T>();   // CTAs per SM the registers must allow
 };
 
 template <int K, typename T, OpMode MODE>

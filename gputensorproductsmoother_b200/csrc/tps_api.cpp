@@ -150,6 +150,8 @@ struct tps_handle {
   DevBuf host_b, host_x;              // device staging of tps_solve_host (kept, so its graph stays valid)
   std::vector<std::unique_ptr<DevBuf>> fmg_sol, fmg_res;  // FMG: FP64 per level (lexicographic)
   DevBuf fmg_tmp;                                        // FMG: FP64 transfer scratch
+  DevBuf var_r[2];      // separate-kernel smoother variants: residual of the finest-level size
+  DevBuf dense_inv[2];  // Exact variant: reference-cell interior patch inverse [FP64, FP32]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
   ~tps_handle()
@@ -1072,6 +1074,52 @@ int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *
     const int p = dt_index(dtype);
     if (zero_init) TPS_CUDA(cudaMemsetAsync(x, 0, (p == 0 ? 8 : 4) * g.N, s));
     smoother_sweep(h, level, p, lex_layout(h, level), x, b, reverse != 0, zero_init != 0, nullptr, s);
+  });
+}
+
+int tps_smoother_step_variant(tps_handle *h, int level, int dtype, void *x, const void *b, int zero_init,
+                              int reverse, int variant, void *stream)
+{
+  if (variant == TPS_SMOOTHER_FUSED) return tps_smoother_step(h, level, dtype, x, b, zero_init, reverse, stream);
+  return guarded(h, [&] {
+    check_level(h, level);
+    if (!x || !b) throw ApiError(TPS_ERR_INVALID, "null vector");
+    if (x == b) throw ApiError(TPS_ERR_INVALID, "x and b must not alias");
+    if (variant != TPS_SMOOTHER_SEPARATE && variant != TPS_SMOOTHER_GLOBAL && variant != TPS_SMOOTHER_EXACT)
+      throw ApiError(TPS_ERR_INVALID, "unknown smoother variant");
+    if (h->has_kappa)
+      throw ApiError(TPS_ERR_UNSUPPORTED, "the separate-kernel smoother variants have constant coefficients");
+    const int p = dt_index(dtype);
+    const size_t es = p == 0 ? 8 : 4;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const LevelGeomH &g = h->lv[level];
+    const VecLayout lay = lex_layout(h, level);
+    if (h->var_r[p].bytes < es * h->fine().N) h->var_r[p].alloc(es * h->fine().N);
+    const void *inv = nullptr;
+    if (variant == TPS_SMOOTHER_EXACT) {
+      if (!h->dense_inv[p].p) {
+        const std::vector<double> a = dense_patch_inverse(h->D, h->dim);
+        if (p == 0) {
+          h->dense_inv[0].alloc(8 * a.size());
+          TPS_CUDA(cudaMemcpy(h->dense_inv[0].p, a.data(), 8 * a.size(), cudaMemcpyHostToDevice));
+        } else {
+          const std::vector<float> f(a.begin(), a.end());
+          h->dense_inv[1].alloc(4 * f.size());
+          TPS_CUDA(cudaMemcpy(h->dense_inv[1].p, f.data(), 4 * f.size(), cudaMemcpyHostToDevice));
+        }
+      }
+      inv = h->dense_inv[p].p;
+    }
+    if (zero_init) TPS_CUDA(cudaMemsetAsync(x, 0, es * g.N, s));
+    const int nc = 1 << h->dim;
+    for (int i = 0; i < nc; ++i) {
+      const int c = reverse ? nc - 1 - i : i;
+      if (variant == TPS_SMOOTHER_GLOBAL)
+        level_laplace(h, level, p, lay, h->var_r[p].p, x, b, 1, s);  // r = b - A x on interior rows
+      else
+        TPS_CUDA(h->kt->patch_residual[h->dim - 2][p](g, lay, x, b, h->var_r[p].p, c, s));
+      TPS_CUDA(h->kt->patch_solve[h->dim - 2][p](g, lay, x, h->var_r[p].p, inv, c, h->omega, s));
+    }
   });
 }
 

@@ -79,6 +79,26 @@ int tps_laplace_vmult(tps_handle *h, int level, int dtype, void *dst, const void
 int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *b,
                       int zero_init, int reverse, void *stream);
 
+/* The reference's other smoother variants (SmootherVariant GLOBAL, SEPERATE,
+ * Exact; include/patch_base.cuh:28-90, dispatched in
+ * PatchSmootherImpl::step_impl, include/patch_smoother.cuh:185-260), as
+ * cross-checks of tps_smoother_step (TPS_SMOOTHER_FUSED).  Per colour the
+ * residual r_I = (b - A x)_I is formed on the patch interiors -- per patch
+ * from its box (SEPARATE, EXACT) or by the level operator (GLOBAL) -- into a
+ * handle-owned vector, then x_I <- omega (x_I + A_II^{-1} r_I) per patch by
+ * the fast diagonalisation (SEPARATE, GLOBAL) or by the dense inverse of the
+ * assembled interior patch matrix (EXACT; computed in FP64 on the host at the
+ * first EXACT call of a handle: (2k-1)^dim squared entries, about 5 s of host
+ * time for 3D Q7).  Same sweep as TPS_SMOOTHER_FUSED up to rounding.  dtype
+ * TPS_F64 or TPS_F32; constant coefficient only (TPS_ERR_UNSUPPORTED with
+ * kappa); lexicographic caller vectors. */
+#define TPS_SMOOTHER_FUSED 0
+#define TPS_SMOOTHER_SEPARATE 1
+#define TPS_SMOOTHER_GLOBAL 2
+#define TPS_SMOOTHER_EXACT 3
+int tps_smoother_step_variant(tps_handle *h, int level, int dtype, void *x, const void *b,
+                              int zero_init, int reverse, int variant, void *stream);
+
 /* MGTransferCUDA::prolongate_and_add / restrict_and_add
  * (include/cuda_mg_transfer.template.cuh:575-671).  to_level / from_level is the
  * finer level (>= 1). */

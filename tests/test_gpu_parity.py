@@ -68,6 +68,50 @@ def test_smoother_step(cuda, oracle, dim, k, n, dtype, zero_init, reverse):
     assert err < (TOL64 if dtype == torch.float64 else TOL32), err
 
 
+@pytest.mark.parametrize("dim,k,n", CASES)
+@pytest.mark.parametrize("variant", ["separate", "global", "exact"])
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("zero_init,reverse", [(False, False), (True, True)])
+def test_smoother_variants(cuda, oracle, dim, k, n, variant, dtype, zero_init, reverse):
+    """The reference's SEPERATE, GLOBAL and Exact smoother variants (separate
+    residual and local-solve kernels, written independently of the fused
+    ones) give the oracle's sweep.  Exact in FP32 sums up to (2k-1)^3 products
+    per entry of its dense inverse, hence the looser 1e-4."""
+    if variant == "exact" and dim == 3 and k == 7 and (zero_init or dtype == torch.float32):
+        pytest.skip("one 3D Q7 Exact case: its dense inverse takes ~5 s of host time per handle")
+    P = tps.PoissonProblem(dim, k, n)
+    N = P.n_dofs()
+    rng = np.random.default_rng(300 + 10 * dim + k)
+    x0 = rng.uniform(-1, 1, N)
+    b = rng.uniform(-1, 1, N)
+    npdt = np.float64 if dtype == torch.float64 else np.float32
+    ref = oracle.smoother_step(dim, k, n, x0.astype(npdt), b.astype(npdt), zero_init=zero_init,
+                               reverse=reverse)
+    x = dev(x0, dtype)
+    sm = tps.PatchSmoother(P, variant=variant)
+    (sm.vmult if zero_init else sm.step)(x, dev(b, dtype), reverse=reverse)
+    torch.cuda.synchronize()
+    err = relerr(x.cpu().numpy(), ref)
+    tol = TOL64 if dtype == torch.float64 else (1e-4 if variant == "exact" else TOL32)
+    assert err < tol, err
+    # a second sweep continues from the first, as the fused one does
+    ref2 = oracle.smoother_step(dim, k, n, ref.astype(npdt), b.astype(npdt), reverse=reverse)
+    sm.step(x, dev(b, dtype), reverse=reverse)
+    torch.cuda.synchronize()
+    assert relerr(x.cpu().numpy(), ref2) < 4 * tol
+    P.close()
+
+
+def test_smoother_variant_errors(cuda):
+    P = tps.PoissonProblem(3, 2, 4, kappa=np.ones(64))
+    x = P.new_vector()
+    with pytest.raises(tps.TpsError):
+        tps.PatchSmoother(P, variant="global").step(x, P.new_vector())
+    with pytest.raises(ValueError):
+        tps.PatchSmoother(P, variant="nonsense")
+    P.close()
+
+
 @pytest.mark.parametrize("dim,k", [(2, k) for k in range(1, 8)] + [(3, k) for k in range(1, 8)])
 @pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
 def test_transfer(cuda, oracle, dim, k, dtype):
