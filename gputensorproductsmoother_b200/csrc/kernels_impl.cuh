@@ -141,15 +141,20 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
   const T scale = static_cast<T>(stiffness_scale(DIM, g.h));
   if constexpr (DIM == 3) {
     using Sz = OpStream<K, T>;
-    const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, Sz::CZ));
+    // at least one CTA per SM of a 148-SM part: 8 layers per CTA on 32^3 and
+    // larger Q4 levels, 1 on 16^3 and smaller (measured, us per FP64 apply
+    // with 8 layers vs 1: 16^3 24.7 vs 19.5, 8^3 23.0 vs 19.6; with 2 layers
+    // on 32^3 the recomputed leading layers made it 33.0 -> 39.6)
+    const int cz = opstream_layers<K, T>(g.n, 148);
+    const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, cz));
     const size_t smem = sizeof(T) * Sz::ELEMS;
     if (mode == 0)
       laplace3d_stream_kernel<K, T, OpMode::Vmult><<<grid, Sz::NT, smem, s>>>(
-          static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, l.sy, l.sz, scale);
+          static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, l.sy, l.sz, scale, cz);
     else
       laplace3d_stream_kernel<K, T, OpMode::Residual><<<grid, Sz::NT, smem, s>>>(
           static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1, g.n, l.sy,
-          l.sz, scale);
+          l.sz, scale, cz);
   } else {
     using Tl = OpTile<DIM, K>;
     const dim3 grid(ceil_div(g.n, Tl::CX), ceil_div(g.n, Tl::CY), 1);
@@ -395,7 +400,7 @@ template <int DIM, typename T, bool MASK>
 cudaError_t prolong_impl(const LevelGeomH &gc, const VecLayout &lc, const VecLayout &lf, void *fine,
                          const void *coarse, void *tmp, cudaStream_t s)
 {
-  constexpr int C = XYTile<K>::C;
+  constexpr int C = ProlTile<K, T>::C;
   const int N1c = gc.N1, N1f = 2 * gc.n * K + 1;
   const unsigned gxy = ceil_div(gc.n, C);
   if constexpr (DIM == 2) {

@@ -241,7 +241,7 @@ struct OpStream {
   static constexpr int OX = TX * K, OY = TY * K;      // output tile
   static constexpr int WX = (TX + 1) * K + 1, WY = (TY + 1) * K + 1;  // staged plane
   static constexpr int NT = (OX * OY + 31) / 32 * 32;
-  static constexpr int CZ = 8;                        // cell layers per CTA
+  static constexpr int CZ = 8;                        // cell layers per CTA (at most; see opstream_layers)
   static constexpr int PL = WX * WY;                  // one staged input plane
   static constexpr int XS = WY * OX;                  // one x-contracted plane (per product)
   static constexpr int TS = OY * OX;                  // one xy-contracted plane (per product)
@@ -253,10 +253,23 @@ struct OpStream {
   static constexpr int MINB = opstream_minb<K, T>();   // CTAs per SM the registers must allow
 };
 
+// cell layers per CTA for a level of n cells per direction: the most (up to
+// CZ, fewer leading layers recomputed) that still gives at least `want` CTAs;
+// one on small levels, where a CTA's layer march is the latency
+template <int K, typename T>
+inline int opstream_layers(int n, int want)
+{
+  using S = OpStream<K, T>;
+  const int xy = ((n + S::TX - 1) / S::TX) * ((n + S::TY - 1) / S::TY);
+  for (int cz = S::CZ; cz > 1; cz /= 2)
+    if (xy * ((n + cz - 1) / cz) >= want) return cz;
+  return 1;
+}
+
 template <int K, typename T, OpMode MODE>
 __global__ void __launch_bounds__(OpStream<K, T>::NT, OpStream<K, T>::MINB)
     laplace3d_stream_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs,
-                            int N1g, int n_cells, int64_t sy, int64_t sz, T scale)
+                            int N1g, int n_cells, int64_t sy, int64_t sz, T scale, int cz)
 {
   using S = OpStream<K, T>;
   constexpr int NT = S::NT, WX = S::WX, WY = S::WY, OX = S::OX, OY = S::OY, PL = S::PL;
@@ -268,8 +281,8 @@ __global__ void __launch_bounds__(OpStream<K, T>::NT, OpStream<K, T>::MINB)
   const int tid = threadIdx.x;
   const int cx0 = blockIdx.x * S::TX, cy0 = blockIdx.y * S::TY;
   const int gx0 = (cx0 - 1) * K, gy0 = (cy0 - 1) * K;  // staged plane origin
-  const int cz_begin = blockIdx.z * S::CZ;
-  const int cz_end = min(cz_begin + S::CZ, n_cells);
+  const int cz_begin = blockIdx.z * cz;  // cz cell layers per CTA
+  const int cz_end = min(cz_begin + cz, n_cells);
   const int c_first = cz_begin > 0 ? cz_begin - 1 : 0;  // leading layer: carry only
 
   // this thread's staged xy entries (fixed for every plane): global xy offset

@@ -26,8 +26,20 @@ enum class XYOut { AddInterior = 0, SetInterior = 1, SetAll = 2 };
 
 template <int K>
 struct XYTile {
-  static constexpr int C = K <= 4 ? 4 : 2;  // coarse cells per CTA and direction
+  // restriction: coarse cells per CTA and direction, 8 (k <= 4) or 4, so
+  // that the second pass of a 256-thread CTA has a task per thread and the
+  // fine-plane halo costs (2k(C+1)+1)^2 / (2kC)^2 = 1.3x at k = 4 (1.6x with
+  // 4 cells; measured at 3D Q4 64^3: FP32 85 -> 70 us, FP64 124 -> 113 us)
+  static constexpr int C = K <= 4 ? 8 : 4;
   static constexpr int NT = 256;
+};
+
+// prolongation: 8 coarse cells per CTA for FP32 at k <= 4 (measured 58 -> 53
+// us at 3D Q4 64^3), else 4 (k <= 4; FP64 measured 99 us with 4, 115 with 8)
+// or 2
+template <int K, typename T>
+struct ProlTile {
+  static constexpr int C = (sizeof(T) == 4 && K <= 4) ? 8 : K <= 4 ? 4 : 2;
 };
 
 // 1D prolongation of one coarse cell: v[0..k] coarse nodes -> out[0..2k-1]
@@ -75,7 +87,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
                       int64_t in_sy, int64_t in_plane, int64_t out_sy, int64_t out_plane,
                       int plane0, int mask_in)
 {
-  constexpr int C = XYTile<K>::C, NT = XYTile<K>::NT;
+  constexpr int C = ProlTile<K, T>::C, NT = XYTile<K>::NT;
   constexpr int WI = C * K + 1;  // coarse inputs per direction
   constexpr int WO = 2 * K * C;  // fine outputs per direction
   __shared__ T sIn[WI * WI];
