@@ -22,10 +22,9 @@
 //    S^T_y -> S^T_z, scale, S_z -> S_x -> S_y + store.  Every contraction keeps
 //    one 1D line per thread in registers and applies the centro-symmetric 1D
 //    matrices in even/odd folded form (about half the dense multiply-adds)
-//    with scalar FMAs whose coefficients are constant-bank operands.  A
-//    packed FP32x2 form (__ffma2_rn on (even, odd) pairs, TPS_SM3_PACKED=1)
-//    halves the FMA count but needs a constant load per coefficient pair; it
-//    measured within 1.5 % of the scalar form, which is the default.  The
+//    with scalar FMAs whose coefficients are constant-bank operands (degree
+//    <= 5), or in a packed form (__ffma2_rn on (even, odd) pairs; degree >= 6,
+//    where it measured faster; see sm3_packed).  The
 //    sums of two products (M_y Z2 + L_y Z1, M_x V1 + L_x V2) run as one
 //    accumulation chain, and every kernel variant uses the same chains, so
 //    the variants give bit-identical sweeps;
@@ -314,12 +313,25 @@ __device__ __forceinline__ void apply_evec_s(const T (&in)[2 * K - 1], T (&out)[
 #ifndef TPS_SM3_PACKED
 #define TPS_SM3_PACKED 0
 #endif
+#ifndef TPS_SM3_PACKED_MIN_K
+#define TPS_SM3_PACKED_MIN_K 6
+#endif
+// packed (even, odd) pair contractions from degree 6 up, scalar below.
+// Measured on B200, ms per 32^3 sweep, CTA kernel, scalar vs packed: Q7 FP32
+// 0.820 vs 0.679, FP64 1.668 vs 1.620; Q6 FP32 0.500 vs 0.476, FP64 1.115 vs
+// 1.035; at Q4 the two were within 1.5 %.  (Two-product sums as separate
+// products and an add instead of one chain measured slower at every degree.)
+template <int K>
+constexpr bool sm3_packed()
+{
+  return TPS_SM3_PACKED != 0 || K >= TPS_SM3_PACKED_MIN_K;
+}
 template <int K, typename T>
 __device__ __forceinline__ void rows_mass(const typename Pair<T>::type (&eo)[K > 1 ? K : 1], const T ec,
                                           T (&out)[2 * K - 1])
 {
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  if constexpr (TPS_SM3_PACKED) fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo, ec, out);
+  if constexpr (sm3_packed<K>()) fold_rows2<K, T>(tb.pmass_fp, tb.pmass_fe, eo, ec, out);
   else fold_rows_s<K, T>(tb.pmass_fe, tb.pmass_fo, eo, ec, out);
 }
 template <int K, typename T>
@@ -327,7 +339,7 @@ __device__ __forceinline__ void rows_lap(const typename Pair<T>::type (&eo)[K > 
                                          T (&out)[2 * K - 1])
 {
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  if constexpr (TPS_SM3_PACKED) fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo, ec, out);
+  if constexpr (sm3_packed<K>()) fold_rows2<K, T>(tb.plap_fp, tb.plap_fe, eo, ec, out);
   else fold_rows_s<K, T>(tb.plap_fe, tb.plap_fo, eo, ec, out);
 }
 // interior rows of M u + L v (patch mass and stiffness)
@@ -337,7 +349,7 @@ __device__ __forceinline__ void rows_mass_lap(const typename Pair<T>::type (&eou
                                               T (&out)[2 * K - 1])
 {
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  if constexpr (TPS_SM3_PACKED)
+  if constexpr (sm3_packed<K>())
     fold_rows_sum2<K, T>(tb.pmass_fp, tb.pmass_fe, eou, ecu, tb.plap_fp, tb.plap_fe, eov, ecv, out);
   else
     fold_rows_sum_s<K, T>(tb.pmass_fe, tb.pmass_fo, eou, ecu, tb.plap_fe, tb.plap_fo, eov, ecv, out);
@@ -345,7 +357,7 @@ __device__ __forceinline__ void rows_mass_lap(const typename Pair<T>::type (&eou
 template <int K, typename T, bool TRANSPOSE>
 __device__ __forceinline__ void evec_apply(const T (&in)[2 * K - 1], T (&out)[2 * K - 1])
 {
-  if constexpr (TPS_SM3_PACKED) apply_evec2<K, T, TRANSPOSE>(in, out);
+  if constexpr (sm3_packed<K>()) apply_evec2<K, T, TRANSPOSE>(in, out);
   else apply_evec_s<K, T, TRANSPOSE>(in, out);
 }
 
