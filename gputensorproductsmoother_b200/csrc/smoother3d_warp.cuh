@@ -389,7 +389,10 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
     }
     __syncwarp();
     // ---- S along y and store x_I ----
-    const int64_t base = fx + 1 + (fy + 1) * a.sy + (fz + 1) * a.sz;
+    // 64-bit patch base once; 32-bit offsets within the patch (a patch spans
+    // less than 2 planes of a level of < 2^31 entries)
+    T *const xp = x + (fx + 1 + (fy + 1) * a.sy + (fz + 1) * a.sz);
+    const int sy32 = static_cast<int>(a.sy), sz32 = static_cast<int>(a.sz);
 #pragma unroll
     for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
       const int t = lane + 32 * p;
@@ -400,9 +403,9 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
 #pragma unroll
         for (int jj = 0; jj < M; ++jj) v[jj] = s[jj * QD.r];
         evec_apply<K, T, false>(v, q);
-        T *dst = x + base + xx + z * a.sz;
+        const int o = xx + z * sz32;
 #pragma unroll
-        for (int jj = 0; jj < M; ++jj) dst[jj * a.sy] = q[jj];
+        for (int jj = 0; jj < M; ++jj) xp[o + jj * sy32] = q[jj];
       }
     }
     __syncwarp();  // the Q buffers (inside the Z region) are read before the next z stage
