@@ -2,6 +2,7 @@
 // (kRedBlocks CTAs, a multiple of the 148 SMs), 64-bit indices, 128-bit
 // vector accesses are left to the compiler for the aligned FP64 streams.
 #include "blas.cuh"
+#include "launch.cuh"
 
 namespace tps {
 namespace {
@@ -50,6 +51,7 @@ __device__ __forceinline__ double block_sum(double v, double *sh)
 
 __global__ void convert_d2f_kernel(float *dst, const double *src, int64_t n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     dst[i] = __double2float_rn(src[i]);
@@ -57,6 +59,7 @@ __global__ void convert_d2f_kernel(float *dst, const double *src, int64_t n)
 
 __global__ void convert_f2d_kernel(double *dst, const float *src, int64_t n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     dst[i] = static_cast<double>(src[i]);
@@ -64,6 +67,7 @@ __global__ void convert_f2d_kernel(double *dst, const float *src, int64_t n)
 
 __global__ void copy_d_kernel(double *dst, const double *src, int64_t n, int round32)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     dst[i] = round32 ? static_cast<double>(__double2float_rn(src[i])) : src[i];
@@ -72,6 +76,7 @@ __global__ void copy_d_kernel(double *dst, const double *src, int64_t n, int rou
 template <typename T>
 __global__ void copy_boundary_kernel(T *dst, const T *src, int dim, int N1)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   // one thread per boundary entry, in three coalesced groups (3D): the z = 0
   // and z = N1-1 planes, the y = 0 and y = N1-1 rows of the other planes, and
   // the x = 0 and x = N1-1 ends of the remaining rows (2D: the y rows, then
@@ -110,6 +115,7 @@ __global__ void copy_boundary_kernel(T *dst, const T *src, int dim, int N1)
 __global__ void __launch_bounds__(kRedThreads)
     dot_kernel(const double *a, const double *b, int64_t n, double *partial)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ double sh[32];
   double s = 0.0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -122,6 +128,7 @@ __global__ void __launch_bounds__(kRedThreads)
 // reduce n_dots arrays of kRedBlocks partial sums; one CTA per dot
 __global__ void __launch_bounds__(kRedThreads) reduce_kernel(const double *partial, double *out)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ double sh[32];
   double s = 0.0;
   for (int i = threadIdx.x; i < kRedBlocks; i += kRedThreads) s += partial[blockIdx.x * kRedBlocks + i];
@@ -133,6 +140,7 @@ __global__ void __launch_bounds__(kRedThreads)
     cg_init_kernel(const double *r, const double *b, void *d, int d_kind, PadMap pm, int64_t n,
                    double *partial)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ double sh[32];
   double s_rr = 0.0, s_bb = 0.0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -154,6 +162,7 @@ __global__ void __launch_bounds__(kRedThreads)
 template <int NDOT, typename Op>
 __global__ void __launch_bounds__(kRedThreads) finalize_kernel(const double *partial, CGScalars *sc, Op op)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ double sh[32];
   double v[NDOT];
 #pragma unroll
@@ -209,6 +218,7 @@ __global__ void __launch_bounds__(kRedThreads)
     cg_first_direction_kernel(double *p, const void *z, int z_kind, PadMap pm, const double *r,
                               int64_t n, double *partial)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ double sh[32];
   double s = 0.0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -225,6 +235,7 @@ __global__ void __launch_bounds__(kRedThreads)
     cg_update_xr_kernel(double *x, double *r, const double *p, const double *q, void *d,
                         int d_kind, PadMap pm, int64_t n, double *partial, const CGScalars *sc)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ double sh[32];
   const double alpha = sc->alpha;
   double s = 0.0;
@@ -244,6 +255,7 @@ __global__ void __launch_bounds__(kRedThreads)
     cg_dots_z_kernel(const void *z, int z_kind, PadMap pm, const double *q, const double *r,
                      int64_t n, double *partial)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ double sh[32];
   double s1 = 0.0, s2 = 0.0;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
@@ -263,6 +275,7 @@ __global__ void __launch_bounds__(kRedThreads)
 __global__ void cg_update_p_kernel(double *p, const void *z, int z_kind, PadMap pm, int64_t n,
                                    const CGScalars *sc)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   const double beta = sc->beta;
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
@@ -271,6 +284,7 @@ __global__ void cg_update_p_kernel(double *p, const void *z, int z_kind, PadMap 
 
 __global__ void axpy_kernel(double *y, double a, const double *x, int64_t n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     y[i] += a * x[i];
@@ -278,6 +292,7 @@ __global__ void axpy_kernel(double *y, double a, const double *x, int64_t n)
 
 __global__ void scale_kernel(double *y, double a, int64_t n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     y[i] *= a;
@@ -285,6 +300,7 @@ __global__ void scale_kernel(double *y, double a, int64_t n)
 
 __global__ void sub_kernel(double *dst, const double *a, const double *b, int64_t n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     dst[i] = a[i] - b[i];
@@ -292,6 +308,7 @@ __global__ void sub_kernel(double *dst, const double *a, const double *b, int64_
 
 __global__ void to_vcycle_kernel(void *d, int d_kind, PadMap pm, const double *src, int64_t n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     store_kind(d, d_kind, pad_index(i, pm), src[i]);
@@ -299,6 +316,7 @@ __global__ void to_vcycle_kernel(void *d, int d_kind, PadMap pm, const double *s
 
 __global__ void from_vcycle_kernel(double *dst, const void *z, int z_kind, PadMap pm, int64_t n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
        i += static_cast<int64_t>(gridDim.x) * blockDim.x)
     dst[i] = load_kind(z, z_kind, pad_index(i, pm));
@@ -308,6 +326,7 @@ __global__ void from_vcycle_kernel(double *dst, const void *z, int z_kind, PadMa
 template <typename T>
 __global__ void coarse_dense_kernel(const T *inv, const int *idx, int n, T *su, const T *d)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   const int row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
   if (row >= n) return;
   T s = T(0);
@@ -327,17 +346,17 @@ unsigned stream_grid(int64_t n, int threads)
 
 cudaError_t launch_convert_f64_to_f32(float *dst, const double *src, int64_t n, cudaStream_t s)
 {
-  convert_d2f_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, src, n);
+  TPS_LAUNCH((convert_d2f_kernel), stream_grid(n, 256), 256, 0, s, dst, src, n);
   return cudaGetLastError();
 }
 cudaError_t launch_convert_f32_to_f64(double *dst, const float *src, int64_t n, cudaStream_t s)
 {
-  convert_f2d_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, src, n);
+  TPS_LAUNCH((convert_f2d_kernel), stream_grid(n, 256), 256, 0, s, dst, src, n);
   return cudaGetLastError();
 }
 cudaError_t launch_copy_f64(double *dst, const double *src, int64_t n, int round32, cudaStream_t s)
 {
-  copy_d_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, src, n, round32);
+  TPS_LAUNCH((copy_d_kernel), stream_grid(n, 256), 256, 0, s, dst, src, n, round32);
   return cudaGetLastError();
 }
 cudaError_t launch_copy_boundary(void *dst, const void *src, int dim, int N1, int elem_bytes,
@@ -347,103 +366,103 @@ cudaError_t launch_copy_boundary(void *dst, const void *src, int dim, int N1, in
   const int64_t count = dim == 3 ? 2 * n1 * n1 + 2 * m * n1 + 2 * m * m : 2 * n1 + 2 * m;
   const unsigned g = static_cast<unsigned>((count + 255) / 256);
   if (elem_bytes == 8)
-    copy_boundary_kernel<double><<<g, 256, 0, s>>>(static_cast<double *>(dst),
+    TPS_LAUNCH((copy_boundary_kernel<double>), g, 256, 0, s, static_cast<double *>(dst),
                                                    static_cast<const double *>(src), dim, N1);
   else
-    copy_boundary_kernel<float><<<g, 256, 0, s>>>(static_cast<float *>(dst),
+    TPS_LAUNCH((copy_boundary_kernel<float>), g, 256, 0, s, static_cast<float *>(dst),
                                                   static_cast<const float *>(src), dim, N1);
   return cudaGetLastError();
 }
 cudaError_t launch_dot_f64(const double *a, const double *b, int64_t n, double *partial,
                            cudaStream_t s)
 {
-  dot_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(a, b, n, partial);
+  TPS_LAUNCH((dot_kernel), kRedBlocks, kRedThreads, 0, s, a, b, n, partial);
   return cudaGetLastError();
 }
 cudaError_t launch_reduce(const double *partial, int n_dots, double *out, cudaStream_t s)
 {
-  reduce_kernel<<<n_dots, kRedThreads, 0, s>>>(partial, out);
+  TPS_LAUNCH((reduce_kernel), n_dots, kRedThreads, 0, s, partial, out);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_init(const double *r, const double *b, void *d, int d_kind, PadMap pm,
                            int64_t n, double *partial, cudaStream_t s)
 {
-  cg_init_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(r, b, d, d_kind, pm, n, partial);
+  TPS_LAUNCH((cg_init_kernel), kRedBlocks, kRedThreads, 0, s, r, b, d, d_kind, pm, n, partial);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_finalize_init(const double *partial, CGScalars *sc, cudaStream_t s)
 {
-  finalize_kernel<2><<<1, kRedThreads, 0, s>>>(partial, sc, OpInit{});
+  TPS_LAUNCH((finalize_kernel<2, OpInit>), 1, kRedThreads, 0, s, partial, sc, OpInit{});
   return cudaGetLastError();
 }
 cudaError_t launch_cg_first_direction(double *p, const void *z, int z_kind, PadMap pm,
                                       const double *r, int64_t n, double *partial, cudaStream_t s)
 {
-  cg_first_direction_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(p, z, z_kind, pm, r, n, partial);
+  TPS_LAUNCH((cg_first_direction_kernel), kRedBlocks, kRedThreads, 0, s, p, z, z_kind, pm, r, n, partial);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_finalize_rz(const double *partial, CGScalars *sc, cudaStream_t s)
 {
-  finalize_kernel<1><<<1, kRedThreads, 0, s>>>(partial, sc, OpRz{});
+  TPS_LAUNCH((finalize_kernel<1, OpRz>), 1, kRedThreads, 0, s, partial, sc, OpRz{});
   return cudaGetLastError();
 }
 cudaError_t launch_cg_alpha(const double *p, const double *q, int64_t n, double *partial,
                             CGScalars *sc, cudaStream_t s)
 {
-  dot_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(p, q, n, partial);
-  finalize_kernel<1><<<1, kRedThreads, 0, s>>>(partial, sc, OpAlpha{});
+  TPS_LAUNCH((dot_kernel), kRedBlocks, kRedThreads, 0, s, p, q, n, partial);
+  TPS_LAUNCH((finalize_kernel<1, OpAlpha>), 1, kRedThreads, 0, s, partial, sc, OpAlpha{});
   return cudaGetLastError();
 }
 cudaError_t launch_cg_update_xr(double *x, double *r, const double *p, const double *q, void *d,
                                 int d_kind, PadMap pm, int64_t n, double *partial,
                                 const CGScalars *sc, cudaStream_t s)
 {
-  cg_update_xr_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(x, r, p, q, d, d_kind, pm, n, partial, sc);
+  TPS_LAUNCH((cg_update_xr_kernel), kRedBlocks, kRedThreads, 0, s, x, r, p, q, d, d_kind, pm, n, partial, sc);
   return cudaGetLastError();
 }
 cudaError_t launch_cg_finalize_rr(const double *partial, CGScalars *sc, cudaStream_t s)
 {
-  finalize_kernel<1><<<1, kRedThreads, 0, s>>>(partial, sc, OpRr{});
+  TPS_LAUNCH((finalize_kernel<1, OpRr>), 1, kRedThreads, 0, s, partial, sc, OpRr{});
   return cudaGetLastError();
 }
 cudaError_t launch_cg_beta(const void *z, int z_kind, PadMap pm, const double *q, const double *r,
                            int64_t n, double *partial, CGScalars *sc, cudaStream_t s)
 {
-  cg_dots_z_kernel<<<kRedBlocks, kRedThreads, 0, s>>>(z, z_kind, pm, q, r, n, partial);
-  finalize_kernel<2><<<1, kRedThreads, 0, s>>>(partial, sc, OpBeta{});
+  TPS_LAUNCH((cg_dots_z_kernel), kRedBlocks, kRedThreads, 0, s, z, z_kind, pm, q, r, n, partial);
+  TPS_LAUNCH((finalize_kernel<2, OpBeta>), 1, kRedThreads, 0, s, partial, sc, OpBeta{});
   return cudaGetLastError();
 }
 cudaError_t launch_cg_update_p(double *p, const void *z, int z_kind, PadMap pm, int64_t n,
                                const CGScalars *sc, cudaStream_t s)
 {
-  cg_update_p_kernel<<<stream_grid(n, 256), 256, 0, s>>>(p, z, z_kind, pm, n, sc);
+  TPS_LAUNCH((cg_update_p_kernel), stream_grid(n, 256), 256, 0, s, p, z, z_kind, pm, n, sc);
   return cudaGetLastError();
 }
 cudaError_t launch_axpy_f64(double *y, double a, const double *x, int64_t n, cudaStream_t s)
 {
-  axpy_kernel<<<stream_grid(n, 256), 256, 0, s>>>(y, a, x, n);
+  TPS_LAUNCH((axpy_kernel), stream_grid(n, 256), 256, 0, s, y, a, x, n);
   return cudaGetLastError();
 }
 cudaError_t launch_scale_f64(double *y, double a, int64_t n, cudaStream_t s)
 {
-  scale_kernel<<<stream_grid(n, 256), 256, 0, s>>>(y, a, n);
+  TPS_LAUNCH((scale_kernel), stream_grid(n, 256), 256, 0, s, y, a, n);
   return cudaGetLastError();
 }
 cudaError_t launch_sub_f64(double *dst, const double *a, const double *b, int64_t n, cudaStream_t s)
 {
-  sub_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, a, b, n);
+  TPS_LAUNCH((sub_kernel), stream_grid(n, 256), 256, 0, s, dst, a, b, n);
   return cudaGetLastError();
 }
 cudaError_t launch_to_vcycle(void *d, int d_kind, PadMap pm, const double *src, int64_t n,
                              cudaStream_t s)
 {
-  to_vcycle_kernel<<<stream_grid(n, 256), 256, 0, s>>>(d, d_kind, pm, src, n);
+  TPS_LAUNCH((to_vcycle_kernel), stream_grid(n, 256), 256, 0, s, d, d_kind, pm, src, n);
   return cudaGetLastError();
 }
 cudaError_t launch_from_vcycle(double *dst, const void *z, int z_kind, PadMap pm, int64_t n,
                                cudaStream_t s)
 {
-  from_vcycle_kernel<<<stream_grid(n, 256), 256, 0, s>>>(dst, z, z_kind, pm, n);
+  TPS_LAUNCH((from_vcycle_kernel), stream_grid(n, 256), 256, 0, s, dst, z, z_kind, pm, n);
   return cudaGetLastError();
 }
 cudaError_t launch_coarse_dense(const void *inv, const int *idx, int n_int, void *su,
@@ -451,11 +470,11 @@ cudaError_t launch_coarse_dense(const void *inv, const int *idx, int n_int, void
 {
   const unsigned g = static_cast<unsigned>((n_int * 32 + 255) / 256);
   if (elem_bytes == 8)
-    coarse_dense_kernel<double><<<g, 256, 0, s>>>(static_cast<const double *>(inv), idx, n_int,
+    TPS_LAUNCH((coarse_dense_kernel<double>), g, 256, 0, s, static_cast<const double *>(inv), idx, n_int,
                                                   static_cast<double *>(su),
                                                   static_cast<const double *>(d));
   else
-    coarse_dense_kernel<float><<<g, 256, 0, s>>>(static_cast<const float *>(inv), idx, n_int,
+    TPS_LAUNCH((coarse_dense_kernel<float>), g, 256, 0, s, static_cast<const float *>(inv), idx, n_int,
                                                  static_cast<float *>(su),
                                                  static_cast<const float *>(d));
   return cudaGetLastError();
@@ -470,6 +489,7 @@ namespace {
 
 __global__ void batch_check_kernel(BatchLoop b, int first, cudaGraphConditionalHandle loop)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   __shared__ int any;
   if (threadIdx.x == 0) any = 0;
   __syncthreads();
@@ -495,6 +515,7 @@ __global__ void batch_check_kernel(BatchLoop b, int first, cudaGraphConditionalH
 
 __global__ void batch_select_kernel(const int *active, const __grid_constant__ BatchConds cond, int n)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   for (int i = threadIdx.x; i < n; i += blockDim.x) cudaGraphSetConditional(cond.h[i], active[i] ? 1u : 0u);
 }
 
@@ -502,13 +523,13 @@ __global__ void batch_select_kernel(const int *active, const __grid_constant__ B
 
 cudaError_t launch_batch_check(BatchLoop b, int first, cudaGraphConditionalHandle loop, cudaStream_t s)
 {
-  batch_check_kernel<<<1, 256, 0, s>>>(b, first, loop);
+  TPS_LAUNCH((batch_check_kernel), 1, 256, 0, s, b, first, loop);
   return cudaGetLastError();
 }
 
 cudaError_t launch_batch_select(const int *active, const BatchConds &cond, int n, cudaStream_t s)
 {
-  batch_select_kernel<<<1, 256, 0, s>>>(active, cond, n);
+  TPS_LAUNCH((batch_select_kernel), 1, 256, 0, s, active, cond, n);
   return cudaGetLastError();
 }
 

@@ -168,6 +168,7 @@ __global__ void __launch_bounds__(KappaCfg<DIM, K>::NT)
     cell_apply_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ kappa,
                       int n, int colour, int ncx, int ncy, int64_t sy, int64_t sz, T s)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using C = KappaCfg<DIM, K>;
   constexpr int NP = C::NP;
   __shared__ T in[C::CELL], out[C::CELL], t1[C::CELL], t2[C::CELL];
@@ -199,6 +200,7 @@ template <int DIM, typename T>
 __global__ void finish_residual_kernel(T *__restrict__ dst, const T *__restrict__ rhs, int N1,
                                        int64_t sy, int64_t sz)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   const int64_t rows = DIM == 3 ? int64_t(N1) * N1 : N1;
   for (int64_t i = blockIdx.x * int64_t(blockDim.x) + threadIdx.x; i < rows * N1;
        i += int64_t(gridDim.x) * blockDim.x) {
@@ -221,6 +223,7 @@ __global__ void __launch_bounds__(KappaCfg<DIM, K>::NT)
     cell_energy_kernel(double *__restrict__ e, const double *__restrict__ u,
                        const double *__restrict__ lam, int n, int64_t sy, int64_t sz, double s)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using C = KappaCfg<DIM, K>;
   constexpr int NP = C::NP;
   __shared__ double in[C::CELL], out[C::CELL], t1[C::CELL], t2[C::CELL];
@@ -267,6 +270,7 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
                           int n, int colour, int nx_c, int ny_c, int64_t sy, int64_t sz, T s,
                           T fd_scale, T omega)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = KSm<DIM, K, T>;
   constexpr int NP = S::NP, N1 = S::N1, M = S::M, NT = S::NT;
   const DegreeTables<K, T> &tb = c_tables<K, T>;

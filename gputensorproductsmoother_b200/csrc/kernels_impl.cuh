@@ -149,10 +149,10 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
     const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, cz));
     const size_t smem = sizeof(T) * Sz::ELEMS;
     if (mode == 0)
-      laplace3d_stream_kernel<K, T, OpMode::Vmult><<<grid, Sz::NT, smem, s>>>(
+      TPS_LAUNCH((laplace3d_stream_kernel<K, T, OpMode::Vmult>), grid, Sz::NT, smem, s,
           static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, l.sy, l.sz, scale, cz);
     else
-      laplace3d_stream_kernel<K, T, OpMode::Residual><<<grid, Sz::NT, smem, s>>>(
+      TPS_LAUNCH((laplace3d_stream_kernel<K, T, OpMode::Residual>), grid, Sz::NT, smem, s,
           static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1, g.n, l.sy,
           l.sz, scale, cz);
   } else {
@@ -160,10 +160,10 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
     const dim3 grid(ceil_div(g.n, Tl::CX), ceil_div(g.n, Tl::CY), 1);
     const size_t smem = laplace_smem<DIM, T>();
     if (mode == 0)
-      laplace_kernel<DIM, K, T, OpMode::Vmult><<<grid, Tl::NT, smem, s>>>(
+      TPS_LAUNCH((laplace_kernel<DIM, K, T, OpMode::Vmult>), grid, Tl::NT, smem, s,
           static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, l.sy, l.sz, scale);
     else
-      laplace_kernel<DIM, K, T, OpMode::Residual><<<grid, Tl::NT, smem, s>>>(
+      TPS_LAUNCH((laplace_kernel<DIM, K, T, OpMode::Residual>), grid, Tl::NT, smem, s,
           static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1,
           l.sy, l.sz, scale);
   }
@@ -196,7 +196,7 @@ void smoother3d_launch(Sm3Args a, const SmootherMaps *maps, void *x, const void 
   if (maps && maps->valid) {
     using S = Sm3<K, T, PPB>;
     a.n_batches = static_cast<int>(ceil_div(a.n_patches, S::PPB));
-    smoother3d_kernel<K, T, true, PPB><<<sm3_grid<T, true, PPB>(a.n_batches), S::NT, S::BYTES, s>>>(
+    TPS_LAUNCH((smoother3d_kernel<K, T, true, PPB>), sm3_grid<T, true, PPB>(a.n_batches), S::NT, S::BYTES, s,
         *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),
         static_cast<T *>(x), static_cast<const T *>(b), a, scale, fd, err);
   } else {
@@ -204,7 +204,7 @@ void smoother3d_launch(Sm3Args a, const SmootherMaps *maps, void *x, const void 
     using S = Sm3<K, T, P0>;
     a.n_batches = static_cast<int>(ceil_div(a.n_patches, S::PPB));
     CUtensorMap none{};
-    smoother3d_kernel<K, T, false, P0><<<a.n_batches, S::NT, S::BYTES, s>>>(
+    TPS_LAUNCH((smoother3d_kernel<K, T, false, P0>), a.n_batches, S::NT, S::BYTES, s,
         none, none, static_cast<T *>(x), static_cast<const T *>(b), a, scale, fd, err);
   }
 }
@@ -230,7 +230,7 @@ void smoother3d_warp_launch(const Sm3Args &a, const SmootherMaps *maps, void *x,
     }
     const int need = static_cast<int>(ceil_div(a.n_patches, WA));
     const int grid = need < per_sm * n_sm ? need : per_sm * n_sm;
-    smoother3d_warp_kernel<K, T, WA><<<grid, S::NT, S::BYTES, s>>>(
+    TPS_LAUNCH((smoother3d_warp_kernel<K, T, WA>), grid, S::NT, S::BYTES, s,
         *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),
         static_cast<T *>(x), a, scale, fd, err);
   }
@@ -264,7 +264,7 @@ cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const voi
     (void)zero_x;  // the 2D kernel always reads x (x == 0 gives the same sweep)
     (void)maps;
     (void)err;
-    smoother_colour_kernel<DIM, K, T><<<ceil_div(count, S::PPB), S::NT, smoother_smem<DIM, T>(), s>>>(
+    TPS_LAUNCH((smoother_colour_kernel<DIM, K, T>), ceil_div(count, S::PPB), S::NT, smoother_smem<DIM, T>(), s,
         static_cast<T *>(x), static_cast<const T *>(b), l.sy, l.sz, nx, ny, count, cx, cy, cz,
         static_cast<T>(sc), static_cast<T>(1.0 / sc), static_cast<T>(omega));
   } else {
@@ -339,7 +339,7 @@ cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const 
     a.sz = l.sz;
     magic_div(static_cast<uint32_t>(nx), a.mx, a.sx);
     magic_div(static_cast<uint32_t>(nx) * static_cast<uint32_t>(ny), a.mxy, a.sxy);
-    smoother3d_tc_kernel<K><<<tc_grid(static_cast<int>(ceil_div(count, C::U))), C::NT, C::BYTES, s>>>(
+    TPS_LAUNCH((smoother3d_tc_kernel<K>), tc_grid(static_cast<int>(ceil_div(count, C::U))), C::NT, C::BYTES, s,
         *reinterpret_cast<const CUtensorMap *>(maps->tx), *reinterpret_cast<const CUtensorMap *>(maps->tb),
         static_cast<float *>(x), a, static_cast<float>(sc), static_cast<float>(omega / sc), err);
     return cudaGetLastError();
@@ -404,16 +404,16 @@ cudaError_t prolong_impl(const LevelGeomH &gc, const VecLayout &lc, const VecLay
   const int N1c = gc.N1, N1f = 2 * gc.n * K + 1;
   const unsigned gxy = ceil_div(gc.n, C);
   if constexpr (DIM == 2) {
-    prolong_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, 1), XYTile<K>::NT, 0, s>>>(
+    TPS_LAUNCH((prolong_xy_kernel<K, T, XYOut::AddInterior>), dim3(gxy, gxy, 1), XYTile<K>::NT, 0, s,
         static_cast<T *>(fine), static_cast<const T *>(coarse), N1c, N1f, lc.sy, 0, lf.sy, 0, 0, MASK ? 1 : 0);
   } else {
     const int64_t P = static_cast<int64_t>(N1c) * N1c;
-    prolong_z_kernel<K, T, MASK><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
+    TPS_LAUNCH((prolong_z_kernel<K, T, MASK>), dim3(ceil_div(P, 256), gc.n), 256, 0, s,
         static_cast<T *>(tmp), static_cast<const T *>(coarse), N1c, N1f, gc.n, lc.sy, lc.sz);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     // fine interior planes 1..N1f-2 from tmp planes 1..N1f-2
-    prolong_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, N1f - 2), XYTile<K>::NT, 0, s>>>(
+    TPS_LAUNCH((prolong_xy_kernel<K, T, XYOut::AddInterior>), dim3(gxy, gxy, N1f - 2), XYTile<K>::NT, 0, s,
         static_cast<T *>(fine), static_cast<const T *>(tmp), N1c, N1f, N1c, P, lf.sy, lf.sz, 1, MASK ? 1 : 0);
   }
   return cudaGetLastError();
@@ -445,22 +445,22 @@ cudaError_t restrict_(const LevelGeomH &gc, const VecLayout &lc, const VecLayout
   const size_t smem = restrict_smem<T>();
   if constexpr (DIM == 2) {
     if (add)
-      restrict_xy_kernel<K, T, XYOut::AddInterior><<<dim3(gxy, gxy, 1), XYTile<K>::NT, smem, s>>>(
+      TPS_LAUNCH((restrict_xy_kernel<K, T, XYOut::AddInterior>), dim3(gxy, gxy, 1), XYTile<K>::NT, smem, s,
           static_cast<T *>(coarse), static_cast<const T *>(fine), N1c, N1f, lf.sy, 0, lc.sy, 0, 0, 1);
     else
-      restrict_xy_kernel<K, T, XYOut::SetInterior><<<dim3(gxy, gxy, 1), XYTile<K>::NT, smem, s>>>(
+      TPS_LAUNCH((restrict_xy_kernel<K, T, XYOut::SetInterior>), dim3(gxy, gxy, 1), XYTile<K>::NT, smem, s,
           static_cast<T *>(coarse), static_cast<const T *>(fine), N1c, N1f, lf.sy, 0, lc.sy, 0, 0, 1);
   } else {
     const int64_t P = static_cast<int64_t>(N1c) * N1c;
-    restrict_xy_kernel<K, T, XYOut::SetAll><<<dim3(gxy, gxy, N1f), XYTile<K>::NT, smem, s>>>(
+    TPS_LAUNCH((restrict_xy_kernel<K, T, XYOut::SetAll>), dim3(gxy, gxy, N1f), XYTile<K>::NT, smem, s,
         static_cast<T *>(tmp), static_cast<const T *>(fine), N1c, N1f, lf.sy, lf.sz, N1c, P, 0, N1f);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (add)
-      restrict_z_kernel<K, T, true><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
+      TPS_LAUNCH((restrict_z_kernel<K, T, true>), dim3(ceil_div(P, 256), gc.n), 256, 0, s,
           static_cast<T *>(coarse), static_cast<const T *>(tmp), N1c, N1f, lc.sy, lc.sz);
     else
-      restrict_z_kernel<K, T, false><<<dim3(ceil_div(P, 256), gc.n), 256, 0, s>>>(
+      TPS_LAUNCH((restrict_z_kernel<K, T, false>), dim3(ceil_div(P, 256), gc.n), 256, 0, s,
           static_cast<T *>(coarse), static_cast<const T *>(tmp), N1c, N1f, lc.sy, lc.sz);
   }
   return cudaGetLastError();
@@ -484,7 +484,7 @@ cudaError_t cell_sweep(const LevelGeomH &g, const VecLayout &l, T *dst, const T 
     cell_lattice(DIM, g.n, c, nx, ny, nz);
     const int count = nx * ny * nz;
     if (count == 0) continue;
-    cell_apply_kernel<DIM, K, T, MASS><<<count, KappaCfg<DIM, K>::NT, 0, st>>>(
+    TPS_LAUNCH((cell_apply_kernel<DIM, K, T, MASS>), count, KappaCfg<DIM, K>::NT, 0, st,
         dst, src, kappa, g.n, c, nx, ny, l.sy, l.sz, static_cast<T>(s));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -504,7 +504,7 @@ cudaError_t kappa_laplace(const LevelGeomH &g, const VecLayout &l, void *dst, co
   if (e != cudaSuccess) return e;
   // Dirichlet rows end at 0 like the unit-coefficient kernel's untouched rows
   // of zero-initialised work vectors; tps_laplace_vmult then copies src there
-  finish_residual_kernel<DIM, T><<<1184, 256, 0, st>>>(
+  TPS_LAUNCH((finish_residual_kernel<DIM, T>), 1184, 256, 0, st,
       static_cast<T *>(dst), mode == 1 ? static_cast<const T *>(rhs) : nullptr, g.N1, l.sy, l.sz);
   return cudaGetLastError();
 }
@@ -517,7 +517,7 @@ cudaError_t kappa_smoother(const LevelGeomH &g, const VecLayout &l, void *x, con
   colour_lattice(DIM, g.n, colour, nx, ny, nz, count);
   if (count == 0) return cudaSuccess;
   const double sc = stiffness_scale(DIM, g.h);
-  kappa_smoother_kernel<DIM, K, T><<<count, KSm<DIM, K, T>::NT, sizeof(T) * KSm<DIM, K, T>::ELEMS, st>>>(
+  TPS_LAUNCH((kappa_smoother_kernel<DIM, K, T>), count, KSm<DIM, K, T>::NT, sizeof(T) * KSm<DIM, K, T>::ELEMS, st,
       static_cast<T *>(x), static_cast<const T *>(b), static_cast<const T *>(kappa), g.n, colour,
       nx, ny, l.sy, l.sz, static_cast<T>(sc), static_cast<T>(1.0 / sc), static_cast<T>(omega));
   return cudaGetLastError();
@@ -539,7 +539,7 @@ cudaError_t cell_energy(const LevelGeomH &g, const VecLayout &l, double *e, cons
                         const double *lam, cudaStream_t st)
 {
   const int64_t ncell = DIM == 3 ? int64_t(g.n) * g.n * g.n : int64_t(g.n) * g.n;
-  cell_energy_kernel<DIM, K><<<static_cast<unsigned>(ncell), KappaCfg<DIM, K>::NT, 0, st>>>(
+  TPS_LAUNCH((cell_energy_kernel<DIM, K>), static_cast<unsigned>(ncell), KappaCfg<DIM, K>::NT, 0, st,
       e, u, lam, g.n, l.sy, l.sz, stiffness_scale(DIM, g.h));
   return cudaGetLastError();
 }
@@ -566,7 +566,7 @@ cudaError_t patch_residual(const LevelGeomH &g, const VecLayout &l, const void *
   const PatchColour c = patch_colour<DIM>(g, l, colour);
   if (c.count == 0) return cudaSuccess;
   using S = PVar<DIM, K>;
-  patch_residual_kernel<DIM, K, T><<<c.count, S::NT, sizeof(T) * S::RES_ELEMS, s>>>(
+  TPS_LAUNCH((patch_residual_kernel<DIM, K, T>), c.count, S::NT, sizeof(T) * S::RES_ELEMS, s,
       static_cast<const T *>(x), static_cast<const T *>(b), static_cast<T *>(r), c,
       static_cast<T>(stiffness_scale(DIM, g.h)));
   return cudaGetLastError();
@@ -579,7 +579,7 @@ cudaError_t patch_solve(const LevelGeomH &g, const VecLayout &l, void *x, const 
   const PatchColour c = patch_colour<DIM>(g, l, colour);
   if (c.count == 0) return cudaSuccess;
   using S = PVar<DIM, K>;
-  patch_solve_kernel<DIM, K, T><<<c.count, S::NT, sizeof(T) * S::SOLVE_ELEMS, s>>>(
+  TPS_LAUNCH((patch_solve_kernel<DIM, K, T>), c.count, S::NT, sizeof(T) * S::SOLVE_ELEMS, s,
       static_cast<T *>(x), static_cast<const T *>(r), static_cast<const T *>(inv), c, static_cast<T>(omega),
       static_cast<T>(1.0 / stiffness_scale(DIM, g.h)));
   return cudaGetLastError();

@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT, 2)
     laplace_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs,
                    int N1g, int64_t sy, int64_t sz, T scale)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using Tl = OpTile<DIM, K>;
   constexpr int NT = Tl::NT, WX = Tl::WX, WY = Tl::WY, WZ = Tl::WZ;
   constexpr int OX = Tl::OX, OY = Tl::OY, OZ = Tl::OZ, RX = Tl::RX;
@@ -271,6 +272,7 @@ __global__ void __launch_bounds__(OpStream<K, T>::NT, OpStream<K, T>::MINB)
     laplace3d_stream_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs,
                             int N1g, int n_cells, int64_t sy, int64_t sz, T scale, int cz)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = OpStream<K, T>;
   constexpr int NT = S::NT, WX = S::WX, WY = S::WY, OX = S::OX, OY = S::OY, PL = S::PL;
   constexpr int XS = S::XS, TS = S::TS, EPT = S::EPT;

@@ -100,6 +100,7 @@ __global__ void __launch_bounds__(SmootherShape<DIM, K>::NT)
                            int nx_c, int ny_c, int n_patches_c, int cx, int cy, int cz, T scale,
                            T inv_scale, T omega)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = SmootherShape<DIM, K>;
   constexpr int N1 = S::N1, M = S::M, PPB = S::PPB, NT = S::NT;
   const DegreeTables<K, T> &tb = c_tables<K, T>;

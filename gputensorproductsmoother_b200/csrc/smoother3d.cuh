@@ -397,6 +397,7 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
                       const T *__restrict__ b, const Sm3Args a, T scale, T fd_scale,
                       int *__restrict__ err)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = Sm3<K, T, PPB_>;
   using P2 = typename Pair<T>::type;
   constexpr int N1 = S::N1, M = S::M, W = S::W, PPB = S::PPB, NT = S::NT, AL = S::A;

@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(Tc3<K>::NT, Tc3<K>::MINB)
                          float *__restrict__ x, const Sm3Args a, float scale, float fd_scale,
                          int *__restrict__ err)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using C = Tc3<K>;
   constexpr int N1 = C::N1, M = C::M, U = C::U, NT = C::NT;
   const DegreeTables<K, float> &tb = c_tables<K, float>;

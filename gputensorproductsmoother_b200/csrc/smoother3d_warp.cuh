@@ -166,6 +166,7 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
     smoother3d_warp_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
                            T *__restrict__ x, const Sm3Args a, T scale, T fd_scale, int *__restrict__ err)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = Wp3<K, T, WARPS>;
   using Lo = typename S::L;
   using P2 = typename Pair<T>::type;

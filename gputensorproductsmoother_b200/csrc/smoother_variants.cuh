@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(PVar<DIM, K>::NT)
     patch_residual_kernel(const T *__restrict__ x, const T *__restrict__ b, T *__restrict__ r,
                           const PatchColour c, T scale)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = PVar<DIM, K>;
   constexpr int N1 = S::N1, M = S::M, NT = S::NT;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
@@ -174,6 +175,7 @@ __global__ void __launch_bounds__(PVar<DIM, K>::NT)
     patch_solve_kernel(T *__restrict__ x, const T *__restrict__ r, const T *__restrict__ inv,
                        const PatchColour c, T omega, T inv_scale)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = PVar<DIM, K>;
   constexpr int M = S::M, NT = S::NT, INT = S::INT;
   const DegreeTables<K, T> &tb = c_tables<K, T>;

@@ -11,6 +11,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "launch.cuh"
+
 namespace tps {
 
 template <int K>

@@ -87,6 +87,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
                       int64_t in_sy, int64_t in_plane, int64_t out_sy, int64_t out_plane,
                       int plane0, int mask_in)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   constexpr int C = ProlTile<K, T>::C, NT = XYTile<K>::NT;
   constexpr int WI = C * K + 1;  // coarse inputs per direction
   constexpr int WO = 2 * K * C;  // fine outputs per direction
@@ -151,6 +152,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
                        int64_t in_sy, int64_t in_plane, int64_t out_sy, int64_t out_plane,
                        int plane0, int n_planes_total)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   constexpr int C = XYTile<K>::C, NT = XYTile<K>::NT;
   constexpr int WI = 2 * K * (C + 1) + 1;  // fine inputs per direction
   constexpr int WO = C * K;                // coarse outputs per direction
@@ -215,6 +217,7 @@ template <int K, typename T, bool MASK = true>
 __global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coarse, int N1c,
                                  int N1f, int n_cells_c, int64_t c_sy, int64_t c_sz)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   const int64_t P = static_cast<int64_t>(N1c) * N1c;
   const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   const int c = blockIdx.y;  // coarse cell along z
@@ -238,6 +241,7 @@ template <int K, typename T, bool ADD>
 __global__ void restrict_z_kernel(T *__restrict__ coarse, const T *__restrict__ tmp, int N1c,
                                   int N1f, int64_t c_sy, int64_t c_sz)
 {
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   const int64_t P = static_cast<int64_t>(N1c) * N1c;
   const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   const int c = blockIdx.y;  // coarse cell along z: outputs c*k + b, b < k
