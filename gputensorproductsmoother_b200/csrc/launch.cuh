@@ -18,6 +18,12 @@
 #ifndef TPS_PDL
 #define TPS_PDL 1  // 0: plain stream-ordered launches (same kernels)
 #endif
+// 1: each CTA also allows the next kernel's launch right after its wait.
+// Measured slower (CG 64^3 FP64 24.57 vs 23.16 ms, 16^3 FP32 1.78 vs 1.65
+// ms): the waiting dependent CTAs take SM resources from the running grid.
+#ifndef TPS_PDL_EARLY
+#define TPS_PDL_EARLY 0
+#endif
 
 namespace tps {
 
@@ -25,6 +31,11 @@ __device__ __forceinline__ void griddep_wait()
 {
 #if defined(__CUDA_ARCH__)
   asm volatile("griddepcontrol.wait;" ::: "memory");
+#if TPS_PDL_EARLY
+  // the dependent grid may launch once every CTA of this grid has passed
+  // here; its CTAs then wait in their own griddep_wait() for this grid's end
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
 #endif
 }
 
