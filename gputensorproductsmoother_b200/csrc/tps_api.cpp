@@ -1316,6 +1316,12 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host, double *x_host,
                    tps_report *report)
 {
+  return tps_solve_host_guess(h, opts, b_host, x_host, x_host, report);
+}
+
+int tps_solve_host_guess(tps_handle *h, const tps_solve_opts *opts, const double *b_host, const double *x0_host,
+                         double *x_host, tps_report *report)
+{
   if (!h) return TPS_ERR_INVALID;
   if (!b_host || !x_host) {
     h->err = "null host buffer";
@@ -1331,7 +1337,10 @@ int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_ho
       h->host_x.alloc(sizeof(double) * N);
     }
     TPS_CUDA(cudaMemcpyAsync(h->host_b.p, b_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
-    TPS_CUDA(cudaMemcpyAsync(h->host_x.p, x_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    if (x0_host)
+      TPS_CUDA(cudaMemcpyAsync(h->host_x.p, x0_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+    else
+      TPS_CUDA(cudaMemsetAsync(h->host_x.p, 0, sizeof(double) * N, s));
     status = tps_solve(h, opts, h->host_b.as<double>(), h->host_x.as<double>(), report, s);
     if (status == TPS_OK || status == TPS_ERR_NOT_CONVERGED) {
       TPS_CUDA(cudaMemcpyAsync(x_host, h->host_x.p, sizeof(double) * N, cudaMemcpyDeviceToHost, s));

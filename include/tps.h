@@ -200,6 +200,12 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
  * The handle keeps two device staging vectors (16 N bytes) between calls. */
 int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
                    double *x_host, tps_report *report);
+/* The same with a separate initial guess: x0_host (N entries, may equal
+ * x_host) is copied in, or, when NULL, the solve starts from x = 0 on the
+ * device without a host-to-device copy of the guess; the solution is written
+ * to x_host.  tps_solve_host(h, o, b, x, r) is this call with x0_host = x. */
+int tps_solve_host_guess(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
+                         const double *x0_host, double *x_host, tps_report *report);
 
 /* Patches-per-batch autotuner of the 3D smoother (the reference's
  * AdditionalData::patch_per_block, include/patch_smoother.cuh:101-118, chosen
