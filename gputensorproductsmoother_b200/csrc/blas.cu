@@ -7,11 +7,13 @@
 namespace tps {
 namespace {
 
+// entry i of a lexicographic level vector in the row-padded layout (rows of
+// N1 entries sy apart); level vectors have fewer than 2^31 entries
 __device__ __forceinline__ int64_t pad_index(int64_t i, PadMap pm)
 {
   if (pm.sy == pm.N1) return i;
-  const int64_t row = i / pm.N1;
-  return row * pm.sy + (i - row * pm.N1);
+  const int row = fast_div(static_cast<int>(i), pm.m, pm.s);
+  return static_cast<int64_t>(row) * pm.sy + (i - static_cast<int64_t>(row) * pm.N1);
 }
 
 // d_kind/z_kind: 0 = FP64, 1 = FP32, 2 = FP64 rounded through FP32

@@ -7,6 +7,8 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "intdiv.cuh"
+
 namespace tps {
 
 constexpr int kRedBlocks = 592;   // 4 x 148 SMs
@@ -17,7 +19,15 @@ constexpr int kRedThreads = 512;
 struct PadMap {
   int N1;
   int64_t sy;
+  uint32_t m, s;  // i / N1 == (i * m) >> s (magic_div), for i < 2^31
 };
+
+inline PadMap make_padmap(int N1, int64_t sy)
+{
+  PadMap pm{N1, sy, 0, 0};
+  magic_div(static_cast<uint32_t>(N1), pm.m, pm.s);
+  return pm;
+}
 
 // Device-resident scalars of the CG iteration (no host round trip inside an
 // iteration, so one iteration can be captured in a CUDA graph).

@@ -515,7 +515,7 @@ void check_tc(tps_handle *h)
 PadMap fine_padmap(tps_handle *h, int p)
 {
   const VecLayout &l = h->vc[p].layout.back();
-  return PadMap{l.N1, l.sy};
+  return make_padmap(l.N1, l.sy);
 }
 
 void fine_vmult64(tps_handle *h, double *dst, const double *src, cudaStream_t s)
@@ -787,7 +787,7 @@ void fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, c
     }
     if (tmp) h->fmg_tmp.alloc(tmp);
   }
-  auto padmap = [&](int l) { return PadMap{V.layout[l].N1, V.layout[l].sy}; };
+  auto padmap = [&](int l) { return make_padmap(V.layout[l].N1, V.layout[l].sy); };
   const int zk = p == 1 ? 1 : 0;
   TPS_CUDA(cudaEventRecord(h->ev0, s));
   // coarse level: coarse solve, then one more smoother step

@@ -222,7 +222,7 @@ __global__ void prolong_z_kernel(T *__restrict__ tmp, const T *__restrict__ coar
   const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   const int c = blockIdx.y;  // coarse cell along z
   if (idx >= P) return;
-  const int gx = static_cast<int>(idx % N1c), gy = static_cast<int>(idx / N1c);
+  const int gy = static_cast<int>(idx) / N1c, gx = static_cast<int>(idx) - gy * N1c;  // idx < N1c^2 < 2^31
   const bool bxy = gx == 0 || gx == N1c - 1 || gy == 0 || gy == N1c - 1;
   T v[K + 1], o[2 * K];
 #pragma unroll
@@ -246,7 +246,7 @@ __global__ void restrict_z_kernel(T *__restrict__ coarse, const T *__restrict__ 
   const int64_t idx = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x;
   const int c = blockIdx.y;  // coarse cell along z: outputs c*k + b, b < k
   if (idx >= P) return;
-  const int gx = static_cast<int>(idx % N1c), gy = static_cast<int>(idx / N1c);
+  const int gy = static_cast<int>(idx) / N1c, gx = static_cast<int>(idx) - gy * N1c;  // idx < N1c^2 < 2^31
   if (gx == 0 || gx == N1c - 1 || gy == 0 || gy == N1c - 1) return;
   T v[4 * K + 1], o[K];
 #pragma unroll
