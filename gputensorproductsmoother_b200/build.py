@@ -23,7 +23,7 @@ OBJ_DIR = os.path.join(CSRC, "_build")
 LIB_PATH = os.path.join(PKG_DIR, "libtps.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-fopenmp",
                      "--expt-relaxed-constexpr", "-I" + os.path.join(REPO, "include"),
                      "-I" + CSRC]
 
@@ -78,7 +78,7 @@ def build(verbose: bool = False, jobs: int | None = None, extra_flags: list[str]
     newest = max(os.path.getmtime(o) for o in objs)
     if not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < newest:
         cmd = [_nvcc()] + _host_compiler() + ARCH + ["-shared", "-o", LIB_PATH] + objs + \
-            ["-lcudart"]
+            ["-lcudart", "-lgomp"]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stdout}\n{r.stderr}")

@@ -307,38 +307,56 @@ std::vector<double> dense_patch_inverse(const DegreeData &D, int dim)
       A[e * nn + f] = v;
     }
   }
-  // A = L L^T (lower triangle of A, row-major)
+  return spd_inverse(A, n);
+}
+
+std::vector<double> spd_inverse(std::vector<double> &A, int n)
+{
+  const size_t nn = static_cast<size_t>(n);
+  // A = L L^T in the lower triangle: row j, then the rows below it in parallel
   for (size_t j = 0; j < nn; ++j) {
     double s = A[j * nn + j];
     for (size_t p = 0; p < j; ++p) s -= A[j * nn + p] * A[j * nn + p];
-    if (!(s > 0.0)) throw std::runtime_error("interior patch matrix is not positive definite");
+    if (!(s > 0.0)) throw std::runtime_error("matrix is not positive definite");
     const double d = std::sqrt(s);
     A[j * nn + j] = d;
-    for (size_t i = j + 1; i < nn; ++i) {
-      double t = A[i * nn + j];
-      for (size_t p = 0; p < j; ++p) t -= A[i * nn + p] * A[j * nn + p];
-      A[i * nn + j] = t / d;
+    const double *lj = &A[j * nn];
+#pragma omp parallel for schedule(static) if (nn - j > 256)
+    for (long long i = static_cast<long long>(j) + 1; i < static_cast<long long>(nn); ++i) {
+      double *li = &A[static_cast<size_t>(i) * nn];
+      double t = li[j];
+      for (size_t p = 0; p < j; ++p) t -= li[p] * lj[p];
+      li[j] = t / d;
     }
   }
-  // WT[c][p] = (L^{-1})[p][c] for p >= c
+  // WT[c][p] = (L^{-1})[p][c] for p >= c; columns are independent
   std::vector<double> WT(nn * nn, 0.0);
-  for (size_t c = 0; c < nn; ++c) {
-    WT[c * nn + c] = 1.0 / A[c * nn + c];
+#pragma omp parallel for schedule(dynamic, 8)
+  for (long long cc = 0; cc < static_cast<long long>(nn); ++cc) {
+    const size_t c = static_cast<size_t>(cc);
+    double *w = &WT[c * nn];
+    w[c] = 1.0 / A[c * nn + c];
     for (size_t i = c + 1; i < nn; ++i) {
+      const double *li = &A[i * nn];
       double t = 0.0;
-      for (size_t p = c; p < i; ++p) t += A[i * nn + p] * WT[c * nn + p];
-      WT[c * nn + i] = -t / A[i * nn + i];
+      for (size_t p = c; p < i; ++p) t += li[p] * w[p];
+      w[i] = -t / li[i];
     }
   }
-  // A^{-1} = L^{-T} L^{-1}: inv[i][j] = sum over p >= max(i, j) of W[p][i] W[p][j]
+  // A^{-1}[i][j] = sum over p >= max(i, j) of W[p][i] W[p][j]
   std::vector<double> inv(nn * nn);
-  for (size_t i = 0; i < nn; ++i)
+#pragma omp parallel for schedule(dynamic, 8)
+  for (long long ii = 0; ii < static_cast<long long>(nn); ++ii) {
+    const size_t i = static_cast<size_t>(ii);
+    const double *wi = &WT[i * nn];
     for (size_t j = i; j < nn; ++j) {
+      const double *wj = &WT[j * nn];
       double t = 0.0;
-      for (size_t p = j; p < nn; ++p) t += WT[i * nn + p] * WT[j * nn + p];
+      for (size_t p = j; p < nn; ++p) t += wi[p] * wj[p];
       inv[i * nn + j] = t;
       inv[j * nn + i] = t;
     }
+  }
   return inv;
 }
 

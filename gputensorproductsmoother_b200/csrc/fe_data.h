@@ -39,6 +39,12 @@ DegreeData make_degree_data(int k);
 // the full symmetric inverse, row-major.
 std::vector<double> dense_patch_inverse(const DegreeData &D, int dim);
 
+// Inverse of the symmetric positive definite n x n matrix A (row-major,
+// overwritten): Cholesky factorisation A = L L^T, W = L^{-1}, A^{-1} = W^T W,
+// every inner product over contiguous rows, independent rows on host threads
+// (OpenMP).  Throws std::runtime_error if A is not positive definite.
+std::vector<double> spd_inverse(std::vector<double> &A, int n);
+
 // Symmetric-definite generalized eigenproblem A v = lambda B v (FP64,
 // Cholesky + cyclic Jacobi); V column-major-as-rows like DegreeData::evec.
 void generalized_eigen(int m, const double *A, const double *B, double *V, double *lambda);

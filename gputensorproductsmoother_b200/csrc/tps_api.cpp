@@ -253,33 +253,12 @@ void build_dense_coarse(tps_handle *h)
       }
     }
   }
-  // Cholesky and explicit inverse (coarse systems hold at most a few thousand DoFs)
-  std::vector<double> &L = A;
-  for (int j = 0; j < ni; ++j) {
-    double d = L[static_cast<size_t>(j) * ni + j];
-    for (int p = 0; p < j; ++p) d -= L[static_cast<size_t>(j) * ni + p] * L[static_cast<size_t>(j) * ni + p];
-    if (!(d > 0)) throw ApiError(TPS_ERR_INVALID, "coarse operator not positive definite");
-    d = std::sqrt(d);
-    L[static_cast<size_t>(j) * ni + j] = d;
-    for (int i = j + 1; i < ni; ++i) {
-      double t = L[static_cast<size_t>(i) * ni + j];
-      for (int p = 0; p < j; ++p) t -= L[static_cast<size_t>(i) * ni + p] * L[static_cast<size_t>(j) * ni + p];
-      L[static_cast<size_t>(i) * ni + j] = t / d;
-    }
-  }
-  std::vector<double> inv(static_cast<size_t>(ni) * ni, 0.0), col(ni);
-  for (int c = 0; c < ni; ++c) {
-    for (int i = 0; i < ni; ++i) {
-      double t = i == c ? 1.0 : 0.0;
-      for (int p = 0; p < i; ++p) t -= L[static_cast<size_t>(i) * ni + p] * col[p];
-      col[i] = t / L[static_cast<size_t>(i) * ni + i];
-    }
-    for (int i = ni - 1; i >= 0; --i) {
-      double t = col[i];
-      for (int p = i + 1; p < ni; ++p) t -= L[static_cast<size_t>(p) * ni + i] * col[p];
-      col[i] = t / L[static_cast<size_t>(i) * ni + i];
-    }
-    for (int i = 0; i < ni; ++i) inv[static_cast<size_t>(i) * ni + c] = col[i];
+  // explicit inverse (coarse systems hold at most a few thousand DoFs)
+  std::vector<double> inv;
+  try {
+    inv = spd_inverse(A, ni);
+  } catch (const std::runtime_error &) {
+    throw ApiError(TPS_ERR_INVALID, "coarse operator not positive definite");
   }
   h->coarse_inv_host = std::move(inv);
   h->coarse_coord.resize(3 * static_cast<size_t>(ni));
