@@ -257,13 +257,20 @@ __global__ void __launch_bounds__(KappaCfg<DIM, K>::NT)
 template <int DIM, int K, typename T>
 struct KSm {
   static constexpr int NP = K + 1, N1 = 2 * K + 1, M = 2 * K - 1;
+  static constexpr int NC = 1 << DIM;  // cells of a patch
   static constexpr int BOX = DIM == 3 ? N1 * N1 * N1 : N1 * N1;
   static constexpr int INT = DIM == 3 ? M * M * M : M * M;
   static constexpr int CELL = DIM == 3 ? NP * NP * NP : NP * NP;
-  static constexpr int NT = 128;
-  static constexpr int ELEMS = 2 * BOX + 4 * CELL + 2 * INT;
+  static constexpr int NT = DIM == 3 ? 256 : 128;
+  // X[BOX] | TA | TB | UA | UB (NC cells each); the local solve reuses UA, UB
+  static constexpr int ELEMS = BOX + 4 * NC * CELL;
+  static_assert(NC * CELL >= INT, "the local-solve buffers live in the cell buffers");
 };
 
+// kappa patch smoother: one CTA per patch.  The box residual is assembled
+// from the 2^d cells of the patch contracted at once (each 1D stage has a
+// line task per cell and line, so the CTA's threads share all cells' work),
+// the per-cell results are combined per interior node, then the local solve.
 template <int DIM, int K, typename T>
 __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
     kappa_smoother_kernel(T *__restrict__ x, const T *__restrict__ b, const T *__restrict__ kappa,
@@ -272,13 +279,13 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
 {
   griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = KSm<DIM, K, T>;
-  constexpr int NP = S::NP, N1 = S::N1, M = S::M, NT = S::NT;
+  constexpr int NP = S::NP, N1 = S::N1, M = S::M, NT = S::NT, NC = S::NC, CELL = S::CELL;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ T kps[NC];  // the patch cells' coefficients (indexed by run-time cell)
   T *X = reinterpret_cast<T *>(smem_raw);
-  T *R = X + S::BOX;  // box accumulator of A(kappa) x
-  T *cin = R + S::BOX, *cout_ = cin + S::CELL, *t1 = cout_ + S::CELL, *t2 = t1 + S::CELL;
-  T *Q1 = t2 + S::CELL, *Q2 = Q1 + S::INT;
+  T *TA = X + S::BOX, *TB = TA + NC * CELL, *UA = TB + NC * CELL, *UB = UA + NC * CELL;
+  T *Q1 = UA, *Q2 = UB;  // local solve, after the residual is assembled
   const int j = blockIdx.x;
   const int px = (colour & 1) + 2 * (j % nx_c);
   const int py = ((colour >> 1) & 1) + 2 * (DIM == 3 ? (j / nx_c) % ny_c : j / nx_c);
@@ -287,35 +294,120 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
   for (int l = threadIdx.x; l < S::BOX; l += NT) {
     const int lx = l % N1, ly = (l / N1) % N1, lz = DIM == 3 ? l / (N1 * N1) : 0;
     X[l] = x[first + lx + ly * sy + lz * sz];
-    R[l] = T(0);
+  }
+  T kpat[NC];
+#pragma unroll
+  for (int cc = 0; cc < NC; ++cc) {
+    const int ox = cc & 1, oy = (cc >> 1) & 1, oz = (cc >> 2) & 1;
+    kpat[cc] = kappa[int64_t(px + ox) + int64_t(py + oy) * n + (DIM == 3 ? int64_t(pz + oz) * n * n : 0)];
+  }
+  if (threadIdx.x < NC) {
+#pragma unroll
+    for (int cc = 0; cc < NC; ++cc)
+      if (cc == threadIdx.x) kps[cc] = kpat[cc];
   }
   __syncthreads();
-  T kpat[1 << DIM];
-  for (int cc = 0; cc < (1 << DIM); ++cc) {
+  constexpr int LINES = CELL / NP;  // lines of one cell along one direction
+  // x: TA = M_x x_c, TB = L_x x_c, per cell [c][z][y][x]
+  for (int t = threadIdx.x; t < NC * LINES; t += NT) {
+    const int cc = t / LINES, r = t % LINES;
     const int ox = cc & 1, oy = (cc >> 1) & 1, oz = (cc >> 2) & 1;
-    const int64_t cidx = int64_t(px + ox) + int64_t(py + oy) * n +
-                         (DIM == 3 ? int64_t(pz + oz) * n * n : 0);
-    const T kc = kappa[cidx];
-    kpat[cc] = kc;
-    for (int l = threadIdx.x; l < S::CELL; l += NT) {
-      const int lx = l % NP, ly = (l / NP) % NP, lz = DIM == 3 ? l / (NP * NP) : 0;
-      cin[l] = X[(lx + ox * K) + (ly + oy * K) * N1 + (lz + oz * K) * N1 * N1];
+    const int yl = r % NP, zl = DIM == 3 ? r / NP : 0;
+    const T *src = X + (DIM == 3 ? (oz * K + zl) * N1 * N1 : 0) + (oy * K + yl) * N1 + ox * K;
+    T v[NP];
+#pragma unroll
+    for (int q = 0; q < NP; ++q) v[q] = src[q];
+    T *da = TA + cc * CELL + r * NP, *db = TB + cc * CELL + r * NP;
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      T a = T(0), c = T(0);
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        a += tb.cmass[i * NP + q] * v[q];
+        c += tb.clap[i * NP + q] * v[q];
+      }
+      da[i] = a;
+      db[i] = c;
     }
-    __syncthreads();
-    cell_local_apply<DIM, K, T>(cin, cout_, t1, t2, s * kc, threadIdx.x, NT);
-    for (int l = threadIdx.x; l < S::CELL; l += NT) {
-      const int lx = l % NP, ly = (l / NP) % NP, lz = DIM == 3 ? l / (NP * NP) : 0;
-      R[(lx + ox * K) + (ly + oy * K) * N1 + (lz + oz * K) * N1 * N1] += cout_[l];
-    }
-    __syncthreads();
   }
+  __syncthreads();
+  if constexpr (DIM == 3) {
+    // y: UA = M_y TA, UB = L_y TA + M_y TB
+    for (int t = threadIdx.x; t < NC * LINES; t += NT) {
+      const int cc = t / LINES, r = t % LINES;
+      const int xl = r % NP, zl = r / NP;
+      const T *sa = TA + cc * CELL + zl * NP * NP + xl, *sb = TB + cc * CELL + zl * NP * NP + xl;
+      T va[NP], vb[NP];
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        va[q] = sa[q * NP];
+        vb[q] = sb[q * NP];
+      }
+      T *da = UA + cc * CELL + zl * NP * NP + xl, *db = UB + cc * CELL + zl * NP * NP + xl;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        T a = T(0), c = T(0);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) {
+          a += tb.cmass[i * NP + q] * va[q];
+          c += tb.clap[i * NP + q] * va[q] + tb.cmass[i * NP + q] * vb[q];
+        }
+        da[i * NP] = a;
+        db[i * NP] = c;
+      }
+    }
+    __syncthreads();
+    // z: TA = s kappa_c (L_z UA + M_z UB) = the cell's A_c x_c
+    for (int t = threadIdx.x; t < NC * LINES; t += NT) {
+      const int cc = t / LINES, r = t % LINES;
+      const T *sa = UA + cc * CELL + r, *sb = UB + cc * CELL + r;
+      T va[NP], vb[NP];
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        va[q] = sa[q * NP * NP];
+        vb[q] = sb[q * NP * NP];
+      }
+      const T sk = s * kps[cc];
+      T *d = TA + cc * CELL + r;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        T a = T(0);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) a += tb.clap[i * NP + q] * va[q] + tb.cmass[i * NP + q] * vb[q];
+        d[i * NP * NP] = sk * a;
+      }
+    }
+  } else {
+    // y: UA = s kappa_c (L_y TA + M_y TB)
+    for (int t = threadIdx.x; t < NC * LINES; t += NT) {
+      const int cc = t / LINES, xl = t % LINES;
+      const T *sa = TA + cc * CELL + xl, *sb = TB + cc * CELL + xl;
+      T va[NP], vb[NP];
+#pragma unroll
+      for (int q = 0; q < NP; ++q) {
+        va[q] = sa[q * NP];
+        vb[q] = sb[q * NP];
+      }
+      const T sk = s * kps[cc];
+      T *d = UA + cc * CELL + xl;
+#pragma unroll
+      for (int i = 0; i < NP; ++i) {
+        T a = T(0);
+#pragma unroll
+        for (int q = 0; q < NP; ++q) a += tb.clap[i * NP + q] * va[q] + tb.cmass[i * NP + q] * vb[q];
+        d[i * NP] = sk * a;
+      }
+    }
+  }
+  __syncthreads();
+  const T *OUT = DIM == 3 ? TA : UA;
   // D^-1/2 of interior DoF l: mean kappa of the patch cells containing it
   auto dinv_sqrt = [&](int l) -> T {
     const int c3[3] = {l % M + 1, (l / M) % M + 1, DIM == 3 ? l / (M * M) + 1 : 0};
     T acc = T(0);
     int cnt = 0;
 #pragma unroll
-    for (int cc = 0; cc < (1 << DIM); ++cc) {
+    for (int cc = 0; cc < NC; ++cc) {
       bool in = true;
 #pragma unroll
       for (int d = 0; d < DIM; ++d) {
@@ -329,10 +421,42 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
     }
     return T(1) / sqrt(acc / T(cnt));
   };
-  // interior residual r = D^-1/2 (b_I - (A(kappa) x)_I) into Q1 (lexicographic m^d)
-  for (int l = threadIdx.x; l < S::INT; l += NT) {
-    const int lx = l % M + 1, ly = (l / M) % M + 1, lz = DIM == 3 ? l / (M * M) + 1 : 0;
-    Q1[l] = (b[first + lx + ly * sy + lz * sz] - R[lx + ly * N1 + lz * N1 * N1]) * dinv_sqrt(l);
+  // (A(kappa) x)_l of interior node l: the sum over the patch cells containing it
+  auto ax_node = [&](int l) -> T {
+    const int c3[3] = {l % M + 1, (l / M) % M + 1, DIM == 3 ? l / (M * M) + 1 : 0};
+    T acc = T(0);
+#pragma unroll
+    for (int cc = 0; cc < NC; ++cc) {
+      bool in = true;
+      int li = 0, mul = 1;
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        const int o = (cc >> d) & 1;
+        in = in && !(o == 0 && c3[d] > K) && !(o == 1 && c3[d] < K);
+        li += (c3[d] - o * K) * mul;
+        mul *= NP;
+      }
+      if (in) acc += OUT[cc * CELL + li];
+    }
+    return acc;
+  };
+  // interior residual r = D^-1/2 (b_I - (A(kappa) x)_I); Q1 overlaps the cell
+  // results in 2D, so all of them are combined before Q1 is written
+  constexpr int RU = (S::INT + NT - 1) / NT;
+  T rloc[RU];
+#pragma unroll
+  for (int u = 0; u < RU; ++u) {
+    const int l = threadIdx.x + u * NT;
+    if (l < S::INT) {
+      const int lx = l % M + 1, ly = (l / M) % M + 1, lz = DIM == 3 ? l / (M * M) + 1 : 0;
+      rloc[u] = (b[first + lx + ly * sy + lz * sz] - ax_node(l)) * dinv_sqrt(l);
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < RU; ++u) {
+    const int l = threadIdx.x + u * NT;
+    if (l < S::INT) Q1[l] = rloc[u];
   }
   __syncthreads();
   // fast diagonalization: S^T along each direction, scale, S back (ping-pong Q1/Q2)
