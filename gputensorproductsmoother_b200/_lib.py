@@ -21,7 +21,7 @@ TPS_F64, TPS_F32, TPS_TF32 = 0, 1, 2
 VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32 = 0, 1, 2, 3
 DRIVER_CG, DRIVER_GMRES = 0, 1
 SMOOTHER_VARIANTS = 4  # TPS_SMOOTHER_VARIANTS
-SMOOTHER_FUSED, SMOOTHER_SEPARATE, SMOOTHER_GLOBAL, SMOOTHER_EXACT = 0, 1, 2, 3
+SMOOTHER_FUSED, SMOOTHER_SEPARATE, SMOOTHER_GLOBAL, SMOOTHER_EXACT, SMOOTHER_ADDITIVE = 0, 1, 2, 3, 4
 MAX_HISTORY = 256
 
 
@@ -87,6 +87,7 @@ SIGNATURES = [
     ("tps_smoother_variants", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_set_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tps_get_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("tps_set_smoother_kind", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double]),
     ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("tps_batch_destroy", ctypes.c_int, [_VP]),
     ("tps_batch_last_error", ctypes.c_char_p, [_VP]),

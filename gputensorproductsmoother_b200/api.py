@@ -120,6 +120,14 @@ class PoissonProblem:
                 self.handle)
         return list(out)
 
+    def set_smoother_kind(self, kind: str = "fused", damping: float = 0.0) -> None:
+        """Smoothing of the V-cycle's levels >= 1: "fused" (the reference's
+        coloured multiplicative sweep, the default) or "additive" (the
+        additive vertex-patch Schwarz step, damping in [0, 2/2^dim), 0 selects
+        1/2^dim).  The coarse solve is unchanged."""
+        code = {"fused": L.SMOOTHER_FUSED, "additive": L.SMOOTHER_ADDITIVE}[kind]
+        L.check(L.lib().tps_set_smoother_kind(self.handle, code, float(damping)), self.handle)
+
     def smoother_variant(self, level: int | None = None, dtype: str = "fp32") -> int:
         """The 3D smoother variant the level's sweeps use now (set, autotuned
         or the library default)."""
@@ -228,10 +236,12 @@ class PatchSmoother:
     default kernels), or the separate-kernel cross-checks "separate" (patch
     residual kernel + fast-diagonalisation kernel), "global" (level operator
     residual + fast diagonalisation) and "exact" (patch residual + dense
-    inverse of the interior patch matrix)."""
+    inverse of the interior patch matrix); "additive" is the additive
+    vertex-patch Schwarz step (no reference counterpart), damped by the
+    problem's additive damping (PoissonProblem.set_smoother_kind)."""
 
     VARIANTS = {"fused": L.SMOOTHER_FUSED, "separate": L.SMOOTHER_SEPARATE, "global": L.SMOOTHER_GLOBAL,
-                "exact": L.SMOOTHER_EXACT}
+                "exact": L.SMOOTHER_EXACT, "additive": L.SMOOTHER_ADDITIVE}
 
     def __init__(self, problem: PoissonProblem, level: int | None = None, tensor_cores: bool = False,
                  variant: str = "fused"):

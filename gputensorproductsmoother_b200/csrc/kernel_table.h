@@ -99,6 +99,8 @@ struct KernelTable {
                                       void *r, int colour, cudaStream_t);
   cudaError_t (*patch_solve[2][2])(const LevelGeomH &, const VecLayout &, void *x, const void *r,
                                    const void *inv, int colour, double omega, cudaStream_t);
+  // x += w a over n entries ([dtype])
+  cudaError_t (*scaled_add[2])(void *x, const void *a, double w, int64_t n, cudaStream_t);
 };
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no libcuda

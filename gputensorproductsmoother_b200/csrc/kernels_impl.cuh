@@ -585,6 +585,15 @@ cudaError_t patch_solve(const LevelGeomH &g, const VecLayout &l, void *x, const 
   return cudaGetLastError();
 }
 
+template <typename T>
+cudaError_t scaled_add(void *x, const void *a, double w, int64_t n, cudaStream_t s)
+{
+  const int64_t blocks = (n + 255) / 256;
+  TPS_LAUNCH((scaled_add_kernel<T>), static_cast<unsigned>(blocks < 4 * 148 ? blocks : 4 * 148), 256, 0, s,
+             static_cast<T *>(x), static_cast<const T *>(a), static_cast<T>(w), n);
+  return cudaGetLastError();
+}
+
 }  // namespace deg_impl
 }  // namespace
 
@@ -621,6 +630,7 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
      {&deg_impl::patch_residual<3, double>, &deg_impl::patch_residual<3, float>}},
     {{&deg_impl::patch_solve<2, double>, &deg_impl::patch_solve<2, float>},
      {&deg_impl::patch_solve<3, double>, &deg_impl::patch_solve<3, float>}},
+    {&deg_impl::scaled_add<double>, &deg_impl::scaled_add<float>},
 };
 
 }  // namespace tps

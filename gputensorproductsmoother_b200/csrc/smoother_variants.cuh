@@ -224,4 +224,14 @@ __global__ void __launch_bounds__(PVar<DIM, K>::NT)
   }
 }
 
+// x += w a over n entries (the additive step's damped correction)
+template <typename T>
+__global__ void scaled_add_kernel(T *__restrict__ x, const T *__restrict__ a, T w, int64_t n)
+{
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
+  for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < n;
+       i += static_cast<int64_t>(gridDim.x) * blockDim.x)
+    x[i] += w * a[i];
+}
+
 }  // namespace tps

@@ -151,6 +151,9 @@ struct tps_handle {
   std::vector<std::unique_ptr<DevBuf>> fmg_sol, fmg_res;  // FMG: FP64 per level (lexicographic)
   DevBuf fmg_tmp;                                        // FMG: FP64 transfer scratch
   DevBuf var_r[2];      // separate-kernel smoother variants: residual of the finest-level size
+  DevBuf var_acc[2];    // additive step: the summed patch solves
+  int sm_kind = TPS_SMOOTHER_FUSED;  // V-cycle smoothing on levels >= 1
+  double add_omega = 0.0;            // additive damping (0: 1/2^dim)
   DevBuf dense_inv[2];  // Exact variant: reference-cell interior patch inverse [FP64, FP32]
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 
@@ -447,6 +450,60 @@ void coarse_solve(tps_handle *h, int p, cudaStream_t s, bool tc)
   }
 }
 
+// entries of a level vector in layout lay, row padding included
+int64_t layout_elems(const tps_handle *h, const VecLayout &lay)
+{
+  return h->dim == 3 ? lay.sz * lay.N1 : lay.sy * lay.N1;
+}
+
+// the additive step's scratch vectors of precision p, sized for the finest
+// level in any layout (rows are padded by fewer than 4 entries); allocated
+// before any graph capture by tps_set_smoother_kind
+void ensure_additive_scratch(tps_handle *h, int p)
+{
+  const int64_t N1 = h->fine().N1;
+  const int64_t n = h->dim == 3 ? (N1 + 4) * N1 * N1 : (N1 + 4) * N1;
+  const size_t bytes = (p == 0 ? 8 : 4) * static_cast<size_t>(n);
+  if (h->var_r[p].bytes < bytes) h->var_r[p].alloc(bytes);
+  if (h->var_acc[p].bytes < bytes) h->var_acc[p].alloc(bytes);
+}
+
+double additive_omega(const tps_handle *h) { return h->add_omega > 0 ? h->add_omega : 1.0 / (1 << h->dim); }
+
+// Additive vertex-patch Schwarz step (no reference counterpart; the
+// reference's sweep is the coloured multiplicative one): r = b - A x (r = b
+// when x == 0), acc = the sum over all patches of A_II^{-1} r_I (the patch
+// solve with omega 1 adds into the zeroed acc colour by colour, so no two
+// writes of one launch meet: deterministic), x += omega acc.
+void additive_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void *x, const void *b, bool x_zero,
+                    cudaStream_t s)
+{
+  if (h->has_kappa) throw ApiError(TPS_ERR_UNSUPPORTED, "the additive step has a constant coefficient");
+  ensure_additive_scratch(h, p);
+  const LevelGeomH &g = h->lv[level];
+  const size_t es = p == 0 ? 8 : 4;
+  const int64_t n = layout_elems(h, lay);
+  const void *r = b;
+  if (!x_zero) {
+    level_laplace(h, level, p, lay, h->var_r[p].p, x, b, 1, s);
+    r = h->var_r[p].p;
+  }
+  TPS_CUDA(cudaMemsetAsync(h->var_acc[p].p, 0, es * static_cast<size_t>(n), s));
+  for (int c = 0; c < (1 << h->dim); ++c)
+    TPS_CUDA(h->kt->patch_solve[h->dim - 2][p](g, lay, h->var_acc[p].p, r, nullptr, c, 1.0, s));
+  TPS_CUDA(h->kt->scaled_add[p](x, h->var_acc[p].p, additive_omega(h), n, s));
+}
+
+// the V-cycle's smoothing on levels >= 1: the additive step when selected
+void level_smooth(tps_handle *h, int level, int p, const VecLayout &lay, void *x, const void *b, bool reverse,
+                  bool x_zero, const SmootherMaps *maps, cudaStream_t s, bool tc)
+{
+  if (h->sm_kind == TPS_SMOOTHER_ADDITIVE)
+    additive_sweep(h, level, p, lay, x, b, x_zero, s);
+  else
+    smoother_sweep(h, level, p, lay, x, b, reverse, x_zero, maps, s, tc);
+}
+
 // MultigridSolvers::v_cycle (include/solver.cuh:1952-2001) on precision p:
 // input d[level], output su[level]; tc: FP32 3D sweeps on the tensor cores;
 // zero_init = false continues from the current su[level] (a further cycle of
@@ -463,15 +520,14 @@ void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s,
   const VecLayout &lay = V.layout[level], &lc = V.layout[level - 1];
   const int di = h->dim - 2;
   if (zero_init) TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, V.su[level]->bytes, s));
-  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, zero_init, &V.maps[level], s, tc);
+  level_smooth(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, zero_init, &V.maps[level], s, tc);
   level_laplace(h, level, p, lay, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s);
   TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], lc, lay, V.d[level - 1]->p, V.t[level]->p,
                                    V.tmp[level]->p, 0, s));
   vcycle_rec(h, level - 1, p, symmetric, s, tc);
   TPS_CUDA(h->kt->prolong[di][p](h->lv[level - 1], lc, lay, V.su[level]->p, V.su[level - 1]->p,
                                  V.tmp[level]->p, s));
-  smoother_sweep(h, level, p, lay, V.su[level]->p, V.d[level]->p, symmetric, false,
-                 &V.maps[level], s, tc);
+  level_smooth(h, level, p, lay, V.su[level]->p, V.d[level]->p, symmetric, false, &V.maps[level], s, tc);
 }
 
 int vprec_index(int precision)
@@ -1064,7 +1120,8 @@ int tps_smoother_step_variant(tps_handle *h, int level, int dtype, void *x, cons
     check_level(h, level);
     if (!x || !b) throw ApiError(TPS_ERR_INVALID, "null vector");
     if (x == b) throw ApiError(TPS_ERR_INVALID, "x and b must not alias");
-    if (variant != TPS_SMOOTHER_SEPARATE && variant != TPS_SMOOTHER_GLOBAL && variant != TPS_SMOOTHER_EXACT)
+    if (variant != TPS_SMOOTHER_SEPARATE && variant != TPS_SMOOTHER_GLOBAL && variant != TPS_SMOOTHER_EXACT &&
+        variant != TPS_SMOOTHER_ADDITIVE)
       throw ApiError(TPS_ERR_INVALID, "unknown smoother variant");
     if (h->has_kappa)
       throw ApiError(TPS_ERR_UNSUPPORTED, "the separate-kernel smoother variants have constant coefficients");
@@ -1090,6 +1147,10 @@ int tps_smoother_step_variant(tps_handle *h, int level, int dtype, void *x, cons
       inv = h->dense_inv[p].p;
     }
     if (zero_init) TPS_CUDA(cudaMemsetAsync(x, 0, es * g.N, s));
+    if (variant == TPS_SMOOTHER_ADDITIVE) {
+      additive_sweep(h, level, p, lay, x, b, zero_init != 0, s);
+      return;
+    }
     const int nc = 1 << h->dim;
     for (int i = 0; i < nc; ++i) {
       const int c = reverse ? nc - 1 - i : i;
@@ -1241,6 +1302,31 @@ int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant)
     if (variant < 0 || variant >= kSmootherVariants) throw ApiError(TPS_ERR_INVALID, "variant out of range");
     if (static_cast<int>(h->sm_variant[p].size()) != h->n_levels) h->sm_variant[p].assign(h->n_levels, 0);
     h->sm_variant[p][level] = variant;
+    if (h->graph) {  // later solves re-capture with the chosen kernel
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+  });
+}
+
+int tps_set_smoother_kind(tps_handle *h, int kind, double damping)
+{
+  return guarded(h, [&] {
+    if (kind != TPS_SMOOTHER_FUSED && kind != TPS_SMOOTHER_ADDITIVE)
+      throw ApiError(TPS_ERR_INVALID, "kind must be TPS_SMOOTHER_FUSED or TPS_SMOOTHER_ADDITIVE");
+    if (kind == TPS_SMOOTHER_ADDITIVE) {
+      if (h->has_kappa) throw ApiError(TPS_ERR_UNSUPPORTED, "the additive step has a constant coefficient");
+      if (!(damping >= 0.0 && damping < 2.0 / (1 << h->dim)))
+        throw ApiError(TPS_ERR_INVALID, "additive damping must lie in [0, 2/2^dim) (0: 1/2^dim)");
+      h->add_omega = damping;
+      ensure_additive_scratch(h, 0);
+      ensure_additive_scratch(h, 1);
+    }
+    h->sm_kind = kind;
+    if (h->graph) {  // a captured CG iteration holds the previous smoothing
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
   });
 }
 
@@ -1262,6 +1348,10 @@ int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level)
     if (!h->own_stream) TPS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     autotune_levels(h, p, h->own_stream);
     TPS_CUDA(cudaStreamSynchronize(h->own_stream));
+    if (h->graph) {  // later solves re-capture with the chosen kernels
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
     if (ppb_per_level)
       for (int l = 0; l < h->n_levels; ++l)
         ppb_per_level[l] = h->kt->smoother_ppb(h->dim, p == 0 ? 0 : 1, h->sm_variant[p][l]);

@@ -96,8 +96,21 @@ int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *
 #define TPS_SMOOTHER_SEPARATE 1
 #define TPS_SMOOTHER_GLOBAL 2
 #define TPS_SMOOTHER_EXACT 3
+/* Additive vertex-patch Schwarz step (no reference counterpart: the reference
+ * sweep is multiplicative; the benchmark's 2D configuration names the additive
+ * form): x <- x + omega sum_p R_p^T A_p,II^{-1} R_p (b - A x), every patch's
+ * residual from the same x, the handle's additive damping omega (see
+ * tps_set_smoother_kind).  reverse is ignored; constant coefficient. */
+#define TPS_SMOOTHER_ADDITIVE 4
 int tps_smoother_step_variant(tps_handle *h, int level, int dtype, void *x, const void *b,
                               int zero_init, int reverse, int variant, void *stream);
+/* Smoothing of the V-cycle's levels >= 1 (the coarse solve is unchanged):
+ * TPS_SMOOTHER_FUSED (the default, the reference's coloured sweep) or
+ * TPS_SMOOTHER_ADDITIVE with damping omega in [0, 2/2^dim) (the additive step
+ * converges below 2/2^dim, since at most 2^dim patch colours overlap; 0
+ * selects 1/2^dim).  Applies to later solves, V-cycles and FMG of this handle
+ * and allocates the additive step's two scratch vectors. */
+int tps_set_smoother_kind(tps_handle *h, int kind, double damping);
 
 /* MGTransferCUDA::prolongate_and_add / restrict_and_add
  * (include/cuda_mg_transfer.template.cuh:575-671).  to_level / from_level is the

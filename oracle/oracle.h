@@ -33,7 +33,9 @@ int orc_patch_eigen(int k, double h, double *S, double *lam);
                               const double *kappa);                                    \
   void orc_prolongate_add##SUF(int dim, int k, int nc, REAL *fine, const REAL *coarse); \
   void orc_prolongate_add_nb##SUF(int dim, int k, int nc, REAL *fine, const REAL *coarse); \
-  void orc_restrict_add##SUF(int dim, int k, int nc, REAL *coarse, const REAL *fine);
+  void orc_restrict_add##SUF(int dim, int k, int nc, REAL *coarse, const REAL *fine); \
+  void orc_smoother_additive##SUF(int dim, int k, int n, double omega, REAL *x,        \
+                                  const REAL *b, int zero_init);
 ORC_LEVEL_DECL(_d, double)
 ORC_LEVEL_DECL(_f, float)
 #undef ORC_LEVEL_DECL
@@ -46,6 +48,10 @@ long orc_hier_ndofs(const orc_hier *H, int level);
 /* precision: 0 = FP64 V-cycle, 1 = FP32 V-cycle, 2 = FP64 V-cycle whose input
  * is rounded to FP32 precision first (the reference's "double" V-cycle). */
 void orc_vcycle(orc_hier *H, int precision, int symmetric, double *dst, const double *src);
+/* V-cycle smoothing on levels >= 1 by the additive step with damping omega
+ * (on != 0) instead of the coloured multiplicative sweep (the coarse solve
+ * is unchanged) */
+void orc_hier_set_additive(orc_hier *H, int on, double omega);
 void orc_vcycle_level(orc_hier *H, int precision, int symmetric, int level, double *dst,
                       const double *src);
 void orc_fine_vmult(orc_hier *H, double *dst, const double *src);

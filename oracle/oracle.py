@@ -47,6 +47,9 @@ def lib():
             getattr(L, "orc_smoother_step" + suf).argtypes = [
                 ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ptr, ptr,
                 ctypes.c_int, ctypes.c_int, _dp]
+            getattr(L, "orc_smoother_additive" + suf).argtypes = [
+                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                ctypes.c_int]
             getattr(L, "orc_prolongate_add" + suf).argtypes = [
                 ctypes.c_int, ctypes.c_int, ctypes.c_int, ptr, ptr]
             getattr(L, "orc_restrict_add" + suf).argtypes = [
@@ -54,6 +57,7 @@ def lib():
         L.orc_hier_create.restype = ctypes.c_void_p
         L.orc_hier_create.argtypes = [ctypes.c_int] * 4 + [_dp]
         L.orc_hier_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_hier_set_additive.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_double]
         L.orc_hier_ndofs.restype = ctypes.c_long
         L.orc_hier_ndofs.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.orc_vcycle.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp]
@@ -142,6 +146,15 @@ def smoother_step(dim, k, n, x, b, omega=1.0, zero_init=False, reverse=False, ka
     return x
 
 
+def smoother_additive(dim, k, n, x, b, omega, zero_init=False):
+    """Additive vertex-patch Schwarz step on a copy of x (every patch's residual
+    from the old x, solves summed, x += omega * sum); returns the new x."""
+    x = np.array(x, copy=True)
+    b = np.ascontiguousarray(b, dtype=x.dtype)
+    getattr(lib(), "orc_smoother_additive" + _sfx(x.dtype))(dim, k, n, omega, _p(x), _p(b), int(zero_init))
+    return x
+
+
 def prolongate_add(dim, k, nc, fine, coarse):
     fine = np.array(fine, copy=True)
     coarse = np.ascontiguousarray(coarse, dtype=fine.dtype)
@@ -180,6 +193,11 @@ class Hierarchy:
         dst = np.zeros_like(src)
         lib().orc_fine_vmult(self.h, _p(dst), _p(src))
         return dst
+
+    def set_additive(self, omega):
+        """Smooth levels >= 1 of later V-cycles with the additive step (damping
+        omega); omega None restores the coloured sweep."""
+        lib().orc_hier_set_additive(self.h, 0 if omega is None else 1, 0.0 if omega is None else omega)
 
     def vcycle(self, src, precision=0, symmetric=False, level=None):
         src = np.ascontiguousarray(src, dtype=np.float64)

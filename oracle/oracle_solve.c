@@ -34,6 +34,8 @@ struct orc_hier {
   double *d64[3];   /* scratch per level group: allocated per level below */
   double **dd, **sud, **td;  /* FP64 V-cycle vectors */
   float **df, **suf, **tf;   /* FP32 V-cycle vectors */
+  int additive;       /* additive smoothing on levels >= 1 */
+  double add_omega;
   /* dense coarse factor */
   int use_dense_coarse;
   long n_int_coarse;
@@ -52,6 +54,12 @@ static int is_boundary(int dim, int N1, long i)
 {
   int x = (int)(i % N1), y = (int)((i / N1) % N1), z = dim == 3 ? (int)(i / ((long)N1 * N1)) : 0;
   return x == 0 || x == N1 - 1 || y == 0 || y == N1 - 1 || (dim == 3 && (z == 0 || z == N1 - 1));
+}
+
+void orc_hier_set_additive(orc_hier *H, int on, double omega)
+{
+  H->additive = on;
+  H->add_omega = omega;
 }
 
 orc_hier *orc_hier_create(int dim, int k, int n_coarse, int n_levels, const double *kappa_fine)
@@ -208,14 +216,20 @@ void orc_coarse_solve(orc_hier *H, double *dst, const double *src)
     }                                                                                     \
     const int n = H->n[l];                                                                \
     const long N = H->N[l];                                                               \
-    orc_smoother_step##SUF(dim, k, n, 1.0, H->SU[l], H->D[l], zero_init, 0, H->kappa[l]); \
+    if (H->additive)                                                                      \
+      orc_smoother_additive##SUF(dim, k, n, H->add_omega, H->SU[l], H->D[l], zero_init);  \
+    else                                                                                  \
+      orc_smoother_step##SUF(dim, k, n, 1.0, H->SU[l], H->D[l], zero_init, 0, H->kappa[l]); \
     orc_laplace_vmult##SUF(dim, k, n, H->T[l], H->SU[l], H->kappa[l]);                    \
     for (long i = 0; i < N; ++i) H->T[l][i] = H->D[l][i] - H->T[l][i];                    \
     memset(H->D[l - 1], 0, sizeof(REAL) * H->N[l - 1]);                                   \
     orc_restrict_add##SUF(dim, k, H->n[l - 1], H->D[l - 1], H->T[l]);                     \
     vcycle_rec##SUF(H, symmetric, l - 1, 1);                                              \
     orc_prolongate_add##SUF(dim, k, H->n[l - 1], H->SU[l], H->SU[l - 1]);                 \
-    orc_smoother_step##SUF(dim, k, n, 1.0, H->SU[l], H->D[l], 0, symmetric, H->kappa[l]); \
+    if (H->additive)                                                                      \
+      orc_smoother_additive##SUF(dim, k, n, H->add_omega, H->SU[l], H->D[l], 0);          \
+    else                                                                                  \
+      orc_smoother_step##SUF(dim, k, n, 1.0, H->SU[l], H->D[l], 0, symmetric, H->kappa[l]); \
   }
 
 DEFINE_VCYCLE(_d, double, dd, sud, td)
