@@ -15,7 +15,7 @@ TPS_OK = 0
 STATUS_NAMES = {
     0: "TPS_OK", 1: "TPS_ERR_INVALID", 2: "TPS_ERR_CUDA", 3: "TPS_ERR_ALLOC",
     4: "TPS_ERR_NOT_CONVERGED", 5: "TPS_ERR_BREAKDOWN", 6: "TPS_ERR_NONFINITE",
-    7: "TPS_ERR_UNSUPPORTED",
+    7: "TPS_ERR_UNSUPPORTED", 8: "TPS_ERR_TIMEOUT",
 }
 TPS_F64, TPS_F32, TPS_TF32 = 0, 1, 2
 VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32 = 0, 1, 2, 3
@@ -88,6 +88,9 @@ SIGNATURES = [
     ("tps_set_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tps_get_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_set_smoother_kind", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_double]),
+    ("tps_device_status", ctypes.c_int, [_VP]),
+    ("tps_selftest_wait_timeout", ctypes.c_int, [_VP, ctypes.c_longlong, _VP]),
+    ("tps_inject_alloc_failure", None, [ctypes.c_int]),
     ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("tps_batch_destroy", ctypes.c_int, [_VP]),
     ("tps_batch_last_error", ctypes.c_char_p, [_VP]),

@@ -161,6 +161,12 @@ class PoissonProblem:
                                         _stream()), self.handle)
         return e
 
+    def check_device(self) -> None:
+        """Synchronizes the device and raises TpsError(TPS_ERR_TIMEOUT) when a
+        bounded device wait of an earlier level call ran out (the flag is
+        cleared by the check).  The solvers check it themselves."""
+        L.check(L.lib().tps_device_status(self.handle), self.handle)
+
     def close(self):
         if getattr(self, "_h", None):
             L.lib().tps_destroy(self._h)

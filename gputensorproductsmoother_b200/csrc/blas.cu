@@ -3,6 +3,7 @@
 // vector accesses are left to the compiler for the aligned FP64 streams.
 #include "blas.cuh"
 #include "launch.cuh"
+#include "ptx.cuh"
 
 namespace tps {
 namespace {
@@ -532,6 +533,31 @@ cudaError_t launch_batch_check(BatchLoop b, int first, cudaGraphConditionalHandl
 cudaError_t launch_batch_select(const int *active, const BatchConds &cond, int n, cudaStream_t s)
 {
   TPS_LAUNCH((batch_select_kernel), 1, 256, 0, s, active, cond, n);
+  return cudaGetLastError();
+}
+
+namespace {
+
+// One thread waits, with the smoothers' bounded wait, on an mbarrier that
+// nothing arrives on (parity 0 of a fresh barrier: its first phase never
+// completes).  The wait gives up after `cycles` SM cycles and the timeout is
+// recorded in `err` the way the smoother kernels record a TMA stage that did
+// not arrive.
+__global__ void __launch_bounds__(32) wait_timeout_selftest_kernel(int *err, long long cycles)
+{
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    if (!mbar_wait_bounded(&bar, 0, cycles)) atomicExch(err, 1);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_wait_timeout_selftest(int *err, long long cycles, cudaStream_t s)
+{
+  TPS_LAUNCH((wait_timeout_selftest_kernel), 1, 32, 0, s, err, cycles);
   return cudaGetLastError();
 }
 

@@ -45,6 +45,9 @@ struct CGScalars {
 };
 
 // dst[i] = (Tout) src[i]; round32 != 0 rounds through FP32 first
+// one CTA whose bounded mbarrier wait runs out after `cycles` SM cycles and
+// sets *err (the timeout path of the smoother kernels, exercised without a fault)
+cudaError_t launch_wait_timeout_selftest(int *err, long long cycles, cudaStream_t s);
 cudaError_t launch_convert_f64_to_f32(float *dst, const double *src, int64_t n, cudaStream_t s);
 cudaError_t launch_convert_f32_to_f64(double *dst, const float *src, int64_t n, cudaStream_t s);
 cudaError_t launch_copy_f64(double *dst, const double *src, int64_t n, int round32, cudaStream_t s);

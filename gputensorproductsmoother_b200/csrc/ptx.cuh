@@ -79,13 +79,14 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
-// Bounded wait on an mbarrier phase by one thread: gives up after ~2^31 SM
-// cycles (about a second) and reports failure instead of spinning forever.
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+// Bounded wait on an mbarrier phase by one thread: gives up after `limit` SM
+// cycles (default 2^31, about a second) and reports failure instead of
+// spinning forever.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, long long limit = 1ll << 31)
 {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1ll << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }

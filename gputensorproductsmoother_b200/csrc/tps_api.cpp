@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -77,6 +78,17 @@ struct ApiError : std::runtime_error {
                      std::string(#call) + ": " + cudaGetErrorString(e_));                    \
   } while (0)
 
+// tps_inject_alloc_failure: the n-th device allocation from now fails; 0 = off
+std::atomic<int> g_alloc_fault{0};
+
+bool injected_alloc_fault()
+{
+  int n = g_alloc_fault.load();
+  while (n > 0)
+    if (g_alloc_fault.compare_exchange_weak(n, n - 1)) return n == 1;
+  return false;
+}
+
 struct DevBuf {
   void *p = nullptr;
   size_t bytes = 0;
@@ -94,6 +106,8 @@ struct DevBuf {
   {
     release();
     if (b == 0) return;
+    if (injected_alloc_fault())
+      throw ApiError(TPS_ERR_ALLOC, "cudaMalloc: out of memory (injected by tps_inject_alloc_failure)");
     cudaError_t e = cudaMalloc(&p, b);
     if (e != cudaSuccess) {
       p = nullptr;
@@ -392,47 +406,51 @@ void level_laplace(tps_handle *h, int level, int p, const VecLayout &lay, void *
     TPS_CUDA(h->kt->laplace[h->dim - 2][p](h->lv[level], lay, dst, src, rhs, mode, s));
 }
 
-// per-level coefficients from the finest-level kappa (coarse = mean of the 2^d children)
+// per-level coefficients from the finest-level kappa (coarse = mean of the 2^d
+// children).  Built aside and committed at the end: a rejected kappa or a failed
+// allocation leaves the handle's coefficients as they were.
 void set_kappa_levels(tps_handle *h, const double *kappa_fine)
 {
   const int L = h->n_levels - 1, dim = h->dim;
-  h->kappa_host.assign(h->n_levels, {});
   const int64_t ncf = dim == 3 ? int64_t(h->lv[L].n) * h->lv[L].n * h->lv[L].n
                                : int64_t(h->lv[L].n) * h->lv[L].n;
   for (int64_t c = 0; c < ncf; ++c)
     if (!(kappa_fine[c] > 0.0) || !std::isfinite(kappa_fine[c]))
       throw ApiError(TPS_ERR_INVALID, "kappa must be positive and finite");
-  h->kappa_host[L].assign(kappa_fine, kappa_fine + ncf);
+  std::vector<std::vector<double>> kh(h->n_levels);
+  kh[L].assign(kappa_fine, kappa_fine + ncf);
   for (int l = L - 1; l >= 0; --l) {
     const int n = h->lv[l].n, nf = h->lv[l + 1].n;
     const int64_t nc = dim == 3 ? int64_t(n) * n * n : int64_t(n) * n;
-    h->kappa_host[l].assign(nc, 0.0);
+    kh[l].assign(nc, 0.0);
     for (int64_t c = 0; c < nc; ++c) {
       const int cx = int(c % n), cy = int((c / n) % n), cz = dim == 3 ? int(c / (int64_t(n) * n)) : 0;
       double acc = 0.0;
       for (int q = 0; q < (1 << dim); ++q) {
         const int fx = 2 * cx + (q & 1), fy = 2 * cy + ((q >> 1) & 1), fz = 2 * cz + ((q >> 2) & 1);
-        acc += h->kappa_host[l + 1][fx + int64_t(fy) * nf + (dim == 3 ? int64_t(fz) * nf * nf : 0)];
+        acc += kh[l + 1][fx + int64_t(fy) * nf + (dim == 3 ? int64_t(fz) * nf * nf : 0)];
       }
-      h->kappa_host[l][c] = acc / (1 << dim);
+      kh[l][c] = acc / (1 << dim);
     }
   }
-  for (int p = 0; p < 2; ++p) {
-    h->kappa_dev[p].clear();
-    for (int l = 0; l < h->n_levels; ++l) {
-      h->kappa_dev[p].emplace_back(new DevBuf);
-      const size_t nc = h->kappa_host[l].size();
-      if (p == 0) {
-        h->kappa_dev[p][l]->alloc(sizeof(double) * nc);
-        TPS_CUDA(cudaMemcpy(h->kappa_dev[p][l]->p, h->kappa_host[l].data(), sizeof(double) * nc,
-                            cudaMemcpyHostToDevice));
-      } else {
-        std::vector<float> f(h->kappa_host[l].begin(), h->kappa_host[l].end());
-        h->kappa_dev[p][l]->alloc(sizeof(float) * nc);
-        TPS_CUDA(cudaMemcpy(h->kappa_dev[p][l]->p, f.data(), sizeof(float) * nc, cudaMemcpyHostToDevice));
+  // the device buffers are allocated once and then rewritten in place, so
+  // captured graphs (the CG iteration, a batch) keep valid pointers
+  if (h->kappa_dev[1].size() != static_cast<size_t>(h->n_levels)) {
+    std::vector<std::unique_ptr<DevBuf>> kd[2];
+    for (int p = 0; p < 2; ++p)
+      for (int l = 0; l < h->n_levels; ++l) {
+        kd[p].emplace_back(new DevBuf);
+        kd[p][l]->alloc((p == 0 ? sizeof(double) : sizeof(float)) * kh[l].size());
       }
-    }
+    for (int p = 0; p < 2; ++p) h->kappa_dev[p] = std::move(kd[p]);
   }
+  for (int l = 0; l < h->n_levels; ++l) {
+    const size_t nc = kh[l].size();
+    TPS_CUDA(cudaMemcpy(h->kappa_dev[0][l]->p, kh[l].data(), sizeof(double) * nc, cudaMemcpyHostToDevice));
+    const std::vector<float> f(kh[l].begin(), kh[l].end());
+    TPS_CUDA(cudaMemcpy(h->kappa_dev[1][l]->p, f.data(), sizeof(float) * nc, cudaMemcpyHostToDevice));
+  }
+  h->kappa_host = std::move(kh);
 }
 
 void coarse_solve(tps_handle *h, int p, cudaStream_t s, bool tc)
@@ -560,16 +578,42 @@ void fine_vmult64(tps_handle *h, double *dst, const double *src, cudaStream_t s)
   TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, 8, s));
 }
 
+// Reads and clears the handle's device error flag once the work queued on `s`
+// is done; true when a bounded device wait of an earlier launch ran out.
+bool take_timeout_flag(tps_handle *h, cudaStream_t s)
+{
+  if (!h->err_flag.p) return false;
+  int v = 0;
+  TPS_CUDA(cudaMemcpyAsync(&v, h->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TPS_CUDA(cudaStreamSynchronize(s));
+  if (v == 0) return false;
+  TPS_CUDA(cudaMemsetAsync(h->err_flag.p, 0, sizeof(int), s));
+  TPS_CUDA(cudaStreamSynchronize(s));
+  return true;
+}
+
+// message of a status that a call returns without throwing ("" for TPS_OK)
+const char *status_message(int status)
+{
+  switch (status) {
+    case TPS_ERR_NOT_CONVERGED: return "solver did not converge within max_iter";
+    case TPS_ERR_BREAKDOWN: return "Krylov breakdown (p^T A p <= 0)";
+    case TPS_ERR_NONFINITE: return "non-finite residual";
+    case TPS_ERR_TIMEOUT:
+      return "a bounded device wait ran out (a staged copy did not complete); results since the last check are invalid";
+    default: return "";
+  }
+}
+
 void ensure_krylov(tps_handle *h)
 {
   const int64_t N = h->fine().N;
-  if (!h->r.p) {
-    h->r.alloc(sizeof(double) * N);
-    h->p.alloc(sizeof(double) * N);
-    h->q.alloc(sizeof(double) * N);
-    h->partial.alloc(sizeof(double) * kRedBlocks * 4);
-    h->scalars.alloc(sizeof(CGScalars) + 64);
-  }
+  // each buffer on its own: one whose allocation failed is retried next time
+  if (!h->r.p) h->r.alloc(sizeof(double) * N);
+  if (!h->p.p) h->p.alloc(sizeof(double) * N);
+  if (!h->q.p) h->q.alloc(sizeof(double) * N);
+  if (!h->partial.p) h->partial.alloc(sizeof(double) * kRedBlocks * 4);
+  if (!h->scalars.p) h->scalars.alloc(sizeof(CGScalars) + 64);
   if (!h->ev0) {
     TPS_CUDA(cudaEventCreate(&h->ev0));
     TPS_CUDA(cudaEventCreate(&h->ev1));
@@ -809,18 +853,20 @@ void fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, c
   VcycleVectors &V = vcycle_vectors(h, p);
   ensure_krylov(h);
   if (h->fmg_sol.size() != static_cast<size_t>(h->n_levels)) {
-    h->fmg_sol.clear();
-    h->fmg_res.clear();
+    // built aside and kept only once every allocation succeeded
+    std::vector<std::unique_ptr<DevBuf>> sol, res;
     size_t tmp = 0;
     for (int l = 0; l <= L; ++l) {
-      h->fmg_sol.emplace_back(new DevBuf);
-      h->fmg_res.emplace_back(new DevBuf);
-      if (l < L) h->fmg_sol[l]->alloc(sizeof(double) * h->lv[l].N);
-      h->fmg_res[l]->alloc(sizeof(double) * h->lv[l].N);
+      sol.emplace_back(new DevBuf);
+      res.emplace_back(new DevBuf);
+      if (l < L) sol[l]->alloc(sizeof(double) * h->lv[l].N);
+      res[l]->alloc(sizeof(double) * h->lv[l].N);
       if (l > 0 && dim == 3)
         tmp = std::max(tmp, sizeof(double) * static_cast<size_t>(h->lv[l].N1) * h->lv[l - 1].N1 * h->lv[l - 1].N1);
     }
     if (tmp) h->fmg_tmp.alloc(tmp);
+    h->fmg_sol = std::move(sol);
+    h->fmg_res = std::move(res);
   }
   auto padmap = [&](int l) { return make_padmap(V.layout[l].N1, V.layout[l].sy); };
   const int zk = p == 1 ? 1 : 0;
@@ -884,8 +930,9 @@ int solve_gmres(tps_handle *h, const tps_solve_opts &o, const double *b, double 
   const int basis = 28;  // max_n_tmp_vectors - 2 with deal.II's default of 30
   const int nvec = std::min(basis, std::max(o.max_iter, 1)) + 1;
   while (static_cast<int>(h->gmres_v.size()) < nvec) {
-    h->gmres_v.emplace_back(new DevBuf);
-    h->gmres_v.back()->alloc(sizeof(double) * N);
+    std::unique_ptr<DevBuf> v(new DevBuf);
+    v->alloc(sizeof(double) * N);
+    h->gmres_v.push_back(std::move(v));
   }
   auto Vp = [&](int i) { return h->gmres_v[i]->as<double>(); };
   double *pv = h->p.as<double>();
@@ -1202,6 +1249,10 @@ int tps_fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs
     for (int l = 0; l < h->n_levels; ++l)
       if (!rhs[l] || (bnd && !bnd[l])) throw ApiError(TPS_ERR_INVALID, "a right-hand side (or Dirichlet vector) per level is required");
     fmg(h, precision, n_cycles, rhs, bnd, x, report, static_cast<cudaStream_t>(stream));
+    if (take_timeout_flag(h, static_cast<cudaStream_t>(stream))) {
+      report->converged = 0;
+      throw ApiError(TPS_ERR_TIMEOUT, status_message(TPS_ERR_TIMEOUT));
+    }
   });
 }
 
@@ -1229,11 +1280,13 @@ int tps_solve(tps_handle *h, const tps_solve_opts *opts, const double *b, double
       status = solve_gmres(h, *opts, b, x, report, s);
     else
       throw ApiError(TPS_ERR_INVALID, "unknown driver");
+    if (take_timeout_flag(h, s)) {
+      status = TPS_ERR_TIMEOUT;
+      report->converged = 0;
+    }
   });
   if (rc != TPS_OK) return rc;
-  if (status == TPS_ERR_NOT_CONVERGED) h->err = "solver did not converge within max_iter";
-  if (status == TPS_ERR_BREAKDOWN) h->err = "Krylov breakdown (p^T A p <= 0)";
-  if (status == TPS_ERR_NONFINITE) h->err = "non-finite residual";
+  h->err = status_message(status);
   return status;
 }
 
@@ -1258,7 +1311,7 @@ int tps_set_kappa(tps_handle *h, const double *kappa, int rebuild_coarse)
         }
       }
     }
-    if (h->graph) {  // the captured iteration reads the kappa buffers it was built with
+    if (h->graph) {  // re-captured on the next solve
       cudaGraphExecDestroy(h->graph);
       h->graph = nullptr;
     }
@@ -1379,6 +1432,7 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
     float ms = 0.f;
     TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
     *ms_per_sweep = ms / sweeps;
+    if (take_timeout_flag(h, s)) throw ApiError(TPS_ERR_TIMEOUT, status_message(TPS_ERR_TIMEOUT));
   });
 }
 
@@ -1401,10 +1455,8 @@ int tps_solve_host_guess(tps_handle *h, const tps_solve_opts *opts, const double
     const int64_t N = h->fine().N;
     if (!h->own_stream) TPS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
     cudaStream_t s = h->own_stream;
-    if (!h->host_b.p) {
-      h->host_b.alloc(sizeof(double) * N);
-      h->host_x.alloc(sizeof(double) * N);
-    }
+    if (!h->host_b.p) h->host_b.alloc(sizeof(double) * N);
+    if (!h->host_x.p) h->host_x.alloc(sizeof(double) * N);
     TPS_CUDA(cudaMemcpyAsync(h->host_b.p, b_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
     if (x0_host)
       TPS_CUDA(cudaMemcpyAsync(h->host_x.p, x0_host, sizeof(double) * N, cudaMemcpyHostToDevice, s));
@@ -1416,8 +1468,34 @@ int tps_solve_host_guess(tps_handle *h, const tps_solve_opts *opts, const double
       TPS_CUDA(cudaStreamSynchronize(s));
     }
   });
-  return rc != TPS_OK ? rc : status;
+  if (rc != TPS_OK) return rc;
+  h->err = status_message(status);  // the message of the inner tps_solve
+  return status;
 }
+
+int tps_device_status(tps_handle *h)
+{
+  bool timed_out = false;
+  const int rc = guarded(h, [&] {
+    TPS_CUDA(cudaDeviceSynchronize());
+    timed_out = take_timeout_flag(h, nullptr);
+  });
+  if (rc != TPS_OK) return rc;
+  if (!timed_out) return TPS_OK;
+  h->err = status_message(TPS_ERR_TIMEOUT);
+  return TPS_ERR_TIMEOUT;
+}
+
+int tps_selftest_wait_timeout(tps_handle *h, long long cycles, void *stream)
+{
+  return guarded(h, [&] {
+    if (cycles < 1 || cycles > (1ll << 31)) throw ApiError(TPS_ERR_INVALID, "cycles must be in 1..2^31");
+    if (!h->err_flag.p) h->err_flag.alloc(sizeof(int));
+    TPS_CUDA(launch_wait_timeout_selftest(h->err_flag.as<int>(), cycles, static_cast<cudaStream_t>(stream)));
+  });
+}
+
+void tps_inject_alloc_failure(int n) { g_alloc_fault.store(n > 0 ? n : 0); }
 
 }  // extern "C"
 
@@ -1619,7 +1697,7 @@ int batch_guarded(tps_batch *B, F &&f)
     cudaError_t e = cudaSetDevice(B->device);
     if (e != cudaSuccess) throw ApiError(TPS_ERR_CUDA, cudaGetErrorString(e));
     int st = f();
-    B->err.clear();
+    B->err = status_message(st);
     return st;
   } catch (const ApiError &e) {
     B->err = e.what();
@@ -1764,6 +1842,11 @@ int tps_batch_solve(tps_batch *B, const tps_solve_opts *opts, const double *cons
       else if (!r.converged) si = TPS_ERR_NOT_CONVERGED;
       if (si != TPS_OK && (status == TPS_OK || status == TPS_ERR_NOT_CONVERGED)) status = si;
     }
+    for (int i = 0; i < n; ++i)
+      if (take_timeout_flag(B->sys[i], s)) {
+        reports[i].converged = 0;
+        status = TPS_ERR_TIMEOUT;
+      }
     (void)act;
     return status;
   });

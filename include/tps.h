@@ -28,7 +28,8 @@ typedef enum {
   TPS_ERR_NOT_CONVERGED = 4,/* solver hit max_iter before the tolerance */
   TPS_ERR_BREAKDOWN = 5,    /* Krylov breakdown (p^T A p <= 0, zero norm) */
   TPS_ERR_NONFINITE = 6,    /* NaN/Inf met in a residual or input */
-  TPS_ERR_UNSUPPORTED = 7   /* degree/dimension not compiled in */
+  TPS_ERR_UNSUPPORTED = 7,  /* degree/dimension not compiled in */
+  TPS_ERR_TIMEOUT = 8       /* a bounded device wait ran out (tps_device_status) */
 } tps_status;
 
 typedef enum {
@@ -274,6 +275,26 @@ int tps_batch_solve(tps_batch *b, const tps_solve_opts *opts, const double *cons
  * stream capture.  Calls share the array: calls that overlap on the GPU race. */
 int tps_restrict_add_noalloc(int dim, int degree, int n_coarse_cells, int dtype, void *coarse,
                              const void *fine, void *stream);
+
+/* Failure detection (no counterpart in the reference).  Every device wait of
+ * the library is bounded: the 3D smoothers wait for their TMA stages for at
+ * most ~2^31 SM cycles, then record the timeout in a flag of the handle and
+ * return instead of spinning.  tps_solve, tps_solve_host(_guess), tps_fmg,
+ * tps_time_smoother and tps_batch_solve read the flag once their stream's work
+ * is done, clear it and return TPS_ERR_TIMEOUT when it was set (the results of
+ * the call are then invalid).  The asynchronous level calls leave it set:
+ * tps_device_status synchronizes the device, reads and clears it and returns
+ * TPS_ERR_TIMEOUT or TPS_OK. */
+int tps_device_status(tps_handle *h);
+/* Runs the error path of a bounded wait without any fault: one CTA waits, with
+ * the smoothers' wait loop, on an mbarrier that nothing arrives on, gives up
+ * after `cycles` SM cycles (1 .. 2^31) and records the timeout in the handle's
+ * flag like a smoother launch would.  Asynchronous on `stream`. */
+int tps_selftest_wait_timeout(tps_handle *h, long long cycles, void *stream);
+/* Testing hook: the n-th device allocation of the library from now (n >= 1,
+ * counted over all handles and batches of the process) fails as cudaMalloc does
+ * on a full device, so the calls report TPS_ERR_ALLOC; n = 0 disarms it. */
+void tps_inject_alloc_failure(int n);
 
 #ifdef __cplusplus
 }

@@ -63,6 +63,18 @@ def test_null_arguments_are_rejected():
     assert lib.tps_laplace_vmult(None, 0, 0, None, None, None) == 1
     assert lib.tps_smoother_step(None, 0, 0, None, None, 0, 0, None) == 1
     assert lib.tps_level_info(None, 0, None, None) == 1
+    assert lib.tps_device_status(None) == 1
+    assert lib.tps_selftest_wait_timeout(None, 1000, None) == 1
+
+
+def test_alloc_failure_hook_arms_and_disarms():
+    """The allocation-failure hook is host state only: arming and disarming
+    it needs no device, and a negative count disarms it."""
+    lib = L.lib()
+    lib.tps_inject_alloc_failure(3)
+    lib.tps_inject_alloc_failure(-1)
+    lib.tps_inject_alloc_failure(0)
+    assert L.STATUS_NAMES[8] == "TPS_ERR_TIMEOUT"
 
 
 def test_create_without_device_fails_loudly():
