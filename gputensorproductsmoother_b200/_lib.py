@@ -74,6 +74,8 @@ SIGNATURES = [
                                       ctypes.POINTER(TpsReport)]),
     ("tps_solve_host_guess", ctypes.c_int, [_VP, ctypes.POINTER(TpsSolveOpts), _VP, _VP, _VP,
                                             ctypes.POINTER(TpsReport)]),
+    ("tps_solve_host_many", ctypes.c_int, [_VP, ctypes.POINTER(TpsSolveOpts), ctypes.c_int,
+                                           ctypes.POINTER(_VP), ctypes.POINTER(_VP), ctypes.POINTER(TpsReport)]),
     ("tps_time_smoother", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                          ctypes.POINTER(ctypes.c_double), _VP]),
     ("tps_set_kappa", ctypes.c_int, [_VP, _VP, ctypes.c_int]),

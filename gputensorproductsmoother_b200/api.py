@@ -393,6 +393,33 @@ class MultigridSolvers:
         return self._solve(L.DRIVER_CG, b, x, precision, symmetric, max_iter, rel_tol, 1e-300,
                            use_graph, raise_on_fail)
 
+    def solve_host_many(self, bs, xs=None, precision: str = "fp32", symmetric: bool = True,
+                        max_iter: int = 100, rel_tol: float = 1e-10, raise_on_fail: bool = True):
+        """CG solves (each from x = 0) of a sequence of HOST right-hand sides
+        (contiguous CPU float64 tensors), the copies of one solve overlapped
+        with its neighbours' solves (tps_solve_host_many); pinned tensors are
+        needed for the overlap.  xs: output tensors (allocated pinned when
+        None).  Returns (xs, list of SolveReport)."""
+        p = self.problem
+        n, N = len(bs), p.n_dofs()
+        if n < 1:
+            raise ValueError("at least one right-hand side is required")
+        if xs is None:
+            xs = [torch.empty(N, dtype=torch.float64).pin_memory() for _ in range(n)]
+        if len(xs) != n:
+            raise ValueError(f"{n} output tensors are required")
+        for v in list(bs) + list(xs):
+            if v.is_cuda or v.dtype != torch.float64 or not v.is_contiguous() or v.numel() != N:
+                raise ValueError(f"host vectors must be contiguous CPU float64 tensors of {N} entries")
+        o = L.TpsSolveOpts(L.DRIVER_CG, _PRECISIONS[precision], int(symmetric), max_iter, rel_tol, 1e-300, 1)
+        reps = (L.TpsReport * n)()
+        bp = (ctypes.c_void_p * n)(*[b.data_ptr() for b in bs])
+        xp = (ctypes.c_void_p * n)(*[x.data_ptr() for x in xs])
+        st = L.lib().tps_solve_host_many(p.handle, ctypes.byref(o), n, bp, xp, reps)
+        if st != L.TPS_OK and (raise_on_fail or st != 4):
+            L.check(st, p.handle)
+        return xs, [_report(reps[i]) for i in range(n)]
+
     def solve_gmres(self, b: torch.Tensor, x: torch.Tensor | None = None,
                     precision: str = "fp64_rounded", max_iter: int = 20, reduce: float = 1e-9,
                     abs_tol: float = 1e-16, raise_on_fail: bool = False):

@@ -555,6 +555,24 @@ __global__ void __launch_bounds__(32) wait_timeout_selftest_kernel(int *err, lon
 
 }  // namespace
 
+namespace {
+
+// n 32-bit words src -> dst (dst may be host-mapped memory)
+__global__ void __launch_bounds__(32) copy_words_kernel(const uint32_t *src, uint32_t *dst, int n)
+{
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
+  for (int i = threadIdx.x; i < n; i += 32) dst[i] = src[i];
+}
+
+}  // namespace
+
+cudaError_t launch_copy_words(const void *src, void *dst, int n_words, cudaStream_t s)
+{
+  TPS_LAUNCH((copy_words_kernel), 1, 32, 0, s, static_cast<const uint32_t *>(src), static_cast<uint32_t *>(dst),
+             n_words);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_wait_timeout_selftest(int *err, long long cycles, cudaStream_t s)
 {
   TPS_LAUNCH((wait_timeout_selftest_kernel), 1, 32, 0, s, err, cycles);

@@ -45,6 +45,10 @@ struct CGScalars {
 };
 
 // dst[i] = (Tout) src[i]; round32 != 0 rounds through FP32 first
+// n 32-bit words src -> dst by one small kernel; dst may be host-mapped
+// memory, so a small result reaches the host without a copy-engine transfer
+// (which would queue behind large copies on other streams)
+cudaError_t launch_copy_words(const void *src, void *dst, int n_words, cudaStream_t s);
 // one CTA whose bounded mbarrier wait runs out after `cycles` SM cycles and
 // sets *err (the timeout path of the smoother kernels, exercised without a fault)
 cudaError_t launch_wait_timeout_selftest(int *err, long long cycles, cudaStream_t s);

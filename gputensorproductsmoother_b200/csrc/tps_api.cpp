@@ -120,6 +120,29 @@ struct DevBuf {
   T *as() const { return static_cast<T *>(p); }
 };
 
+// A small host-mapped pinned buffer: kernels write scalars there, the host
+// reads them after synchronizing the stream.
+struct Mailbox {
+  void *host = nullptr;
+  Mailbox() = default;
+  Mailbox(const Mailbox &) = delete;
+  Mailbox &operator=(const Mailbox &) = delete;
+  ~Mailbox()
+  {
+    if (host) cudaFreeHost(host);
+  }
+  static constexpr size_t kBytes = 256;
+  void ensure()
+  {
+    if (host) return;
+    cudaError_t e = cudaHostAlloc(&host, kBytes, cudaHostAllocMapped);
+    if (e != cudaSuccess) {
+      host = nullptr;
+      throw ApiError(TPS_ERR_ALLOC, std::string("cudaHostAlloc: ") + cudaGetErrorString(e));
+    }
+  }
+};
+
 // V-cycle work vectors of one precision.  In 3D their rows are padded to a
 // 16-byte pitch so the smoother can stage patch boxes with TMA.
 struct VcycleVectors {
@@ -148,6 +171,7 @@ struct tps_handle {
   VcycleVectors vc[2];  // [0] FP64, [1] FP32
   std::vector<int> sm_variant[2];  // per level: 3D smoother patches-per-batch variant (autotuned)
   DevBuf err_flag;      // set by a kernel whose bounded wait gave up
+  Mailbox mbox;         // small device results (CG scalars, dots, the error flag) for the host
   // variable coefficient: per-level per-cell kappa (fine given, coarse = mean of children)
   bool has_kappa = false;
   std::vector<std::vector<double>> kappa_host;
@@ -162,6 +186,10 @@ struct tps_handle {
   const double *graph_x = nullptr;  // the captured graph updates this solution vector
   cudaStream_t own_stream = nullptr;  // used by tps_solve_host
   DevBuf host_b, host_x;              // device staging of tps_solve_host (kept, so its graph stays valid)
+  // tps_solve_host_many: copy stream, double-buffered inputs and outputs, events
+  cudaStream_t copy_stream = nullptr;
+  DevBuf pipe_b[2], pipe_x[2];
+  cudaEvent_t pipe_in[2] = {nullptr, nullptr}, pipe_done[2] = {nullptr, nullptr}, pipe_out[2] = {nullptr, nullptr};
   std::vector<std::unique_ptr<DevBuf>> fmg_sol, fmg_res;  // FMG: FP64 per level (lexicographic)
   DevBuf fmg_tmp;                                        // FMG: FP64 transfer scratch
   DevBuf var_r[2];      // separate-kernel smoother variants: residual of the finest-level size
@@ -177,6 +205,12 @@ struct tps_handle {
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (own_stream) cudaStreamDestroy(own_stream);
+    if (copy_stream) cudaStreamDestroy(copy_stream);
+    for (int i = 0; i < 2; ++i) {
+      if (pipe_in[i]) cudaEventDestroy(pipe_in[i]);
+      if (pipe_done[i]) cudaEventDestroy(pipe_done[i]);
+      if (pipe_out[i]) cudaEventDestroy(pipe_out[i]);
+    }
   }
   const LevelGeomH &fine() const { return lv.back(); }
 };
@@ -578,14 +612,26 @@ void fine_vmult64(tps_handle *h, double *dst, const double *src, cudaStream_t s)
   TPS_CUDA(launch_copy_boundary(dst, src, h->dim, g.N1, 8, s));
 }
 
+// `bytes` (a multiple of 4, at most 256) of device memory at src, read on
+// stream s after the work queued there: a one-warp kernel stores them into the
+// handle's host-mapped mailbox, then the stream is synchronized
+void read_small(tps_handle *h, void *out, const void *src, size_t bytes, cudaStream_t s)
+{
+  h->mbox.ensure();
+  void *dst = nullptr;
+  TPS_CUDA(cudaHostGetDevicePointer(&dst, h->mbox.host, 0));
+  TPS_CUDA(launch_copy_words(src, dst, static_cast<int>(bytes / 4), s));
+  TPS_CUDA(cudaStreamSynchronize(s));
+  std::memcpy(out, h->mbox.host, bytes);
+}
+
 // Reads and clears the handle's device error flag once the work queued on `s`
 // is done; true when a bounded device wait of an earlier launch ran out.
 bool take_timeout_flag(tps_handle *h, cudaStream_t s)
 {
   if (!h->err_flag.p) return false;
   int v = 0;
-  TPS_CUDA(cudaMemcpyAsync(&v, h->err_flag.p, sizeof(int), cudaMemcpyDeviceToHost, s));
-  TPS_CUDA(cudaStreamSynchronize(s));
+  read_small(h, &v, h->err_flag.p, sizeof(int), s);
   if (v == 0) return false;
   TPS_CUDA(cudaMemsetAsync(h->err_flag.p, 0, sizeof(int), s));
   TPS_CUDA(cudaStreamSynchronize(s));
@@ -643,10 +689,11 @@ void cg_iteration_body(tps_handle *h, int prec, bool symmetric, double *x, cudaS
   TPS_CUDA(launch_cg_finalize_rr(part, sc, s));
 }
 
+static_assert(sizeof(CGScalars) % 4 == 0 && sizeof(CGScalars) <= Mailbox::kBytes, "CG scalars fit the mailbox");
+
 void read_scalars(tps_handle *h, CGScalars &out, cudaStream_t s)
 {
-  TPS_CUDA(cudaMemcpyAsync(&out, h->scalars.p, sizeof(CGScalars), cudaMemcpyDeviceToHost, s));
-  TPS_CUDA(cudaStreamSynchronize(s));
+  read_small(h, &out, h->scalars.p, sizeof(CGScalars), s);
 }
 
 int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x, tps_report *rep,
@@ -766,8 +813,7 @@ double dev_dot(tps_handle *h, const double *a, const double *b, cudaStream_t s)
   TPS_CUDA(launch_dot_f64(a, b, h->fine().N, part, s));
   TPS_CUDA(launch_reduce(part, 1, part + 2 * kRedBlocks, s));
   double v = 0;
-  TPS_CUDA(cudaMemcpyAsync(&v, part + 2 * kRedBlocks, sizeof(double), cudaMemcpyDeviceToHost, s));
-  TPS_CUDA(cudaStreamSynchronize(s));
+  read_small(h, &v, part + 2 * kRedBlocks, sizeof(double), s);
   return v;
 }
 
@@ -1470,6 +1516,80 @@ int tps_solve_host_guess(tps_handle *h, const tps_solve_opts *opts, const double
   });
   if (rc != TPS_OK) return rc;
   h->err = status_message(status);  // the message of the inner tps_solve
+  return status;
+}
+
+int tps_solve_host_many(tps_handle *h, const tps_solve_opts *opts, int n, const double *const *b_host,
+                        double *const *x_host, tps_report *reports)
+{
+  if (!h) return TPS_ERR_INVALID;
+  if (!opts || n < 1 || !b_host || !x_host || !reports) {
+    h->err = "null argument or n < 1";
+    return TPS_ERR_INVALID;
+  }
+  for (int i = 0; i < n; ++i)
+    if (!b_host[i] || !x_host[i]) {
+      h->err = "null host buffer";
+      return TPS_ERR_INVALID;
+    }
+  int status = TPS_OK;
+  const int rc = guarded(h, [&] {
+    const int64_t N = h->fine().N;
+    const size_t bytes = sizeof(double) * N;
+    if (!h->own_stream) TPS_CUDA(cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking));
+    if (!h->copy_stream) TPS_CUDA(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      if (!h->pipe_b[i].p) h->pipe_b[i].alloc(bytes);
+      if (!h->pipe_x[i].p) h->pipe_x[i].alloc(bytes);
+      if (!h->pipe_in[i]) TPS_CUDA(cudaEventCreateWithFlags(&h->pipe_in[i], cudaEventDisableTiming));
+      if (!h->pipe_done[i]) TPS_CUDA(cudaEventCreateWithFlags(&h->pipe_done[i], cudaEventDisableTiming));
+      if (!h->pipe_out[i]) TPS_CUDA(cudaEventCreateWithFlags(&h->pipe_out[i], cudaEventDisableTiming));
+    }
+    if (!h->host_x.p) h->host_x.alloc(bytes);
+    cudaStream_t s = h->own_stream, cs = h->copy_stream;
+    // the copies stay ordered on the copy stream: H2D of b[i+1] is queued while
+    // solve i runs, then D2H of x[i] once solve i is done, so both overlap solve
+    // i+1.  Every solve starts from zero in host_x (a fixed vector, so the
+    // captured CG iteration is reused) and is copied out to pipe_x.
+    try {
+      TPS_CUDA(cudaMemcpyAsync(h->pipe_b[0].p, b_host[0], bytes, cudaMemcpyHostToDevice, cs));
+      TPS_CUDA(cudaEventRecord(h->pipe_in[0], cs));
+      for (int i = 0; i < n; ++i) {
+        const int sl = i & 1;
+        if (i + 1 < n) {  // pipe_b[sl ^ 1] was last read by solve i-1, which has returned
+          TPS_CUDA(cudaMemcpyAsync(h->pipe_b[sl ^ 1].p, b_host[i + 1], bytes, cudaMemcpyHostToDevice, cs));
+          TPS_CUDA(cudaEventRecord(h->pipe_in[sl ^ 1], cs));
+        }
+        TPS_CUDA(cudaStreamWaitEvent(s, h->pipe_in[sl], 0));
+        TPS_CUDA(cudaMemsetAsync(h->host_x.p, 0, bytes, s));
+        const int si = tps_solve(h, opts, h->pipe_b[sl].as<double>(), h->host_x.as<double>(), &reports[i], s);
+        if (si != TPS_OK && si != TPS_ERR_NOT_CONVERGED && si != TPS_ERR_BREAKDOWN && si != TPS_ERR_NONFINITE &&
+            si != TPS_ERR_TIMEOUT)
+          throw ApiError(si, h->err);
+        if (si != TPS_OK && (status == TPS_OK || status == TPS_ERR_NOT_CONVERGED)) status = si;
+        if (si == TPS_OK || si == TPS_ERR_NOT_CONVERGED) {
+          // pipe_x[sl] still holds x[i-2] until its D2H has completed
+          if (i >= 2) TPS_CUDA(cudaStreamWaitEvent(s, h->pipe_out[sl], 0));
+          TPS_CUDA(cudaMemcpyAsync(h->pipe_x[sl].p, h->host_x.p, bytes, cudaMemcpyDeviceToDevice, s));
+          TPS_CUDA(cudaEventRecord(h->pipe_done[sl], s));
+          TPS_CUDA(cudaStreamWaitEvent(cs, h->pipe_done[sl], 0));
+          TPS_CUDA(cudaMemcpyAsync(x_host[i], h->pipe_x[sl].p, bytes, cudaMemcpyDeviceToHost, cs));
+          TPS_CUDA(cudaEventRecord(h->pipe_out[sl], cs));
+        } else {
+          // no result to copy: later solves must not wait on a stale event
+          TPS_CUDA(cudaEventRecord(h->pipe_out[sl], cs));
+        }
+      }
+      TPS_CUDA(cudaStreamSynchronize(cs));
+    } catch (...) {
+      // no copy may still be writing into the caller's buffers after the return
+      cudaStreamSynchronize(cs);
+      cudaStreamSynchronize(s);
+      throw;
+    }
+  });
+  if (rc != TPS_OK) return rc;
+  h->err = status_message(status);
   return status;
 }
 

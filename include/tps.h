@@ -220,6 +220,19 @@ int tps_solve_host(tps_handle *h, const tps_solve_opts *opts, const double *b_ho
  * to x_host.  tps_solve_host(h, o, b, x, r) is this call with x0_host = x. */
 int tps_solve_host_guess(tps_handle *h, const tps_solve_opts *opts, const double *b_host,
                          const double *x0_host, double *x_host, tps_report *report);
+/* n solves of the same system with HOST right-hand sides b_host[i] and
+ * solutions x_host[i] (N entries each, every solve from x = 0), one after the
+ * other, with the copies overlapped with the solves: b[i+1] is copied in and
+ * x[i-1] out while solve i runs, on a second stream.  Overlap needs pinned
+ * host buffers (cudaHostAlloc / cudaHostRegister); pageable ones give the same
+ * results without it.  reports[i] per solve; x_host[i] is written when solve i
+ * returns TPS_OK or TPS_ERR_NOT_CONVERGED.  The return value is TPS_OK when
+ * every solve converged, else the first failure (a non-convergence only when
+ * nothing worse happened).  The handle keeps 5 more device vectors (40 N bytes)
+ * between calls.  No counterpart in the reference (a host loop over
+ * tps_solve_host_guess, without the overlap). */
+int tps_solve_host_many(tps_handle *h, const tps_solve_opts *opts, int n, const double *const *b_host,
+                        double *const *x_host, tps_report *reports);
 
 /* Patches-per-batch autotuner of the 3D smoother (the reference's
  * AdditionalData::patch_per_block, include/patch_smoother.cuh:101-118, chosen

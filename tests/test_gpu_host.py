@@ -56,3 +56,61 @@ def test_host_solves_match_device_solve(cuda, precision):
         L.check(L.lib().tps_solve_host_guess(P.handle, ctypes.byref(o), None, None, xo.data_ptr(),
                                              ctypes.byref(r)), P.handle)
     P.close()
+
+
+def test_host_solve_sequence_matches_single_solves(cuda):
+    """tps_solve_host_many: the overlapped sequence gives, for every right-hand
+    side, exactly the solve of tps_solve_host_guess from zero; pinned and
+    pageable buffers give the same results."""
+    k, n = 3, 8
+    P = tps.PoissonProblem(3, k, n)
+    N1 = n * k + 1
+    bs = [interior_random(N1, 20 + i) for i in range(5)]
+    o = L.TpsSolveOpts(L.DRIVER_CG, L.VCYCLE_F32, 1, 100, 1e-10, 1e-300, 1)
+    singles = []
+    for b in bs:
+        xh = torch.zeros_like(b)
+        r = L.TpsReport()
+        L.check(L.lib().tps_solve_host_guess(P.handle, ctypes.byref(o), b.data_ptr(), None, xh.data_ptr(),
+                                             ctypes.byref(r)), P.handle)
+        singles.append((xh, r.iterations))
+    MG = tps.MultigridSolvers(P)
+    for pinned in (True, False):
+        bb = [b.clone().pin_memory() if pinned else b.clone() for b in bs]
+        xs = [torch.full_like(b, 5.0) for b in bs]
+        if pinned:
+            xs = [x.pin_memory() for x in xs]
+        xs, reps = MG.solve_host_many(bb, xs, precision="fp32", rel_tol=1e-10)
+        for (x1, it1), x, r in zip(singles, xs, reps):
+            assert r.converged and r.iterations == it1
+            assert torch.equal(x, x1)
+    # one right-hand side, default (pinned) outputs
+    xs, reps = MG.solve_host_many(bs[:1])
+    assert torch.equal(xs[0], singles[0][0])
+    P.close()
+
+
+def test_host_solve_sequence_reports_failures(cuda):
+    k, n = 3, 8
+    P = tps.PoissonProblem(3, k, n)
+    N1 = n * k + 1
+    bs = [interior_random(N1, 30 + i).pin_memory() for i in range(3)]
+    bs[1][N1 * N1 * 12 + N1 * 12 + 12] = float("nan")
+    xs = [torch.full_like(b, 5.0).pin_memory() for b in bs]
+    o = L.TpsSolveOpts(L.DRIVER_CG, L.VCYCLE_F32, 1, 100, 1e-10, 1e-300, 1)
+    reps = (L.TpsReport * 3)()
+    bp = (ctypes.c_void_p * 3)(*[b.data_ptr() for b in bs])
+    xp = (ctypes.c_void_p * 3)(*[x.data_ptr() for x in xs])
+    st = L.lib().tps_solve_host_many(P.handle, ctypes.byref(o), 3, bp, xp, reps)
+    assert st == 6  # TPS_ERR_NONFINITE
+    assert reps[0].converged and reps[2].converged and not reps[1].converged
+    assert torch.all(xs[1] == 5.0)  # no result copied for the failed solve
+    MG = tps.MultigridSolvers(P)
+    x0, _ = MG.solve_cg(bs[0].cuda(), precision="fp32", rel_tol=1e-10)
+    x2, _ = MG.solve_cg(bs[2].cuda(), precision="fp32", rel_tol=1e-10)
+    assert torch.equal(xs[0], x0.cpu()) and torch.equal(xs[2], x2.cpu())
+    # argument errors
+    assert L.lib().tps_solve_host_many(P.handle, ctypes.byref(o), 0, bp, xp, reps) == 1
+    bp[1] = None
+    assert L.lib().tps_solve_host_many(P.handle, ctypes.byref(o), 3, bp, xp, reps) == 1
+    P.close()
