@@ -13,6 +13,8 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <cstring>
 #include <stdexcept>
 
 namespace tps {
@@ -308,6 +310,93 @@ std::vector<double> dense_patch_inverse(const DegreeData &D, int dim)
     }
   }
   return spd_inverse(A, n);
+}
+
+namespace {
+// round to the nearest TF32 value, ties away from zero (as cvt.rna.tf32.f32)
+float round_tf32(double v)
+{
+  float f = static_cast<float>(v);
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  u = (u + 0x1000u) & 0xFFFFE000u;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+}  // namespace
+
+std::vector<float> patch_gemm_image(const DegreeData &D, int nbe, int nbo, int ck)
+{
+  const int k = D.k, n1 = 2 * k + 1, m = 2 * k - 1;
+  const int nb = n1 * n1 * n1, ni = m * m * m, pl = n1 * n1, ipl = m * m;
+  const std::vector<double> inv = dense_patch_inverse(D, 3);  // ni x ni
+  auto idx_box = [&](int z, int y, int x) { return x + n1 * (y + n1 * z); };
+  // G (ni x nb): interior columns A_II^{-1}, ring columns -A_II^{-1} A_IB
+  std::vector<double> G(static_cast<size_t>(ni) * nb, 0.0);
+  std::vector<double> aib(static_cast<size_t>(ni) * nb, 0.0);  // A(i, q) for ring q
+  const double *Mm = D.pmass.data(), *Ll = D.plap.data();
+  for (int i = 0; i < ni; ++i) {
+    const int ix = 1 + i % m, iy = 1 + (i / m) % m, iz = 1 + i / (m * m);
+    for (int q = 0; q < nb; ++q) {
+      const int qx = q % n1, qy = (q / n1) % n1, qz = q / pl;
+      const bool ring = qx == 0 || qx == n1 - 1 || qy == 0 || qy == n1 - 1 || qz == 0 || qz == n1 - 1;
+      if (!ring) continue;
+      aib[static_cast<size_t>(i) * nb + q] =
+          Ll[ix * n1 + qx] * Mm[iy * n1 + qy] * Mm[iz * n1 + qz] + Mm[ix * n1 + qx] * Ll[iy * n1 + qy] * Mm[iz * n1 + qz] +
+          Mm[ix * n1 + qx] * Mm[iy * n1 + qy] * Ll[iz * n1 + qz];
+    }
+  }
+  for (int i = 0; i < ni; ++i) {
+    double *g = &G[static_cast<size_t>(i) * nb];
+    for (int j = 0; j < ni; ++j) {
+      const double w = inv[static_cast<size_t>(i) * ni + j];
+      const int jx = 1 + j % m, jy = 1 + (j / m) % m, jz = 1 + j / (m * m);
+      g[idx_box(jz, jy, jx)] += w;
+      const double *a = &aib[static_cast<size_t>(j) * nb];
+      for (int q = 0; q < nb; ++q) g[q] -= w * a[q];
+    }
+  }
+  // z-parity blocks
+  auto grow = [&](int zi, int r) { return &G[static_cast<size_t>(zi * ipl + r) * nb]; };
+  const int ne = k * ipl, no = (k - 1) * ipl, ke = (k + 1) * pl, ko = k * pl;
+  auto coef = [&](bool odd_out, bool odd_in, int zp, int r, int p, int s) {
+    // output side: E = (y(zp) + y(m-1-zp)) / 2 (zp < k-1), y(k-1) for the centre;
+    // O = (y(zp) - y(m-1-zp)) / 2.  Input side: e_p <- (G(p) + G(n1-1-p)) / 2
+    // (p < k), G(k) for the centre; o_p <- (G(p) - G(n1-1-p)) / 2.
+    auto in = [&](const double *row) {
+      if (p == k) return row[p * pl + s];
+      const double a = row[p * pl + s], b = row[(n1 - 1 - p) * pl + s];
+      return odd_in ? 0.5 * (a - b) : 0.5 * (a + b);
+    };
+    if (zp == k - 1) return in(grow(zp, r));
+    const double a = in(grow(zp, r)), b = in(grow(m - 1 - zp, r));
+    return odd_out ? 0.5 * (a - b) : 0.5 * (a + b);
+  };
+  const int ce = (ke + ck - 1) / ck, co = (ko + ck - 1) / ck;
+  const size_t chunk_e = static_cast<size_t>(nbe) * ck, chunk_o = static_cast<size_t>(nbo) * ck;
+  std::vector<float> img(ce * chunk_e + co * chunk_o, 0.f);
+  auto put = [&](float *base, int n, int kk, float v) {
+    // K-major, no swizzle: 8-row groups of ck/4 core matrices (8 rows x 16 bytes)
+    base[((n >> 3) * (ck / 4) * 128 + (n & 7) * 16 + (kk >> 2) * 128 + (kk & 3) * 4) / 4] = v;
+  };
+  for (int c = 0; c < ce; ++c)
+    for (int n = 0; n < ne; ++n)
+      for (int kk = 0; kk < ck; ++kk) {
+        const int col = c * ck + kk;
+        if (col >= ke) continue;
+        const int zp = n / ipl, r = n % ipl, p = col / pl, s = col % pl;
+        put(&img[c * chunk_e], n, kk, round_tf32(coef(false, false, zp, r, p, s)));
+      }
+  float *go = img.data() + ce * chunk_e;
+  for (int c = 0; c < co; ++c)
+    for (int n = 0; n < no; ++n)
+      for (int kk = 0; kk < ck; ++kk) {
+        const int col = c * ck + kk;
+        if (col >= ko) continue;
+        const int zp = n / ipl, r = n % ipl, p = col / pl, s = col % pl;
+        put(go + c * chunk_o, n, kk, round_tf32(coef(true, true, zp, r, p, s)));
+      }
+  return img;
 }
 
 std::vector<double> spd_inverse(std::vector<double> &A, int n)

@@ -39,6 +39,20 @@ DegreeData make_degree_data(int k);
 // the full symmetric inverse, row-major.
 std::vector<double> dense_patch_inverse(const DegreeData &D, int dim);
 
+// B operand image of the 3D patch-GEMM smoother (smoother3d_gemm.cuh).  The
+// patch step x_I = G u, G = [A_II^{-1} | -A_II^{-1} A_IB] over the (2k+1)^3
+// box (reference-cell A, FP64), split by the parity of the box in z:
+//   G_E (k (2k-1)^2 rows, (k+1)(2k+1)^2 columns), G_O ((k-1)(2k-1)^2 rows,
+//   k (2k+1)^2 columns),
+// row index zp * (2k-1)^2 + yi * (2k-1) + xi (zp: interior plane pair, k-1 the
+// centre plane), column index p * (2k+1)^2 + y * (2k+1) + x (p: box plane
+// pair, k the centre plane), the factors 1/2 of the folding included.  Each
+// block is cut into chunks of `ck` columns; a chunk holds `nb` rows (zero
+// padded) in the K-major no-swizzle operand layout of tcgen05 (8-row groups
+// of ck/4 core matrices of 8 rows x 16 bytes), values rounded to nearest TF32.
+// Returns G_E's chunks followed by G_O's as FP32 words.
+std::vector<float> patch_gemm_image(const DegreeData &D, int nbe, int nbo, int ck);
+
 // Inverse of the symmetric positive definite n x n matrix A (row-major,
 // overwritten): Cholesky factorisation A = L L^T, W = L^{-1}, A^{-1} = W^T W,
 // every inner product over contiguous rows, independent rows on host threads

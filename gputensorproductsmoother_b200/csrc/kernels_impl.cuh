@@ -10,6 +10,7 @@
 #include "laplace.cuh"
 #include "smoother.cuh"
 #include "smoother3d.cuh"
+#include "smoother3d_gemm.cuh"
 #include "smoother3d_tc.cuh"
 #include "smoother3d_warp.cuh"
 #include "smoother_variants.cuh"
@@ -120,6 +121,9 @@ cudaError_t set_attributes()
   TPS_SET((kappa_smoother_kernel<3, K, T>), (sizeof(T) * KSm<3, K, T>::ELEMS));
 #if TPS_DEGREE >= 2
   if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_tc_kernel<K>), (Tc3<K>::BYTES));
+#if TPS_DEGREE <= 4
+  if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_gemm_kernel<K>), (Pg3<K>::BYTES));
+#endif
 #endif
 #undef TPS_SET
   return cudaSuccess;
@@ -129,6 +133,14 @@ cudaError_t upload(const DegreeData &D)
 {
   cudaError_t e = upload_one<double>(D);
   if (e == cudaSuccess) e = upload_one<float>(D);
+#if TPS_DEGREE >= 2 && TPS_DEGREE <= 4
+  {
+    // built once per process (FP64 dense patch algebra), copied to every device that loads it
+    static const std::vector<float> img = patch_gemm_image(D, Pg3<K>::NBE, Pg3<K>::NBO, Pg3<K>::CK);
+    if (e == cudaSuccess && img.size() != static_cast<size_t>(Pg3<K>::IMG_FLOATS)) e = cudaErrorInvalidValue;
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_pg3_image<K>, img.data(), sizeof(float) * img.size());
+  }
+#endif
   if (e == cudaSuccess) e = set_attributes<double>();
   if (e == cudaSuccess) e = set_attributes<float>();
   return e;
@@ -319,6 +331,41 @@ int tc_grid(int n_units)
 cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const void *b, int colour,
                         double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t s)
 {
+#if TPS_DEGREE <= 4
+  {
+    // degrees 2..4: the patch step as one GEMM over the colour's patches
+    int nx, ny, nz, count;
+    colour_lattice(3, g.n, colour, nx, ny, nz, count);
+    if (count == 0) return cudaSuccess;
+    const double sc = stiffness_scale(3, g.h);
+    Sm3Args a;
+    a.nx_c = nx;
+    a.ny_c = ny;
+    a.n_patches = count;
+    a.cx = colour & 1;
+    a.cy = (colour >> 1) & 1;
+    a.cz = (colour >> 2) & 1;
+    a.n_batches = count;
+    a.zero_x = zero_x;
+    a.sy = l.sy;
+    a.sz = l.sz;
+    magic_div(static_cast<uint32_t>(nx), a.mx, a.sx);
+    magic_div(static_cast<uint32_t>(nx) * static_cast<uint32_t>(ny), a.mxy, a.sxy);
+    static int n_sm = 0;
+    if (n_sm == 0) {
+      int dev = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+      if (n_sm < 1) n_sm = 1;
+    }
+    const int tiles = static_cast<int>(ceil_div(count, 128));
+    TPS_LAUNCH((smoother3d_gemm_kernel<K>), tiles < n_sm ? tiles : n_sm, Pg3<K>::NT, Pg3<K>::BYTES, s,
+        static_cast<float *>(x), static_cast<const float *>(b), a, static_cast<float>(sc),
+        static_cast<float>(omega / sc), err);
+    (void)maps;
+    return cudaGetLastError();
+  }
+#else
   {
     using C = Tc3<K>;
     if (!maps || !maps->tc_valid) return cudaErrorInvalidValue;
@@ -344,6 +391,7 @@ cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const 
         static_cast<float *>(x), a, static_cast<float>(sc), static_cast<float>(omega / sc), err);
     return cudaGetLastError();
   }
+#endif
 }
 
 cudaError_t encode_tc_maps(const VecLayout &l, void *x, const void *b, SmootherMaps *out)

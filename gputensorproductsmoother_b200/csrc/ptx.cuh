@@ -79,6 +79,26 @@ __device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// plain arrival on an mbarrier (release at CTA scope)
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
+// global to shared memory, completion counted on `bar`; no tensor map, no
+// multicast (the source is this GPU's own memory)
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+  asm volatile(
+      "{\n\t.reg .u64 g;\n\t"
+      "cvta.to.global.u64 g, %1;\n\t"
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [g], %2, [%3];\n\t}" ::"r"(
+          smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(src)), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
 // Bounded wait on an mbarrier phase by one thread: gives up after `limit` SM
 // cycles (default 2^31, about a second) and reports failure instead of
 // spinning forever.
@@ -176,6 +196,35 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float *v)
                : "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// four 16-column loads of this thread's TMEM lane (32x32b.x16, columns
+// 16-aligned as for tmem_ld16) and one wait for all of them; the registers
+// are in/out operands of the wait, so no use is scheduled before it
+__device__ __forceinline__ void tmem_ld16x4(uint32_t t0, uint32_t t1, uint32_t t2, uint32_t t3, float *v)
+{
+  uint32_t r[64];
+#define TPS_LD16(o, ta)                                                                                          \
+  asm volatile(                                                                                                  \
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, " \
+      "%15}, [%16];"                                                                                             \
+      : "=r"(r[o + 0]), "=r"(r[o + 1]), "=r"(r[o + 2]), "=r"(r[o + 3]), "=r"(r[o + 4]), "=r"(r[o + 5]),         \
+        "=r"(r[o + 6]), "=r"(r[o + 7]), "=r"(r[o + 8]), "=r"(r[o + 9]), "=r"(r[o + 10]), "=r"(r[o + 11]),       \
+        "=r"(r[o + 12]), "=r"(r[o + 13]), "=r"(r[o + 14]), "=r"(r[o + 15])                                      \
+      : "r"(ta))
+  TPS_LD16(0, t0);
+  TPS_LD16(16, t1);
+  TPS_LD16(32, t2);
+  TPS_LD16(48, t3);
+#undef TPS_LD16
+#define TPS_RW16(o)                                                                                             \
+  "+r"(r[o + 0]), "+r"(r[o + 1]), "+r"(r[o + 2]), "+r"(r[o + 3]), "+r"(r[o + 4]), "+r"(r[o + 5]), "+r"(r[o + 6]), \
+      "+r"(r[o + 7]), "+r"(r[o + 8]), "+r"(r[o + 9]), "+r"(r[o + 10]), "+r"(r[o + 11]), "+r"(r[o + 12]),          \
+      "+r"(r[o + 13]), "+r"(r[o + 14]), "+r"(r[o + 15])
+  asm volatile("tcgen05.wait::ld.sync.aligned;" : TPS_RW16(0), TPS_RW16(16), TPS_RW16(32), TPS_RW16(48) : : "memory");
+#undef TPS_RW16
+#pragma unroll
+  for (int i = 0; i < 64; ++i) v[i] = __uint_as_float(r[i]);
 }
 
 // round to the nearest TF32 value (low 13 mantissa bits cleared)
