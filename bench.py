@@ -545,6 +545,23 @@ def main():
         torch.cuda.synchronize()
         ms64 = e0.elapsed_time(e1) / n64
 
+        # the same FP64 CG with the TF32 V-cycle (3D degrees 2..4: the
+        # tensor-core patch-GEMM smoother), reported beside the headline
+        tf32 = None
+        if dim == 3 and k >= 2:
+            for _ in range(max(1, args.warmup // 2)):
+                reptc = solve("tf32")
+            e0.record(stream)
+            for _ in range(n64):
+                reptc = solve("tf32")
+            e1.record(stream)
+            torch.cuda.synchronize()
+            mstc = e0.elapsed_time(e1) / n64
+            errtc = (torch.linalg.norm(x - x64) / torch.linalg.norm(x64)).item()
+            tf32 = {"ms_per_step": mstc, "value": job_throughput(world, nint, mstc), "iterations": reptc.iterations,
+                    "final_rel_residual": reptc.final_residual, "error_vs_fp64_solve": errtc,
+                    "speedup_vs_fp64": ms64 / mstc}
+
         for _ in range(args.warmup):
             rep = solve("fp32")
         torch.cuda.synchronize()
@@ -578,6 +595,12 @@ def main():
         launch_ms = sweep_ms / colours
         launch_bytes = bytes_sweep / colours
         achieved = launch_bytes / (launch_ms * 1e-3) / 1e9
+        # the same sweep with the TF32 patch-GEMM smoother (tensor cores)
+        tf32_sweep_ms = None
+        if tf32 is not None:
+            L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_TF32, 3, ctypes.byref(msw), sp), P.handle)
+            L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_TF32, 20, ctypes.byref(msw), sp), P.handle)
+            tf32_sweep_ms = msw.value
 
         # e2e through the public C API with host buffers: H2D of b (pinned), the
         # solve from x = 0 (the reference's starting guess, set on the device),
@@ -636,6 +659,11 @@ def main():
         "fp64": {"ms_per_step": ms64, "value": job_throughput(world, nint, ms64),
                  "iterations": rep64.iterations},
         "mixed_speedup_vs_fp64": ms64 / ms,
+        "tf32_vcycle": tf32,
+        "tf32_smoother": None if tf32_sweep_ms is None else {
+            "kernel": f"smoother3d_gemm_kernel<{k}>", "ms_per_sweep": tf32_sweep_ms,
+            "achieved_GBps": bytes_sweep / (tf32_sweep_ms * 1e-3) / 1e9,
+            "frac": bytes_sweep / (tf32_sweep_ms * 1e-3) / 1e9 / hbm_peak},
         "error_vs_fp64_solve": err,
         "e2e": {"value": job_throughput(world, nint, e2e_ms), "unit": "DoF/s",
                 "h2d_bytes_per_step": 8 * P.n_dofs(), "d2h_bytes_per_step": 8 * P.n_dofs(),
