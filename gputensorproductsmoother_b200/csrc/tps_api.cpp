@@ -158,6 +158,7 @@ struct VcycleVectors {
 
 struct tps_handle {
   int dim = 0, k = 0, n_coarse = 0, n_levels = 0, device = 0;
+  int n_sm = 148;  // multiprocessors of the device
   double omega = 1.0;
   std::vector<LevelGeomH> lv;
   const KernelTable *kt = nullptr;
@@ -560,26 +561,38 @@ void level_smooth(tps_handle *h, int level, int p, const VecLayout &lay, void *x
 // input d[level], output su[level]; tc: FP32 3D sweeps on the tensor cores;
 // zero_init = false continues from the current su[level] (a further cycle of
 // v_cycle(level, n_cycles), include/solver.cuh:798-805)
+// Inside the TF32 V-cycle the tensor-core smoother runs a level only where it
+// is faster than the FP32 SIMT kernels: degrees 2..4 (the patch-GEMM kernel)
+// on levels whose colour 0 fills a wave of 128-patch tiles on every SM.
+// Smaller levels are latency-bound and keep the SIMT smoother.
+bool tc_pays(const tps_handle *h, int level)
+{
+  if (h->dim != 3 || h->k > 4) return false;
+  const int64_t c = h->lv[level].n / 2;
+  return c * c * c >= 128 * static_cast<int64_t>(h->n_sm);
+}
+
 void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s, bool tc,
                 bool zero_init = true)
 {
   VcycleVectors &V = h->vc[p];
   if (level == 0) {
-    coarse_solve(h, p, s, tc);
+    coarse_solve(h, p, s, tc && tc_pays(h, 0));
     return;
   }
   const LevelGeomH &g = h->lv[level];
   const VecLayout &lay = V.layout[level], &lc = V.layout[level - 1];
   const int di = h->dim - 2;
   if (zero_init) TPS_CUDA(cudaMemsetAsync(V.su[level]->p, 0, V.su[level]->bytes, s));
-  level_smooth(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, zero_init, &V.maps[level], s, tc);
+  const bool tcl = tc && tc_pays(h, level);
+  level_smooth(h, level, p, lay, V.su[level]->p, V.d[level]->p, false, zero_init, &V.maps[level], s, tcl);
   level_laplace(h, level, p, lay, V.t[level]->p, V.su[level]->p, V.d[level]->p, 1, s);
   TPS_CUDA(h->kt->restrict_[di][p](h->lv[level - 1], lc, lay, V.d[level - 1]->p, V.t[level]->p,
                                    V.tmp[level]->p, 0, s));
   vcycle_rec(h, level - 1, p, symmetric, s, tc);
   TPS_CUDA(h->kt->prolong[di][p](h->lv[level - 1], lc, lay, V.su[level]->p, V.su[level - 1]->p,
                                  V.tmp[level]->p, s));
-  level_smooth(h, level, p, lay, V.su[level]->p, V.d[level]->p, symmetric, false, &V.maps[level], s, tc);
+  level_smooth(h, level, p, lay, V.su[level]->p, V.d[level]->p, symmetric, false, &V.maps[level], s, tcl);
 }
 
 int vprec_index(int precision)
@@ -919,8 +932,8 @@ void fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, c
   TPS_CUDA(cudaEventRecord(h->ev0, s));
   // coarse level: coarse solve, then one more smoother step
   TPS_CUDA(launch_to_vcycle(V.d[0]->p, input_kind(precision), padmap(0), rhs[0], h->lv[0].N, s));
-  coarse_solve(h, p, s, tc);
-  smoother_sweep(h, 0, p, V.layout[0], V.su[0]->p, V.d[0]->p, false, false, &V.maps[0], s, tc);
+  coarse_solve(h, p, s, tc && tc_pays(h, 0));
+  smoother_sweep(h, 0, p, V.layout[0], V.su[0]->p, V.d[0]->p, false, false, &V.maps[0], s, tc && tc_pays(h, 0));
   double *sol0 = L == 0 ? x : h->fmg_sol[0]->as<double>();
   TPS_CUDA(launch_from_vcycle(sol0, V.su[0]->p, zk, padmap(0), h->lv[0].N, s));
   for (int l = 1; l <= L; ++l) {
@@ -1111,6 +1124,7 @@ int tps_create(const tps_problem *pb, tps_handle **out)
     h->omega = pb->relaxation;
     h->device = pb->device;
     TPS_CUDA(cudaSetDevice(pb->device));
+    TPS_CUDA(cudaDeviceGetAttribute(&h->n_sm, cudaDevAttrMultiProcessorCount, pb->device));
     for (int l = 0; l < pb->n_levels; ++l) {
       LevelGeomH g;
       g.n = pb->n_coarse << l;

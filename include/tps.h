@@ -128,7 +128,10 @@ typedef enum {
   TPS_VCYCLE_F64_ROUNDED = 2, /* FP64 V-cycle fed with FP32-rounded input: the
                                 reference's "double" V-cycle (include/solver.cuh:64-78) */
   TPS_VCYCLE_TF32 = 3         /* as TPS_VCYCLE_F32, with the 3D patch solves on the tensor
-                                cores (TF32 operands, FP32 accumulation) */
+                                cores (TF32 operands, FP32 accumulation) on the levels
+                                where that is faster: degrees 2..4, colours of at least
+                                128 patches per multiprocessor; the other levels use the
+                                FP32 smoother */
 } tps_vcycle_precision;
 
 /* MultigridSolvers::vmult (include/solver.cuh:1915-1930): dst = V-cycle(src) on the
