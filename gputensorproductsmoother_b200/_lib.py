@@ -93,6 +93,7 @@ SIGNATURES = [
     ("tps_device_status", ctypes.c_int, [_VP]),
     ("tps_selftest_wait_timeout", ctypes.c_int, [_VP, ctypes.c_longlong, _VP]),
     ("tps_inject_alloc_failure", None, [ctypes.c_int]),
+    ("tps_check_colouring", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tps_batch_create", ctypes.c_int, [ctypes.POINTER(TpsProblem), ctypes.c_int, ctypes.POINTER(_VP)]),
     ("tps_batch_destroy", ctypes.c_int, [_VP]),
     ("tps_batch_last_error", ctypes.c_char_p, [_VP]),

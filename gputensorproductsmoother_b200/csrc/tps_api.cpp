@@ -31,6 +31,29 @@
 #include "fe_data.h"
 #include "kernel_table.h"
 
+// NVTX ranges around the solver phases (header-only NVTX v3; without an
+// attached tool each range is a check of one function pointer).  Ranges in
+// code that is captured into a CUDA graph mark the capture, not its replays.
+#ifndef TPS_NVTX
+#define TPS_NVTX 1
+#endif
+#if TPS_NVTX
+#include <nvtx3/nvToolsExt.h>
+namespace tps {
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
+}  // namespace tps
+#define TPS_RANGE_CAT_(a, b) a##b
+#define TPS_RANGE_CAT(a, b) TPS_RANGE_CAT_(a, b)
+#define TPS_RANGE(name) ::tps::NvtxRange TPS_RANGE_CAT(tps_nvtx_, __LINE__)(name)
+#else
+#define TPS_RANGE(name) ((void)0)
+#endif
+
 namespace tps {
 
 const KernelTable *kernel_table(int degree)
@@ -575,6 +598,11 @@ bool tc_pays(const tps_handle *h, int level)
 void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s, bool tc,
                 bool zero_init = true)
 {
+  static const char *const kLevelNames[] = {"V-cycle level 0", "V-cycle level 1", "V-cycle level 2",
+                                            "V-cycle level 3", "V-cycle level 4", "V-cycle level 5",
+                                            "V-cycle level 6", "V-cycle level 7", "V-cycle level 8",
+                                            "V-cycle level 9", "V-cycle level 10", "V-cycle level 11"};
+  TPS_RANGE(kLevelNames[level < 12 ? level : 11]);
   VcycleVectors &V = h->vc[p];
   if (level == 0) {
     coarse_solve(h, p, s, tc && tc_pays(h, 0));
@@ -712,6 +740,7 @@ void read_scalars(tps_handle *h, CGScalars &out, cudaStream_t s)
 int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x, tps_report *rep,
              cudaStream_t s)
 {
+  TPS_RANGE("tps_solve CG");
   const int p = vprec_index(o.precision);
   if (vprec_tc(o.precision)) check_tc(h);
   vcycle_vectors(h, p);
@@ -762,6 +791,7 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
     // stream capture is not available on the legacy default stream
     bool use_graph = o.use_graph != 0 && s != nullptr;
     for (;;) {
+      TPS_RANGE("CG iteration");
       read_scalars(h, hs, s);
       res = std::sqrt(hs.rr) / bnorm;
       if (it < TPS_MAX_HISTORY) rep->history[it] = res;
@@ -906,6 +936,7 @@ void tc_smoother_step(tps_handle *h, int level, void *x, const void *b, bool zer
 void fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, const double *const *bnd,
          double *x, tps_report *rep, cudaStream_t s)
 {
+  TPS_RANGE("tps_fmg");
   const int p = vprec_index(precision), L = h->n_levels - 1, dim = h->dim;
   const bool tc = vprec_tc(precision);
   if (tc) check_tc(h);
@@ -982,6 +1013,7 @@ void fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, c
 int solve_gmres(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
                 tps_report *rep, cudaStream_t s)
 {
+  TPS_RANGE("tps_solve GMRES");
   ensure_krylov(h);
   vcycle_vectors(h, vprec_index(o.precision));
   const LevelGeomH &g = h->fine();
@@ -1607,6 +1639,69 @@ int tps_solve_host_many(tps_handle *h, const tps_solve_opts *opts, int n, const 
   return status;
 }
 
+int tps_check_colouring(int dim, int degree, int n_cells)
+{
+  g_create_error.clear();
+  if ((dim != 2 && dim != 3) || degree < 1 || degree > kMaxDegree || n_cells < 2 || n_cells > 512) {
+    g_create_error = "tps_check_colouring: dim 2 or 3, degree 1..7, 2..512 cells";
+    return TPS_ERR_INVALID;
+  }
+  const int k = degree, n = n_cells, N1 = n * k + 1, nc = 1 << dim;
+  const int64_t NN = dim == 3 ? int64_t(N1) * N1 * N1 : int64_t(N1) * N1;
+  auto at = [&](int x, int y, int z) { return x + int64_t(N1) * (y + int64_t(N1) * z); };
+  std::vector<uint8_t> interior(static_cast<size_t>(NN));  // owner marks of the current colour
+  std::vector<uint8_t> centre(static_cast<size_t>(NN), 0);  // vertex patches seen over all colours
+  int64_t total = 0;
+  auto fail = [&](const std::string &m) {
+    g_create_error = "tps_check_colouring: " + m;
+    return TPS_ERR_INVALID;
+  };
+  for (int c = 0; c < nc; ++c) {
+    int nx, ny, nz, count;
+    colour_lattice(dim, n, c, nx, ny, nz, count);
+    total += count;
+    std::fill(interior.begin(), interior.end(), 0);
+    const int cx = c & 1, cy = (c >> 1) & 1, cz = (c >> 2) & 1;
+    const int ez = dim == 3 ? 2 * k - 1 : 1;  // interior extent in z
+    // the interiors of one colour's patches are disjoint
+    for (int jz = 0; jz < nz; ++jz)
+      for (int jy = 0; jy < ny; ++jy)
+        for (int jx = 0; jx < nx; ++jx) {
+          const int fx = (cx + 2 * jx) * k, fy = (cy + 2 * jy) * k, fz = dim == 3 ? (cz + 2 * jz) * k : -1;
+          if (fx + 2 * k > N1 - 1 || fy + 2 * k > N1 - 1 || (dim == 3 && fz + 2 * k > N1 - 1))
+            return fail("patch box outside the level");
+          const int64_t v = at(fx + k, fy + k, dim == 3 ? fz + k : 0);
+          if (centre[v]) return fail("vertex patch of colour " + std::to_string(c) + " seen twice");
+          centre[v] = 1;
+          for (int z = 0; z < ez; ++z)
+            for (int y = 1; y < 2 * k; ++y)
+              for (int x = 1; x < 2 * k; ++x) {
+                const int64_t i = at(fx + x, fy + y, dim == 3 ? fz + 1 + z : 0);
+                if (interior[i]) return fail("colour " + std::to_string(c) + ": patch interiors overlap");
+                interior[i] = 1;
+              }
+        }
+    // no patch reads (its box ring) what another patch of the colour writes
+    for (int jz = 0; jz < nz; ++jz)
+      for (int jy = 0; jy < ny; ++jy)
+        for (int jx = 0; jx < nx; ++jx) {
+          const int fx = (cx + 2 * jx) * k, fy = (cy + 2 * jy) * k, fz = dim == 3 ? (cz + 2 * jz) * k : 0;
+          const int bz = dim == 3 ? 2 * k + 1 : 1;
+          for (int z = 0; z < bz; ++z)
+            for (int y = 0; y <= 2 * k; ++y)
+              for (int x = 0; x <= 2 * k; ++x) {
+                const bool ring = x == 0 || x == 2 * k || y == 0 || y == 2 * k || (dim == 3 && (z == 0 || z == 2 * k));
+                if (ring && interior[at(fx + x, fy + y, fz + z)])
+                  return fail("colour " + std::to_string(c) + ": a box ring meets another patch's interior");
+              }
+        }
+  }
+  // every interior vertex is the centre of exactly one patch
+  const int64_t expect = dim == 3 ? int64_t(n - 1) * (n - 1) * (n - 1) : int64_t(n - 1) * (n - 1);
+  if (total != expect) return fail("patch count " + std::to_string(total) + " != " + std::to_string(expect));
+  return TPS_OK;
+}
+
 int tps_device_status(tps_handle *h)
 {
   bool timed_out = false;
@@ -1927,6 +2022,7 @@ int tps_batch_system(tps_batch *b, int i, tps_handle **h)
 int tps_batch_solve(tps_batch *B, const tps_solve_opts *opts, const double *const *rhs, double *const *x,
                     tps_report *reports, void *stream)
 {
+  TPS_RANGE("tps_batch_solve");
   return batch_guarded(B, [&]() -> int {
     if (!opts || !rhs || !x || !reports) throw ApiError(TPS_ERR_INVALID, "null argument");
     if (opts->driver != TPS_DRIVER_CG) throw ApiError(TPS_ERR_INVALID, "batched solves use the CG driver");

@@ -307,6 +307,15 @@ int tps_device_status(tps_handle *h);
  * after `cycles` SM cycles (1 .. 2^31) and records the timeout in the handle's
  * flag like a smoother launch would.  Asynchronous on `stream`. */
 int tps_selftest_wait_timeout(tps_handle *h, long long cycles, void *stream);
+/* Host self-check of the 2^dim colouring (no device work): on a level of
+ * n_cells per direction, every interior vertex is the centre of exactly one
+ * patch, the interiors of one colour's patches are disjoint, and no patch's
+ * box ring (read while the colour runs) meets another patch's interior
+ * (written) -- the race freedom of the in-place colour sweep, which the
+ * reference asserts only for the colour sizes in debug builds
+ * (include/patch_base.template.cuh:1279-1284).  TPS_OK, or TPS_ERR_INVALID
+ * with the first violation in tps_last_error(NULL). */
+int tps_check_colouring(int dim, int degree, int n_cells);
 /* Testing hook: the n-th device allocation of the library from now (n >= 1,
  * counted over all handles and batches of the process) fails as cudaMalloc does
  * on a full device, so the calls report TPS_ERR_ALLOC; n = 0 disarms it. */

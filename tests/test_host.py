@@ -74,3 +74,25 @@ def test_smoother_byte_model_counts_unions(dim, k, n):
 
 def test_launch_model_is_positive():
     assert bench.launches_per_solve(3, 6, 6) > bench.launches_per_solve(3, 6, 1) > 0
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_colouring_is_race_free(dim):
+    """Host bitmap check of the 2^d colouring (tps_check_colouring): every
+    interior vertex is one patch centre, same-colour interiors are disjoint
+    and no box ring read by a colour meets an interior it writes, for every
+    degree and odd, even and non-power-of-two meshes."""
+    from gputensorproductsmoother_b200 import _lib as L
+    lib = L.lib()
+    for k in range(1, 8):
+        for n in (2, 3, 4, 5, 6, 8, 12, 16) if dim == 3 else (2, 3, 4, 5, 7, 8, 16, 24, 64):
+            assert lib.tps_check_colouring(dim, k, n) == 0, (dim, k, n, lib.tps_last_error(None))
+
+
+def test_colouring_check_rejects_bad_arguments():
+    from gputensorproductsmoother_b200 import _lib as L
+    lib = L.lib()
+    assert lib.tps_check_colouring(4, 2, 8) == 1
+    assert lib.tps_check_colouring(3, 0, 8) == 1
+    assert lib.tps_check_colouring(3, 2, 1) == 1
+    assert b"tps_check_colouring" in lib.tps_last_error(None)
