@@ -52,7 +52,20 @@ def parse():
                     help="--mode smoother: FP32 SIMT kernel, tensor-core (TF32) kernel or FP64")
     ap.add_argument("--directions", type=int, default=64,
                     help="--mode adjoint: random unit directions of the finite-difference check")
-    return ap.parse_args()
+    ap.add_argument("--config", default=None,
+                    help="JSON file of option values (keys as the long option names, '-' or '_'); "
+                         "options given on the command line take precedence")
+    args = ap.parse_args()
+    if args.config:
+        with open(args.config) as f:
+            cfg = json.load(f)
+        known = {a.dest for a in ap._actions}
+        unknown = [key for key in cfg if key.replace("-", "_") not in known]
+        if unknown:
+            ap.error(f"unknown keys in {args.config}: {unknown}")
+        ap.set_defaults(**{key.replace("-", "_"): v for key, v in cfg.items()})
+        args = ap.parse_args()
+    return args
 
 
 def run_operator_only(args):

@@ -96,3 +96,19 @@ def test_colouring_check_rejects_bad_arguments():
     assert lib.tps_check_colouring(3, 0, 8) == 1
     assert lib.tps_check_colouring(3, 2, 1) == 1
     assert b"tps_check_colouring" in lib.tps_last_error(None)
+
+
+def test_bench_config_file(tmp_path, monkeypatch):
+    """bench.py --config: JSON option values, command-line options win,
+    unknown keys are rejected."""
+    import json
+    import sys
+    cfg = tmp_path / "c.json"
+    cfg.write_text(json.dumps({"mode": "smoother", "steps": 2, "no-cpu-baseline": True}))
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--config", str(cfg), "--steps", "5"])
+    a = bench.parse()
+    assert (a.mode, a.steps, a.no_cpu_baseline, a.warmup) == ("smoother", 5, True, 3)
+    cfg.write_text(json.dumps({"stepz": 2}))
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--config", str(cfg)])
+    with pytest.raises(SystemExit):
+        bench.parse()
