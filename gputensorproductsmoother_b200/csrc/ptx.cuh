@@ -48,7 +48,7 @@ __device__ __forceinline__ uint32_t mbar_try_wait(uint64_t *bar, uint32_t parity
 }
 
 // 3D tiled TMA load global -> shared, completion counted on `bar`.
-// (No multicast: every load reads this GPU's own memory into this CTA.)
+// (Every load reads this GPU's own memory into this CTA alone.)
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar, int x,
                                             int y, int z)
 {
@@ -86,8 +86,8 @@ __device__ __forceinline__ void mbar_arrive(uint64_t *bar)
 }
 
 // bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
-// global to shared memory, completion counted on `bar`; no tensor map, no
-// multicast (the source is this GPU's own memory)
+// global to shared memory, completion counted on `bar`; no tensor map; the
+// source is this GPU's own memory and the destination this CTA alone
 __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
   asm volatile(
