@@ -182,20 +182,30 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
   return cudaGetLastError();
 }
 
+// CTAs of `kern` resident per SM (at least 1) and the SM count of the
+// current device; the callers keep it in a function-local static, whose
+// initialisation is thread-safe
+struct Residency {
+  int per_sm = 1, n_sm = 1;
+};
+template <typename... KArgs>
+Residency residency(void (*kern)(KArgs...), int threads, size_t smem)
+{
+  Residency r;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (cudaDeviceGetAttribute(&r.n_sm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || r.n_sm < 1) r.n_sm = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&r.per_sm, kern, threads, smem) != cudaSuccess || r.per_sm < 1)
+    r.per_sm = 1;
+  return r;
+}
+
 template <typename T, bool TMA, int PPB>
 int sm3_grid(int n_batches)
 {
-  static int per_sm = -1, n_sm = 0;
-  if (per_sm < 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_kernel<K, T, TMA, PPB>,
-                                                      Sm3<K, T, PPB>::NT, Sm3<K, T, PPB>::BYTES) != cudaSuccess ||
-        per_sm < 1)
-      per_sm = 1;
-  }
-  const int g = per_sm * n_sm;
+  static const Residency r =
+      residency(smoother3d_kernel<K, T, TMA, PPB>, Sm3<K, T, PPB>::NT, Sm3<K, T, PPB>::BYTES);
+  const int g = r.per_sm * r.n_sm;
   return n_batches < g ? n_batches : g;
 }
 
@@ -230,18 +240,9 @@ void smoother3d_warp_launch(const Sm3Args &a, const SmootherMaps *maps, void *x,
   if constexpr (wp3_enabled<K, T>()) {
     constexpr int WA = wp3_warps<K, T>();
     using S = Wp3<K, T, WA>;
-    static int per_sm = -1, n_sm = 0;
-    if (per_sm < 0) {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_warp_kernel<K, T, WA>, S::NT,
-                                                        S::BYTES) != cudaSuccess ||
-          per_sm < 1)
-        per_sm = 1;
-    }
+    static const Residency r = residency(smoother3d_warp_kernel<K, T, WA>, S::NT, S::BYTES);
     const int need = static_cast<int>(ceil_div(a.n_patches, WA));
-    const int grid = need < per_sm * n_sm ? need : per_sm * n_sm;
+    const int grid = need < r.per_sm * r.n_sm ? need : r.per_sm * r.n_sm;
     TPS_LAUNCH((smoother3d_warp_kernel<K, T, WA>), grid, S::NT, S::BYTES, s,
         *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),
         static_cast<T *>(x), a, scale, fd, err);
@@ -312,18 +313,12 @@ int tc_grid(int n_units)
 {
   {
     using C = Tc3<K>;
-    static int per_sm = -1, n_sm = 0;
-    if (per_sm < 0) {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, smoother3d_tc_kernel<K>, C::NT, C::BYTES) !=
-              cudaSuccess ||
-          per_sm < 1)
-        per_sm = 1;
-      if (per_sm * C::TMEM_COLS > 512) per_sm = 512 / C::TMEM_COLS;
-    }
-    const int g = per_sm * n_sm;
+    static const Residency r = [] {
+      Residency q = residency(smoother3d_tc_kernel<K>, C::NT, C::BYTES);
+      if (q.per_sm * C::TMEM_COLS > 512) q.per_sm = 512 / C::TMEM_COLS;  // every CTA's TMEM fits at once
+      return q;
+    }();
+    const int g = r.per_sm * r.n_sm;
     return n_units < g ? n_units : g;
   }
 }
@@ -351,15 +346,10 @@ cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const 
     a.sz = l.sz;
     magic_div(static_cast<uint32_t>(nx), a.mx, a.sx);
     magic_div(static_cast<uint32_t>(nx) * static_cast<uint32_t>(ny), a.mxy, a.sxy);
-    static int n_sm = 0;
-    if (n_sm == 0) {
-      int dev = 0;
-      cudaGetDevice(&dev);
-      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-      if (n_sm < 1) n_sm = 1;
-    }
+    // one CTA per SM (its shared memory and TMEM allow no second)
+    static const Residency r = residency(smoother3d_gemm_kernel<K>, Pg3<K>::NT, Pg3<K>::BYTES);
     const int tiles = static_cast<int>(ceil_div(count, 128));
-    TPS_LAUNCH((smoother3d_gemm_kernel<K>), tiles < n_sm ? tiles : n_sm, Pg3<K>::NT, Pg3<K>::BYTES, s,
+    TPS_LAUNCH((smoother3d_gemm_kernel<K>), tiles < r.n_sm ? tiles : r.n_sm, Pg3<K>::NT, Pg3<K>::BYTES, s,
         static_cast<float *>(x), static_cast<const float *>(b), a, static_cast<float>(sc),
         static_cast<float>(omega / sc), err);
     (void)maps;
