@@ -347,9 +347,13 @@ cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const 
     magic_div(static_cast<uint32_t>(nx), a.mx, a.sx);
     magic_div(static_cast<uint32_t>(nx) * static_cast<uint32_t>(ny), a.mxy, a.sxy);
     // one CTA per SM (its shared memory and TMEM allow no second)
-    static const Residency r = residency(smoother3d_gemm_kernel<K>, Pg3<K>::NT, Pg3<K>::BYTES);
+    static const int n_sm = [] {
+      int dev = 0, n = 0;
+      cudaGetDevice(&dev);
+      return cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0 ? n : 1;
+    }();
     const int tiles = static_cast<int>(ceil_div(count, 128));
-    TPS_LAUNCH((smoother3d_gemm_kernel<K>), tiles < r.n_sm ? tiles : r.n_sm, Pg3<K>::NT, Pg3<K>::BYTES, s,
+    TPS_LAUNCH((smoother3d_gemm_kernel<K>), tiles < n_sm ? tiles : n_sm, Pg3<K>::NT, Pg3<K>::BYTES, s,
         static_cast<float *>(x), static_cast<const float *>(b), a, static_cast<float>(sc),
         static_cast<float>(omega / sc), err);
     (void)maps;
