@@ -65,6 +65,7 @@ def test_null_arguments_are_rejected():
     assert lib.tps_level_info(None, 0, None, None) == 1
     assert lib.tps_device_status(None) == 1
     assert lib.tps_selftest_wait_timeout(None, 1000, None) == 1
+    assert lib.tps_solve_host_many(None, None, 1, None, None, None) == 1
 
 
 def test_alloc_failure_hook_arms_and_disarms():
