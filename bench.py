@@ -13,6 +13,13 @@ solve is reported.
 For N > 1 every rank solves its own seeded instance (independent problems, no
 collective on the data path): value = total DoFs solved per second, timed as
 the max over ranks.
+
+At N = 1 the line also carries, measured after the headline's timed region,
+a record of every other configuration under "configs": 2D Q2 64^2 (FP64 and
+FP32 V-cycles), 3D Q7 32^3 (FP64, FP32 and TF32 tensor-core V-cycles), the
+batched Q3 configuration (one graph launch per batch) and the adjoint check
+of the variable-coefficient Q4 48^3 problem on 64 directions.  The CPU
+baseline is one complete oracle solve of the headline instance.
 """
 from __future__ import annotations
 
@@ -40,6 +47,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="poisson3d_q4_64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the sub-records of the other configurations (2D Q2 64^2, Q7 32^3, "
+                         "batched Q3, adjoint Q4 48^3) that follow the headline measurement")
     ap.add_argument("--mode", default="solve",
                     choices=["solve", "smoother", "operator", "batch", "adjoint", "micro"],
                     help="smoother / operator: only time the finest-level smoother "
@@ -221,72 +231,93 @@ def launches_per_solve(dim: int, n_levels: int, iterations: int) -> int:
     return init + per_it * max(iterations - 1, 0) + readbacks
 
 
-def cpu_baseline(args, dim, k, n, its_full):
-    """The CPU oracle (same algorithm: coloured patch smoother, FP32 V-cycle,
-    FP64 flexible CG) on the host cores, on a bounded sample: the first m CG
-    iterations of the same instance, scaled to the full iteration count."""
-    import numpy as np
+# DRAM traffic of the roofline kernel: ncu captures of its colour-0 launch
+# (dram__bytes_read.sum + dram__bytes_write.sum, the launch's algorithmic
+# bytes, the summary it comes from).  The bench reports it scaled to the
+# average launch by algorithmic bytes; a kernel without a capture reports null.
+TRAFFIC_CAPTURES = {
+    ("smoother3d_warp_kernel<4,float>", "poisson3d_q4_64"):
+        (136.6e6, 167.5e6, "profiles/smoother3d_warp_k4_f32_poisson3d_q4_64.md"),
+}
+
+
+def traffic_per_launch(kernel: str, workload: str, launch_bytes: float):
+    cap = TRAFFIC_CAPTURES.get((kernel, workload))
+    return None if cap is None else cap[0] * launch_bytes / cap[1]
+
+
+def workload_config(args, world: int) -> dict:
+    """The workload description shared by both arms' JSON lines."""
+    from gputensorproductsmoother_b200 import problems, split_cells
+    dim, k, n, _ = problems.WORKLOADS[args.workload]
+    _, levels = split_cells(n)
+    return {"workload": args.workload, "dim": dim, "degree": k, "cells": n,
+            "dofs": (n * k + 1) ** dim, "interior_dofs": problems.interior_dofs(dim, k, n),
+            "levels": levels, "rel_tol": 1e-10, "parallelism": f"replicas x{world}",
+            "l2": "vectors (136 MB FP64) larger than L2; no flush"}
+
+
+def oracle_solve_timed(args, seed: int = 0):
+    """One full solve of the workload by the CPU oracle (the same algorithm:
+    coloured vertex-patch smoother, FP32 V-cycle, FP64 flexible CG to a 1e-10
+    relative residual, from x = 0) on all host cores; returns (seconds,
+    iterations, final relative residual)."""
     from oracle import oracle as O
     from gputensorproductsmoother_b200 import problems, split_cells
+    dim, k, n, gen = problems.WORKLOADS[args.workload]
     nc, nl = split_cells(n)
-    b = problems.WORKLOADS[args.workload][3](dim, k, n, 0, "cpu").numpy()
+    b = gen(dim, k, n, seed, "cpu").numpy()
     H = O.Hierarchy(dim, k, nc, nl)
-    m = 1
     t0 = time.perf_counter()
-    _, it, _ = H.solve_cg(b, precision=1, symmetric=True, rel_tol=1e-10, max_it=m)
+    _, it, hist = H.solve_cg(b, precision=1, symmetric=True, rel_tol=1e-10)
     t = time.perf_counter() - t0
-    # m iterations = (m + 1) V-cycles + m + 1 operator applications; scale per V-cycle
-    t_full = t * (its_full + 1) / (m + 1)
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    nint = (n * k - 1) ** dim
-    return {"value": nint / t_full, "unit": "DoF/s", "cores": cores, "kind": "port",
-            "sample": f"first {m} of {its_full} CG iterations of the same {n}^{dim} Q{k} "
-                      f"instance ({t:.1f} s), scaled by V-cycle count"}, t
+    return t, it, float(hist[-1] / hist[0])
+
+
+def host_threads() -> int:
+    return int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
+
+
+def cpu_baseline(args):
+    """The CPU oracle timed on the host cores: one complete solve of the same
+    instance (measured, not scaled)."""
+    from gputensorproductsmoother_b200 import problems
+    dim, k, n, _ = problems.WORKLOADS[args.workload]
+    t, it, res = oracle_solve_timed(args)
+    nint = problems.interior_dofs(dim, k, n)
+    return {"value": nint / t, "unit": "DoF/s", "cores": host_threads(), "kind": "port",
+            "sample": f"one complete solve of the same {n}^{dim} Q{k} instance ({it} CG iterations to "
+                      f"{res:.1e}, {t:.1f} s, measured)"}
 
 
 def run_reference(args):
-    """Reference arm: the reference's CPU-runnable implementation of this
-    path is the oracle port (the reference itself is GPU+deal.II only)."""
+    """Reference arm: the reference's implementation of this path needs a GPU
+    and deal.II, so its CPU-runnable counterpart is the oracle port (the same
+    algorithm).  Each step is one complete solve of the workload on all host
+    cores, timed; rank 0 only."""
     rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     from gputensorproductsmoother_b200 import problems
     dim, k, n, _ = problems.WORKLOADS[args.workload]
-    import numpy as np
-    from oracle import oracle as O
-    from gputensorproductsmoother_b200 import split_cells
-    nc, nl = split_cells(n)
-    b = problems.WORKLOADS[args.workload][3](dim, k, n, 0, "cpu").numpy()
-    H = O.Hierarchy(dim, k, nc, nl)
-    nint = (n * k - 1) ** dim
-    # each step: one V-cycle-preconditioned CG iteration pair bounded to 1 iteration,
-    # scaled to a full solve of `its` iterations
-    # iterations of a full solve: the same solver on a 16^d instance of the
-    # workload (multigrid iteration counts do not depend on the mesh size)
-    nc16, nl16 = split_cells(16)
-    H16 = O.Hierarchy(dim, k, nc16, nl16)
-    b16 = problems.WORKLOADS[args.workload][3](dim, k, 16, 0, "cpu").numpy()
-    _, its_full, _ = H16.solve_cg(b16, precision=1, symmetric=True, rel_tol=1e-10)
-    x, its, _ = H.solve_cg(b, precision=1, symmetric=True, rel_tol=1e-10, max_it=1)
-    times = []
+    nint = problems.interior_dofs(dim, k, n)
+    times, its = [], None
     for s in range(args.warmup + args.steps):
-        t0 = time.perf_counter()
-        H.solve_cg(b, precision=1, symmetric=True, rel_tol=1e-10, max_it=1)
-        t = time.perf_counter() - t0
+        t, it, res = oracle_solve_timed(args)
         if s >= args.warmup:
-            times.append(t * (its_full + 1) / 2)
+            times.append(t)
+            its = it
     ms = 1000 * statistics.mean(times)
     val = nint / (ms / 1000)
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": "DoF/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
-            "data": "synthetic", "config": {"workload": args.workload, "dim": dim, "degree": k,
-                                            "cells": n, "dofs": (n * k + 1) ** dim},
-            "cpu_baseline": {"value": val, "unit": "DoF/s", "cores": cores, "kind": "port",
-                             "sample": f"1 CG iteration (2 V-cycles) of the {n}^{dim} Q{k} "
-                                       f"instance per step, scaled to {its_full} iterations (the "
-                                       f"oracle's count on the 16^{dim} instance)"},
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 V-cycle / f64 CG",
+            "data": "synthetic (seeded sin-mode RHS)", "config": workload_config(args, world),
+            "iterations": its, "final_rel_residual": res,
+            "cpu_baseline": {"value": val, "unit": "DoF/s", "cores": host_threads(), "kind": "port",
+                             "sample": f"each step one complete solve of the {n}^{dim} Q{k} instance "
+                                       f"({its} CG iterations, measured)"},
             "e2e": {"value": val, "unit": "DoF/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -391,9 +422,14 @@ def batch_systems(seed: int = 0):
 
 
 def run_batch(args):
-    """Times --steps batched solves (one graph launch each) of batch_systems():
-    FP32 V-cycle, FP64 CG to 1e-10, right-hand sides i.i.d. uniform[-1,1]
-    nodal values; prints one JSON line."""
+    """--mode batch: prints measure_batch's record as one JSON line."""
+    print(json.dumps(dict(mode="batch", **measure_batch(args.warmup, args.steps))), flush=True)
+
+
+def measure_batch(warmup: int, steps: int) -> dict:
+    """Times `steps` batched solves (one graph launch each) of batch_systems()
+    after `warmup`: FP32 V-cycle, FP64 CG to 1e-10, right-hand sides i.i.d.
+    uniform[-1,1] nodal values."""
     import numpy as np
     import torch
     import gputensorproductsmoother_b200 as tps
@@ -410,12 +446,12 @@ def run_batch(args):
     xs = [torch.zeros_like(b) for b in rhs]
     stream = torch.cuda.Stream()
     with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
+        for _ in range(max(warmup, 1)):
             for x in xs:
                 x.zero_()
             _, reps = B.solve(rhs, xs, precision="fp32", rel_tol=1e-10)
         times = []
-        for _ in range(max(args.steps, 1)):
+        for _ in range(max(steps, 1)):
             for x in xs:
                 x.zero_()
             _, reps = B.solve(rhs, xs, precision="fp32", rel_tol=1e-10)
@@ -423,18 +459,22 @@ def run_batch(args):
     torch.cuda.synchronize()
     nint = sum((n * k - 1) ** d for (d, k, n) in systems)
     ms = statistics.median(times)
-    print(json.dumps({
-        "mode": "batch", "metric": "batched MG-CG DoF/s to 1e-10 (one graph launch per batch)",
-        "value": nint / (ms * 1e-3), "unit": "DoF/s", "ms_per_batch": ms, "steps": args.steps,
-        "systems": len(systems), "meshes": sorted({n for (_, _, n) in systems}),
-        "interior_dofs": nint, "iterations": sorted({r.iterations for r in reps}),
-        "all_converged": all(r.converged for r in reps),
-        "max_final_residual": max(r.final_residual for r in reps),
-        "graph_launches_per_batch": 1}), flush=True)
     B.close()
+    return {"metric": "batched MG-CG DoF/s to 1e-10 (one graph launch per batch)",
+            "value": nint / (ms * 1e-3), "unit": "DoF/s", "ms_per_batch": ms, "steps": steps,
+            "systems": len(systems), "meshes": sorted({n for (_, _, n) in systems}),
+            "interior_dofs": nint, "iterations": sorted({r.iterations for r in reps}),
+            "all_converged": all(r.converged for r in reps),
+            "max_final_residual": max(r.final_residual for r in reps),
+            "graph_launches_per_batch": 1}
 
 
 def run_adjoint(args):
+    """--mode adjoint: prints measure_adjoint's record as one JSON line."""
+    print(json.dumps(dict(mode="adjoint", **measure_adjoint(args.directions))), flush=True)
+
+
+def measure_adjoint(directions: int) -> dict:
     """Adjoint check of -div(kappa grad u) = f, Q4, 48^3 cells (coarse 3^3),
     kappa = exp(N(0, 0.5^2)) per cell, J = 0.5 ||u - u_t||^2 with u_t a smooth
     field of 8 random sine modes: dJ/df and dJ/dkappa (FP64, adjoint solve)
@@ -442,7 +482,7 @@ def run_adjoint(args):
     (i.i.d. N(0,1) entries for f, relative N(0,1) perturbations kappa * N(0,1)
     for kappa; unit-norm directions over 7.2M DoFs would leave a directional
     derivative ~1/2700 of the gradient norm, below the rounding of J / h).
-    Prints one JSON line with the worst relative deviations."""
+    Returns the worst and median relative deviations."""
     import numpy as np
     import torch
     import gputensorproductsmoother_b200 as tps
@@ -472,7 +512,7 @@ def run_adjoint(args):
     worst_f = worst_k = 0.0
     devs_f, devs_k = [], []
     t0 = time.perf_counter()
-    for d in range(args.directions):
+    for d in range(directions):
         df = torch.tensor(rng.standard_normal(N), device="cuda")
         dk = torch.tensor(rng.standard_normal(n ** dim), device="cuda") * kap
         with torch.no_grad():
@@ -482,13 +522,57 @@ def run_adjoint(args):
         devs_k.append(abs((gk * dk).sum().item() - fd_k.item()) / abs(fd_k.item()))
         worst_f, worst_k = max(devs_f), max(devs_k)
     t_fd = time.perf_counter() - t0
-    print(json.dumps({
-        "mode": "adjoint", "workload": "kappa_q4_48", "dofs": N, "directions": args.directions,
-        "fd_step": h, "max_rel_dev_df": worst_f, "max_rel_dev_dkappa": worst_k,
-        "median_rel_dev_df": statistics.median(devs_f), "median_rel_dev_dkappa": statistics.median(devs_k),
-        "within_1e-6": worst_f <= 1e-6 and worst_k <= 1e-6,
-        "s_forward_plus_adjoint": t_grad, "s_finite_differences": t_fd}), flush=True)
     P.close()
+    return {"workload": "kappa_q4_48", "dofs": N, "directions": directions,
+            "fd_step": h, "max_rel_dev_df": worst_f, "max_rel_dev_dkappa": worst_k,
+            "median_rel_dev_df": statistics.median(devs_f), "median_rel_dev_dkappa": statistics.median(devs_k),
+            "within_1e-6": worst_f <= 1e-6 and worst_k <= 1e-6,
+            "s_forward_plus_adjoint": t_grad, "s_finite_differences": t_fd}
+
+
+def measure_solves(workload: str, precisions, warmup: int = 1, reps: int = 3) -> dict:
+    """Solves of one configuration from x = 0 to 1e-10 with each V-cycle
+    precision (the first must be "fp64": the FP64 GPU solution the others'
+    errors refer to): best time of `reps` (CUDA events on the solving
+    stream), iterations, final residual, DoF/s."""
+    import torch
+    import gputensorproductsmoother_b200 as tps
+    from gputensorproductsmoother_b200 import problems
+    dim, k, n, _ = problems.WORKLOADS[workload]
+    P = tps.PoissonProblem(dim, k, n)
+    S = tps.MultigridSolvers(P)
+    b = problems.make_rhs(workload)
+    x = torch.zeros_like(b)
+    nint = problems.interior_dofs(dim, k, n)
+    out = {"dofs": P.n_dofs(), "interior_dofs": nint}
+    stream = torch.cuda.Stream()
+    x64 = None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for prec in precisions:
+            for _ in range(max(warmup, 1)):
+                x.zero_()
+                _, rep = S.solve_cg(b, x, precision=prec, rel_tol=1e-10)
+            best = 1e30
+            for _ in range(max(reps, 1)):
+                x.zero_()
+                e0.record(stream)
+                _, rep = S.solve_cg(b, x, precision=prec, rel_tol=1e-10)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            rec = {"ms": best, "dof_per_s": nint / (best * 1e-3), "iterations": rep.iterations,
+                   "final_rel_residual": rep.final_residual}
+            if x64 is None:
+                x64 = x.clone()
+            else:
+                rec["error_vs_fp64_solve"] = (torch.linalg.norm(x - x64) / torch.linalg.norm(x64)).item()
+            out[prec] = rec
+    if "fp64" in out:
+        for prec in precisions[1:]:
+            out[prec]["speedup_vs_fp64"] = out["fp64"]["ms"] / out[prec]["ms"]
+    P.close()
+    return out
 
 
 def main():
@@ -664,10 +748,7 @@ def main():
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 V-cycle / f64 CG",
         "data": "synthetic (seeded sin-mode RHS per rank)",
-        "config": {"workload": args.workload, "dim": dim, "degree": k, "cells": n,
-                   "dofs": P.n_dofs(), "interior_dofs": nint, "levels": P.n_levels,
-                   "rel_tol": 1e-10, "parallelism": f"replicas x{world}",
-                   "l2": "vectors (136 MB FP64) larger than L2; no flush"},
+        "config": workload_config(args, world),
         "iterations": rep.iterations, "final_rel_residual": resid_check,
         "fp64": {"ms_per_step": ms64, "value": job_throughput(world, nint, ms64),
                  "iterations": rep64.iterations},
@@ -686,21 +767,30 @@ def main():
                 "error_vs_fp64_solve": e2e_err},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                      "frac": achieved / hbm_peak,
-                     # DRAM bytes of one launch from the ncu capture of the colour-0 launch
-                     # (dram__bytes_read + write = 136.6 MB for 167.5 MB algorithmic),
-                     # scaled to the average launch by its algorithmic bytes
-                     "traffic": (136.6e6 * launch_bytes / 167.5e6) if args.workload == "poisson3d_q4_64" else None,
+                     "traffic": traffic_per_launch(kernel_name, args.workload, launch_bytes),
                      "traffic_unit": "bytes per launch",
+                     "traffic_source": TRAFFIC_CAPTURES.get((kernel_name, args.workload), (0, 0, None))[2],
                      "kernel": kernel_name,
                      "peak_source": peak_src,
                      "algorithmic_bytes_per_launch": launch_bytes, "launch_ms": launch_ms},
         "gpu_launches": args.steps * launches_per_solve(dim, P.n_levels, rep.iterations),
         "clocks": clocks,
     }
+    if rank == 0 and world == 1 and not args.no_configs:
+        # every other configuration, measured after the headline's timed region
+        subs = {}
+        for name, fn in (("poisson2d_q2_64", lambda: measure_solves("poisson2d_q2_64", ("fp64", "fp32"))),
+                         ("poisson3d_q7_32", lambda: measure_solves("poisson3d_q7_32", ("fp64", "fp32", "tf32"))),
+                         ("batched_q3_32rhs_12meshes", lambda: measure_batch(2, 5)),
+                         ("adjoint_kappa_q4_48", lambda: measure_adjoint(64))):
+            try:
+                subs[name] = fn()
+            except Exception as exc:  # report, never hide
+                subs[name] = {"error": repr(exc)}
+        line["configs"] = subs
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            cb, _ = cpu_baseline(args, dim, k, n, rep.iterations)
-            line["cpu_baseline"] = cb
+            line["cpu_baseline"] = cpu_baseline(args)
         except Exception as exc:  # report, never hide
             line["cpu_baseline"] = {"error": repr(exc)}
     if rank == 0:

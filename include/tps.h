@@ -287,8 +287,10 @@ int tps_batch_solve(tps_batch *b, const tps_solve_opts *opts, const double *cons
  * process exits); 8 * (2n_c k+1) * (n_c k+1)^2 bytes (FP64; half for FP32)
  * must fit, larger sizes return TPS_ERR_INVALID.  n_coarse_cells: cells per
  * direction of the coarse level; vectors lexicographic.  The first call on a
- * device does the set-up (symbol address, 1D tables): make it before any
- * stream capture.  Calls share the array: calls that overlap on the GPU race. */
+ * device (and the first one after the device's context was reset, e.g. by
+ * cudaDeviceReset) uploads the 1D tables to constant memory: make it before
+ * any stream capture.  Every call looks the array's address up in the current
+ * context.  Calls share the array: calls that overlap on the GPU race. */
 int tps_restrict_add_noalloc(int dim, int degree, int n_coarse_cells, int dtype, void *coarse,
                              const void *fine, void *stream);
 

@@ -241,3 +241,96 @@ class Hierarchy:
         it = lib().orc_solve_gmres(self.h, precision, _p(b), _p(x), reduce, abs_tol, max_it, basis,
                                    _p(hist))
         return x, it, hist[: it + 1]
+
+
+# ---- adjoint of the variable-coefficient solve (no reference counterpart) ----
+# Restated from the definitions, as the FP64 reference the GPU adjoint is
+# checked against: A(kappa) = sum_c kappa_c A_c (cell stiffness of Q_k with
+# QGauss(k+1), h = 1/n per direction), M = the global FE mass matrix, Dirichlet
+# rows as identity / zero right-hand side (include/laplace_operator.cuh:33-65,
+# 86-101 is the kappa = 1 operator).
+#   forward  A(kappa) u = Z M f            (Z zeroes the Dirichlet rows)
+#   adjoint  A(kappa) lam = Z dJ/du
+#   dJ/df = M lam,   dJ/dkappa_c = -lam_c^T A_c u_c
+
+
+def _mass_global_1d(k, n):
+    _, mass, _, _ = fe1d(k)
+    N1 = n * k + 1
+    M = np.zeros((N1, N1))
+    for c in range(n):
+        M[c * k:c * k + k + 1, c * k:c * k + k + 1] += mass / n
+    return M
+
+
+def _apply_kron(v, dim, mats):
+    """(mats[dim-1] x ... x mats[0]) v for the lexicographic (x fastest) vector v."""
+    N1 = mats[0].shape[1]
+    w = np.asarray(v, dtype=np.float64).reshape((N1,) * dim)
+    for d in range(dim):
+        ax = dim - 1 - d  # axis of direction d (x is the last axis)
+        w = np.moveaxis(np.tensordot(mats[d], w, axes=([1], [ax])), 0, ax)
+    return w.reshape(-1)
+
+
+def zero_dirichlet(v, dim, N1):
+    w = np.array(v, dtype=np.float64, copy=True).reshape((N1,) * dim)
+    for ax in range(dim):
+        sl = [slice(None)] * dim
+        sl[ax] = 0
+        w[tuple(sl)] = 0.0
+        sl[ax] = -1
+        w[tuple(sl)] = 0.0
+    return w.reshape(-1)
+
+
+def mass_vmult(dim, k, n, f):
+    """Global FE mass matrix times the nodal vector f (all rows)."""
+    M = _mass_global_1d(k, n)
+    return _apply_kron(f, dim, [M] * dim)
+
+
+def _cell_blocks(v, dim, k, n):
+    """Cell-local values: array [c_z, c_y, c_x, i_z, i_y, i_x] (3D; [c_y, c_x,
+    i_y, i_x] in 2D) of v at DoF (c k + i) per direction."""
+    N1 = n * k + 1
+    w = np.asarray(v, dtype=np.float64).reshape((N1,) * dim)
+    idx = np.arange(n)[:, None] * k + np.arange(k + 1)[None, :]  # (n, k+1)
+    if dim == 2:
+        return w[idx[:, None, :, None], idx[None, :, None, :]]  # [cy, cx, iy, ix]
+    return w[idx[:, None, None, :, None, None], idx[None, :, None, None, :, None],
+             idx[None, None, :, None, None, :]]
+
+
+def cell_energy(dim, k, n, u, lam):
+    """e_c = lam_c^T A_c u_c with the unit-coefficient cell stiffness A_c
+    (h^(d-2) times the Kronecker sum of the reference 1D matrices); cells
+    lexicographic (x fastest)."""
+    _, Mr, Lr, _ = fe1d(k)
+    U = _cell_blocks(u, dim, k, n)
+    Lm = _cell_blocks(lam, dim, k, n)
+    h = 1.0 / n
+    if dim == 2:
+        AU = np.einsum("ab,cd,yxbd->yxac", Lr, Mr, U) + np.einsum("ab,cd,yxbd->yxac", Mr, Lr, U)
+        e = np.einsum("yxac,yxac->yx", Lm, AU)
+    else:
+        AU = (np.einsum("ab,cd,ef,zyxbdf->zyxace", Lr, Mr, Mr, U) +
+              np.einsum("ab,cd,ef,zyxbdf->zyxace", Mr, Lr, Mr, U) +
+              np.einsum("ab,cd,ef,zyxbdf->zyxace", Mr, Mr, Lr, U))
+        e = np.einsum("zyxace,zyxace->zyx", Lm, AU)
+    return h ** (dim - 2) * e.reshape(-1)
+
+
+def adjoint_gradients(dim, k, n_coarse, n_levels, kappa, f, u_target, rel_tol=1e-13):
+    """FP64 oracle of the adjoint gradients of J = 0.5 ||u - u_target||^2 with
+    A(kappa) u = Z M f: returns (u, dJ/df, dJ/dkappa).  Both solves are the
+    oracle's MG-CG with the FP64 V-cycle."""
+    n = n_coarse * (1 << (n_levels - 1))
+    N1 = n * k + 1
+    H = Hierarchy(dim, k, n_coarse, n_levels, kappa=kappa)
+    b = zero_dirichlet(mass_vmult(dim, k, n, f), dim, N1)
+    u, _, _ = H.solve_cg(b, precision=0, symmetric=True, rel_tol=rel_tol, max_it=400)
+    g = zero_dirichlet(u - np.asarray(u_target, dtype=np.float64), dim, N1)
+    lam, _, _ = H.solve_cg(g, precision=0, symmetric=True, rel_tol=rel_tol, max_it=400)
+    lam = zero_dirichlet(lam, dim, N1)
+    return u, mass_vmult(dim, k, n, lam), -cell_energy(dim, k, n, u, lam)

@@ -96,3 +96,20 @@ def test_solve_opts_default():
     L.lib().tps_solve_opts_default(ctypes.byref(o))
     assert (o.driver, o.precision, o.symmetric, o.max_iter, o.use_graph) == (0, 1, 1, 100, 1)
     assert o.rel_tol == 1e-10
+
+
+def test_noalloc_entry_rejects_bad_sizes_before_any_device_work():
+    """tps_restrict_add_noalloc validates its arguments on the host first:
+    scratch overflow in 3D, and in 2D fine levels beyond 2^31-1 DoFs per
+    direction or coarse-cell tiles beyond the launch grid's y limit."""
+    lib = L.lib()
+    buf = ctypes.c_double()
+    p = ctypes.addressof(buf)
+    assert lib.tps_restrict_add_noalloc(3, 4, 64, L.TPS_F64, p, p, None) == 1
+    assert b"scratch" in lib.tps_last_error(None)
+    assert lib.tps_restrict_add_noalloc(2, 4, 2_000_000_000, L.TPS_F64, p, p, None) == 1
+    assert b"2^31" in lib.tps_last_error(None)
+    assert lib.tps_restrict_add_noalloc(2, 2, 600_000, L.TPS_F64, p, p, None) == 1
+    assert b"grid" in lib.tps_last_error(None)
+    assert lib.tps_restrict_add_noalloc(4, 2, 4, L.TPS_F64, p, p, None) == 1
+    assert lib.tps_restrict_add_noalloc(3, 2, 4, L.TPS_F64, None, p, None) == 1

@@ -175,3 +175,62 @@ def test_dense_coarse_solve_for_three_cell_mesh(oracle):
     b[np.any((idx == 0) | (idx == N1 - 1), axis=0)] = 0
     x = H.coarse_solve(b)
     assert rel(oracle.laplace_vmult(3, 2, 3, x), b) < 1e-11
+
+
+def test_oracle_adjoint_matches_finite_differences(oracle):
+    """The FP64 oracle adjoint (the reference the GPU adjoint is checked
+    against) agrees with central differences of its own solves (h = 1e-6)."""
+    dim, k, nc, nl = 3, 2, 2, 2
+    n = nc * 2 ** (nl - 1)
+    N1 = n * k + 1
+    rng = np.random.default_rng(21)
+    kap = np.exp(rng.normal(0.0, 0.5, n ** dim))
+    f = rng.standard_normal(N1 ** dim)
+
+    def solve(f_, k_):
+        H = oracle.Hierarchy(dim, k, nc, nl, kappa=k_)
+        b = oracle.zero_dirichlet(oracle.mass_vmult(dim, k, n, f_), dim, N1)
+        return H.solve_cg(b, precision=0, rel_tol=1e-14, max_it=400)[0]
+
+    u0 = solve(f, kap)
+    ut = u0 * (1.0 + 0.3 * rng.standard_normal(N1 ** dim))
+
+    def J(f_, k_):
+        return 0.5 * np.sum((solve(f_, k_) - ut) ** 2)
+
+    _, gf, gk = oracle.adjoint_gradients(dim, k, nc, nl, kap, f, ut, rel_tol=1e-14)
+    h = 1e-6
+    for _ in range(3):
+        df = rng.standard_normal(N1 ** dim)
+        dk = rng.standard_normal(n ** dim) * kap
+        fd_f = (J(f + h * df, kap) - J(f - h * df, kap)) / (2 * h)
+        fd_k = (J(f, kap + h * dk) - J(f, kap - h * dk)) / (2 * h)
+        assert abs(gf @ df - fd_f) <= 1e-6 * abs(fd_f)
+        assert abs(gk @ dk - fd_k) <= 1e-6 * abs(fd_k)
+
+
+@pytest.mark.parametrize("dim,k,n", [(2, 2, 4), (3, 2, 4), (3, 3, 2)])
+def test_oracle_cell_energy_and_mass(oracle, dim, k, n):
+    """Per-cell energies sum to lam^T A u and equal the kappa-indicator
+    operator of the oracle; the mass apply equals the dense Kronecker product
+    of the global 1D mass matrices."""
+    N1 = n * k + 1
+    rng = np.random.default_rng(3)
+    u = oracle.zero_dirichlet(rng.uniform(-1, 1, N1 ** dim), dim, N1)
+    lam = oracle.zero_dirichlet(rng.uniform(-1, 1, N1 ** dim), dim, N1)
+    e = oracle.cell_energy(dim, k, n, u, lam)
+    tot = lam @ oracle.laplace_vmult(dim, k, n, u)
+    assert abs(e.sum() - tot) <= 1e-13 * abs(tot)
+    for c in (0, n ** dim - 1):
+        ind = np.zeros(n ** dim)
+        ind[c] = 1.0
+        assert abs(e[c] - lam @ oracle.laplace_vmult(dim, k, n, u, kappa=ind)) <= 1e-13
+    _, mass, _, _ = oracle.fe1d(k)
+    M1 = np.zeros((N1, N1))
+    for c in range(n):
+        M1[c * k:c * k + k + 1, c * k:c * k + k + 1] += mass / n
+    M = M1
+    for _ in range(dim - 1):
+        M = np.kron(M, M1)
+    f = rng.uniform(-1, 1, N1 ** dim)
+    assert np.abs(M @ f - oracle.mass_vmult(dim, k, n, f)).max() <= 1e-15
