@@ -238,6 +238,8 @@ def launches_per_solve(dim: int, n_levels: int, iterations: int) -> int:
 TRAFFIC_CAPTURES = {
     ("smoother3d_warp_kernel<4,float>", "poisson3d_q4_64"):
         (136.6e6, 167.5e6, "profiles/smoother3d_warp_k4_f32_poisson3d_q4_64.md"),
+    ("smoother3d_pair_kernel<4>", "poisson3d_q4_64"):
+        (135.5e6, 167.5e6, "profiles/smoother3d_pair_k4_f32_poisson3d_q4_64.md"),
 }
 
 
@@ -378,7 +380,7 @@ def run_micro(args):
             P.time_smoother(dtype="fp64" if code == L.TPS_F64 else "fp32", sweeps=2)
             ms = P.time_smoother(dtype="fp64" if code == L.TPS_F64 else "fp32", sweeps=10)
             total, _ = smoother_bytes(dim, k, n, 8 if code == L.TPS_F64 else 4)
-            label = "warp/patch" if ppb[v] == -1 else f"ppb={ppb[v]}"
+            label = {-1: "warp/patch", -2: "2 patches/warp f32x2"}.get(ppb[v], f"ppb={ppb[v]}")
             rows.append({"name": f"Smooth {dtname} {label}", "ms": ms, "dof_per_s": N / (ms * 1e-3),
                          "GBps": total / (ms * 1e-3) / 1e9})
         L.check(L.lib().tps_set_smoother_variant(P.handle, code, lf, 0), P.handle)
@@ -685,8 +687,8 @@ def main():
         L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, 3, ctypes.byref(msw), sp), P.handle)
         L.check(L.lib().tps_time_smoother(P.handle, lf, L.TPS_F32, 20, ctypes.byref(msw), sp), P.handle)
         sweep_ms = msw.value
-        kernel_name = (f"smoother3d_warp_kernel<{k},float>" if P.smoother_variant(lf, "fp32") == 3
-                       else f"smoother3d_kernel<{k},float,TMA>")
+        kernel_name = {3: f"smoother3d_warp_kernel<{k},float>", 4: f"smoother3d_pair_kernel<{k}>"}.get(
+            P.smoother_variant(lf, "fp32"), f"smoother3d_kernel<{k},float,TMA>")
         bytes_sweep, per_colour = smoother_bytes(dim, k, n, 4)
         colours = sum(1 for c in per_colour if c > 0)
         launch_ms = sweep_ms / colours

@@ -20,7 +20,7 @@ STATUS_NAMES = {
 TPS_F64, TPS_F32, TPS_TF32 = 0, 1, 2
 VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32 = 0, 1, 2, 3
 DRIVER_CG, DRIVER_GMRES = 0, 1
-SMOOTHER_VARIANTS = 4  # TPS_SMOOTHER_VARIANTS
+SMOOTHER_VARIANTS = 5  # TPS_SMOOTHER_VARIANTS
 SMOOTHER_FUSED, SMOOTHER_SEPARATE, SMOOTHER_GLOBAL, SMOOTHER_EXACT, SMOOTHER_ADDITIVE = 0, 1, 2, 3, 4
 MAX_HISTORY = 256
 

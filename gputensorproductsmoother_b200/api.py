@@ -106,7 +106,7 @@ class PoissonProblem:
     def autotune(self, dtype: str = "fp32") -> list[int]:
         """Time the 3D smoother's kernel variants on every level and keep the
         fastest; returns the chosen patches per batch per level (-1: the
-        one-warp-per-patch kernel)."""
+        one-warp-per-patch kernel, -2: two patches per warp in packed FP32)."""
         out = (ctypes.c_int * self.n_levels)()
         L.check(L.lib().tps_autotune(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], out),
                 self.handle)
@@ -114,7 +114,8 @@ class PoissonProblem:
 
     def smoother_variants(self, dtype: str = "fp32") -> list[int]:
         """Patches per batch of each compiled 3D smoother variant (index =
-        variant; -1: one warp per patch; 0 in 2D)."""
+        variant; -1: one warp per patch; -2: two patches per warp in packed
+        FP32; 0 in 2D)."""
         out = (ctypes.c_int * L.SMOOTHER_VARIANTS)()
         L.check(L.lib().tps_smoother_variants(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], out),
                 self.handle)

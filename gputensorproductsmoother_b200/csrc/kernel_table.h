@@ -38,8 +38,8 @@ struct SmootherMaps {
 };
 
 // compiled variants of the 3D smoother: patches per CTA batch default, half,
-// quarter, and one warp per patch
-constexpr int kSmootherVariants = 4;
+// quarter, one warp per patch, and two patches per warp (packed FP32)
+constexpr int kSmootherVariants = 5;
 
 struct KernelTable {
   int degree;

@@ -11,6 +11,7 @@
 #include "smoother.cuh"
 #include "smoother3d.cuh"
 #include "smoother3d_gemm.cuh"
+#include "smoother3d_pair.cuh"
 #include "smoother3d_tc.cuh"
 #include "smoother3d_warp.cuh"
 #include "smoother_variants.cuh"
@@ -99,6 +100,8 @@ cudaError_t set_attributes()
   TPS_SET((smoother3d_kernel<K, T, false, sm3_variant_ppb<K, T, 0>()>), (Sm3<K, T, sm3_variant_ppb<K, T, 0>()>::BYTES));
   if constexpr (wp3_enabled<K, T>())
     TPS_SET((smoother3d_warp_kernel<K, T, wp3_warps<K, T>()>), (Wp3<K, T, wp3_warps<K, T>()>::BYTES));
+  if constexpr (sizeof(T) == 4 && pp3_enabled<K>())
+    TPS_SET((smoother3d_pair_kernel<K, pp3_warps<K>()>), (Pp3<K, pp3_warps<K>()>::BYTES));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Vmult>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Residual>), (laplace_smem<2, T>()));
   TPS_SET((laplace3d_stream_kernel<K, T, OpMode::Vmult>), (sizeof(T) * OpStream<K, T>::ELEMS));
@@ -249,13 +252,33 @@ void smoother3d_warp_launch(const Sm3Args &a, const SmootherMaps *maps, void *x,
   }
 }
 
+// one colour with two patches per warp in packed FP32 (TMA views required):
+// a persistent grid of the CTAs resident per SM x SMs, capped by the pair count
+void smoother3d_pair_launch(const Sm3Args &a, const SmootherMaps *maps, void *x, float scale, float fd, int *err,
+                            cudaStream_t s)
+{
+  if constexpr (pp3_enabled<K>()) {
+    constexpr int WA = pp3_warps<K>();
+    using S = Pp3<K, WA>;
+    static_assert(S::BYTES + 1024 <= 233472, "pair smoother: one CTA must fit an SM");
+    static const Residency r = residency(smoother3d_pair_kernel<K, WA>, S::NT, S::BYTES);
+    const int need = static_cast<int>(ceil_div(ceil_div(a.n_patches, 2), WA));
+    const int grid = need < r.per_sm * r.n_sm ? need : r.per_sm * r.n_sm;
+    TPS_LAUNCH((smoother3d_pair_kernel<K, WA>), grid, S::NT, S::BYTES, s,
+        *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),
+        static_cast<float *>(x), a, scale, fd, err);
+  }
+}
+
 // patches per batch of a 3D variant (0 in 2D: one fixed kernel shape; -1:
-// the one-warp-per-patch kernel, variant 3, where it is compiled)
+// the one-warp-per-patch kernel, variant 3, -2: two patches per warp in
+// packed FP32, variant 4, where they are compiled)
 int smoother_ppb(int dim, int dtype, int variant)
 {
   if (dim != 3) return 0;
   auto pick = [&](auto tag) -> int {
     using T = decltype(tag);
+    if (variant == 4) return (sizeof(T) == 4 && pp3_enabled<K>()) ? -2 : sm3_variant_ppb<K, T, 0>();
     if (variant == 3) return wp3_enabled<K, T>() ? -1 : sm3_variant_ppb<K, T, 0>();
     return variant == 1 ? sm3_variant_ppb<K, T, 1>() : variant == 2 ? sm3_variant_ppb<K, T, 2>()
                                                                         : sm3_variant_ppb<K, T, 0>();
@@ -294,7 +317,11 @@ cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const voi
     magic_div(static_cast<uint32_t>(nx), a.mx, a.sx);
     magic_div(static_cast<uint32_t>(nx) * static_cast<uint32_t>(ny), a.mxy, a.sxy);
     const T scale = static_cast<T>(sc), fd = static_cast<T>(omega / sc);
-    if (variant == 3 && wp3_enabled<K, T>() && maps && maps->valid)
+    bool pair = false;
+    if constexpr (sizeof(T) == 4) pair = variant == 4 && pp3_enabled<K>() && maps && maps->valid;
+    if (pair)
+      smoother3d_pair_launch(a, maps, x, static_cast<float>(scale), static_cast<float>(fd), err, s);
+    else if (variant == 3 && wp3_enabled<K, T>() && maps && maps->valid)
       smoother3d_warp_launch<T>(a, maps, x, scale, fd, err, s);
     else if (variant == 1)
       smoother3d_launch<T, sm3_variant_ppb<K, T, 1>()>(a, maps, x, b, scale, fd, err, s);

@@ -122,6 +122,9 @@ __device__ __forceinline__ void fold_rows2(const typename Pair<T>::type *fp, con
 
 // The same rows with scalar FMAs: every coefficient is a constant-bank
 // operand of its FMA (the packed pairs above need a constant load per pair).
+// Every chain starts with a product and continues with explicit fused
+// multiply-adds in a fixed order, so the rounding does not depend on which
+// product the compiler would fuse (the packed-pair kernel repeats it exactly).
 template <int K, typename T>
 __device__ __forceinline__ void fold_rows_s(const T *fe, const T *fo, const typename Pair<T>::type (&eo)[K > 1 ? K : 1],
                                             const T ec, T (&out)[2 * K - 1])
@@ -129,18 +132,19 @@ __device__ __forceinline__ void fold_rows_s(const T *fe, const T *fo, const type
   constexpr int M = 2 * K - 1;
 #pragma unroll
   for (int r = 0; r < K - 1; ++r) {
-    T e = fe[r * (K + 1) + K] * ec, o = T(0);
+    T e = fe[r * (K + 1) + K] * ec, o = fo[r * K] * eo[0].y;
+    e = fmadd(fe[r * (K + 1)], eo[0].x, e);
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-      e += fe[r * (K + 1) + j] * eo[j].x;
-      o += fo[r * K + j] * eo[j].y;
+    for (int j = 1; j < K; ++j) {
+      e = fmadd(fe[r * (K + 1) + j], eo[j].x, e);
+      o = fmadd(fo[r * K + j], eo[j].y, o);
     }
-    out[r] = e + o;
-    out[M - 1 - r] = e - o;
+    out[r] = add_rn(e, o);
+    out[M - 1 - r] = sub_rn(e, o);
   }
   T sc = fe[(K - 1) * (K + 1) + K] * ec;
 #pragma unroll
-  for (int j = 0; j < K; ++j) sc += fe[(K - 1) * (K + 1) + j] * eo[j].x;
+  for (int j = 0; j < K; ++j) sc = fmadd(fe[(K - 1) * (K + 1) + j], eo[j].x, sc);
   out[K - 1] = sc;
 }
 
@@ -157,24 +161,27 @@ __device__ __forceinline__ void fold_rows_sum_s(const T *fea, const T *foa,
   constexpr int M = 2 * K - 1;
 #pragma unroll
   for (int r = 0; r < K - 1; ++r) {
-    T e = fea[r * (K + 1) + K] * eca, o = T(0);
-    e += feb[r * (K + 1) + K] * ecb;
+    T e = fea[r * (K + 1) + K] * eca, o = foa[r * K] * eoa[0].y;
+    e = fmadd(feb[r * (K + 1) + K], ecb, e);
+    e = fmadd(fea[r * (K + 1)], eoa[0].x, e);
+    e = fmadd(feb[r * (K + 1)], eob[0].x, e);
+    o = fmadd(fob[r * K], eob[0].y, o);
 #pragma unroll
-    for (int j = 0; j < K; ++j) {
-      e += fea[r * (K + 1) + j] * eoa[j].x;
-      o += foa[r * K + j] * eoa[j].y;
-      e += feb[r * (K + 1) + j] * eob[j].x;
-      o += fob[r * K + j] * eob[j].y;
+    for (int j = 1; j < K; ++j) {
+      e = fmadd(fea[r * (K + 1) + j], eoa[j].x, e);
+      o = fmadd(foa[r * K + j], eoa[j].y, o);
+      e = fmadd(feb[r * (K + 1) + j], eob[j].x, e);
+      o = fmadd(fob[r * K + j], eob[j].y, o);
     }
-    out[r] = e + o;
-    out[M - 1 - r] = e - o;
+    out[r] = add_rn(e, o);
+    out[M - 1 - r] = sub_rn(e, o);
   }
   T sc = fea[(K - 1) * (K + 1) + K] * eca;
-  sc += feb[(K - 1) * (K + 1) + K] * ecb;
+  sc = fmadd(feb[(K - 1) * (K + 1) + K], ecb, sc);
 #pragma unroll
   for (int j = 0; j < K; ++j) {
-    sc += fea[(K - 1) * (K + 1) + j] * eoa[j].x;
-    sc += feb[(K - 1) * (K + 1) + j] * eob[j].x;
+    sc = fmadd(fea[(K - 1) * (K + 1) + j], eoa[j].x, sc);
+    sc = fmadd(feb[(K - 1) * (K + 1) + j], eob[j].x, sc);
   }
   out[K - 1] = sc;
 }
@@ -263,7 +270,10 @@ constexpr int sm3_variant_ppb()
   else return P;
 }
 
-// S or S^T with scalar FMAs (constant-bank coefficients)
+// S or S^T with scalar FMAs (constant-bank coefficients); chains as in
+// fold_rows_s: a product, then explicit fused multiply-adds in a fixed order;
+// the even/odd combinations are unfusable adds (a chain of one product, at
+// degree 2, would otherwise be fused into them)
 template <int K, typename T, bool TRANSPOSE>
 __device__ __forceinline__ void apply_evec_s(const T (&in)[2 * K - 1], T (&out)[2 * K - 1])
 {
@@ -279,34 +289,36 @@ __device__ __forceinline__ void apply_evec_s(const T (&in)[2 * K - 1], T (&out)[
     const T ec = in[C];
 #pragma unroll
     for (int q = 0; q < C; ++q) {
-      T e = tb.evec[C * M + q] * ec, o = T(0);
+      T e = tb.evec[C * M + q] * ec, o = tb.evec[C + 1 + q] * od[0];
+      e = fmadd(tb.evec[q], ev[0], e);
 #pragma unroll
-      for (int j = 0; j < C; ++j) {
-        e += tb.evec[j * M + q] * ev[j];
-        o += tb.evec[j * M + C + 1 + q] * od[j];
+      for (int j = 1; j < C; ++j) {
+        e = fmadd(tb.evec[j * M + q], ev[j], e);
+        o = fmadd(tb.evec[j * M + C + 1 + q], od[j], o);
       }
       out[q] = e;
       out[C + 1 + q] = o;
     }
     T sc = tb.evec[C * M + C] * ec;
 #pragma unroll
-    for (int j = 0; j < C; ++j) sc += tb.evec[j * M + C] * ev[j];
+    for (int j = 0; j < C; ++j) sc = fmadd(tb.evec[j * M + C], ev[j], sc);
     out[C] = sc;
   } else {
 #pragma unroll
     for (int i = 0; i < C; ++i) {
-      T e = tb.evec[i * M + C] * in[C], o = T(0);
+      T e = tb.evec[i * M + C] * in[C], o = tb.evec[i * M + C + 1] * in[C + 1];
+      e = fmadd(tb.evec[i * M], in[0], e);
 #pragma unroll
-      for (int q = 0; q < C; ++q) {
-        e += tb.evec[i * M + q] * in[q];
-        o += tb.evec[i * M + C + 1 + q] * in[C + 1 + q];
+      for (int q = 1; q < C; ++q) {
+        e = fmadd(tb.evec[i * M + q], in[q], e);
+        o = fmadd(tb.evec[i * M + C + 1 + q], in[C + 1 + q], o);
       }
-      out[i] = e + o;
-      out[M - 1 - i] = e - o;
+      out[i] = add_rn(e, o);
+      out[M - 1 - i] = sub_rn(e, o);
     }
-    T sc = T(0);
+    T sc = tb.evec[C * M] * in[0];
 #pragma unroll
-    for (int q = 0; q <= C; ++q) sc += tb.evec[C * M + q] * in[q];
+    for (int q = 1; q <= C; ++q) sc = fmadd(tb.evec[C * M + q], in[q], sc);
     out[C] = sc;
   }
 }
@@ -571,8 +583,8 @@ __global__ void __launch_bounds__(Sm3<K, T, PPB_>::NT)
             T *d1 = Z1 + lp * S::ZSZ + y * N1 + xx, *d2 = Z2 + lp * S::ZSZ + y * N1 + xx;
 #pragma unroll
             for (int i = 0; i < M; ++i) {
-              d1[i * N1 * N1] = tb.pmass[(i + 1) * N1] * v0 + tb.pmass[(i + 1) * N1 + N1 - 1] * vn;
-              d2[i * N1 * N1] = tb.plap[(i + 1) * N1] * v0 + tb.plap[(i + 1) * N1 + N1 - 1] * vn;
+              d1[i * N1 * N1] = fmadd(tb.pmass[(i + 1) * N1 + N1 - 1], vn, tb.pmass[(i + 1) * N1] * v0);
+              d2[i * N1 * N1] = fmadd(tb.plap[(i + 1) * N1 + N1 - 1], vn, tb.plap[(i + 1) * N1] * v0);
             }
           }
         }

@@ -1,0 +1,650 @@
+// 3D fused vertex-patch smoother, FP32, two patches per warp in packed
+// FP32x2 arithmetic (sm_100a).
+//
+// Same per-patch algebra, contraction order and rounding as
+// smoother3d_warp_kernel and smoother3d_kernel (the reference's FUSED_CF
+// patch kernel, include/loop_kernel.cuh:962-1060 with
+// include/evaluate_kernel.cuh:501-590, 1327-1434, 2058-2163): box residual
+// b - A x~ with the interior of x set to zero, then the fast-diagonalisation
+// solve and the store of omega A_II^{-1} r_I.  Every value of the staged
+// intermediates is a pair (patch A, patch B), every multiply-add is one
+// fma.rn.f32x2 over the pair with the coefficient in both halves, so each
+// patch sees exactly the scalar kernels' operations: the sweeps are
+// bit-identical (up to the sign of zero results).
+//
+// Why pairs: the one-warp-per-patch kernel is bound by instruction issue
+// (about 1,700 warp instructions per Q4 patch, the shared-memory pipe 68 %
+// busy).  Here one instruction serves two patches for the arithmetic, the
+// shared-memory traffic of the intermediates (64-bit accesses), the address
+// arithmetic and the loop/TMA skeleton; only the raw box and b-slab reads
+// and the global stores stay per patch.
+//
+// Execution model as in smoother3d_warp_kernel: every warp owns its pairs of
+// patches (patches 2q and 2q+1 of the colour, q = pair index), its stage and
+// its mbarrier; stages are separated by __syncwarp only; the next pair's two
+// x boxes and two b slabs are fetched by TMA (4 copies on one mbarrier) as
+// soon as the x stage has consumed the current ones.  An odd last patch is
+// paired with itself and stored once.  Every wait is bounded.
+//
+// Shared memory (8-byte pair elements): the z- and y-stage outputs Z and V
+// are stored task-major for the stage that reads them (conflict-free
+// consecutive reads), with strides and, at degree 4, a z-stage lane
+// assignment chosen so that the writes are conflict-free as well; the four
+// fast-diagonalisation arrays use the 8-byte layouts WpLayout<K, 8>.  Every
+// stage runs its passes as straight-line code: lanes past the last task redo
+// a valid task and skip the stores, so the loads of one pass can be issued
+// while the previous pass computes (lanes past the last task take task
+// lane mod the task count, which is a valid task at every degree).
+#pragma once
+
+#include <cuda.h>
+
+#include "ptx.cuh"
+#include "smoother3d.cuh"
+#include "smoother3d_warp.cuh"
+#include "tps_common.cuh"
+
+namespace tps {
+
+// ---- packed pair arithmetic (patch A in .x, patch B in .y) -------------------
+__device__ __forceinline__ float2 pr_bc(float c) { return make_float2(c, c); }
+__device__ __forceinline__ float2 pr_add(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 pr_sub(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 pr_mul(float c, float2 a) { return __fmul2_rn(pr_bc(c), a); }
+__device__ __forceinline__ float2 pr_fma(float c, float2 a, float2 acc) { return __ffma2_rn(pr_bc(c), a, acc); }
+
+// v (2k+1 pairs) -> even sums E_j, odd differences O_j (j < k), centre ec
+template <int K>
+__device__ __forceinline__ void pr_fold(const float2 (&v)[2 * K + 1], float2 (&E)[K], float2 (&O)[K], float2 &ec)
+{
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    E[j] = pr_add(v[j], v[2 * K - j]);
+    O[j] = pr_sub(v[j], v[2 * K - j]);
+  }
+  ec = v[K];
+}
+
+// interior rows of one centro-symmetric patch matrix (fold_rows_s, the same
+// chains and order)
+template <int K>
+__device__ __forceinline__ void pr_rows(const float *fe, const float *fo, const float2 (&E)[K], const float2 (&O)[K],
+                                        const float2 ec, float2 (&out)[2 * K - 1])
+{
+  constexpr int M = 2 * K - 1;
+#pragma unroll
+  for (int r = 0; r < K - 1; ++r) {
+    float2 e = pr_mul(fe[r * (K + 1) + K], ec), o = pr_mul(fo[r * K], O[0]);
+    e = pr_fma(fe[r * (K + 1)], E[0], e);
+#pragma unroll
+    for (int j = 1; j < K; ++j) {
+      e = pr_fma(fe[r * (K + 1) + j], E[j], e);
+      o = pr_fma(fo[r * K + j], O[j], o);
+    }
+    out[r] = pr_add(e, o);
+    out[M - 1 - r] = pr_sub(e, o);
+  }
+  float2 sc = pr_mul(fe[(K - 1) * (K + 1) + K], ec);
+#pragma unroll
+  for (int j = 0; j < K; ++j) sc = pr_fma(fe[(K - 1) * (K + 1) + j], E[j], sc);
+  out[K - 1] = sc;
+}
+
+// interior rows of A u + B v with one accumulation chain (fold_rows_sum_s)
+template <int K>
+__device__ __forceinline__ void pr_rows_sum(const float *fea, const float *foa, const float2 (&Ea)[K],
+                                            const float2 (&Oa)[K], const float2 eca, const float *feb,
+                                            const float *fob, const float2 (&Eb)[K], const float2 (&Ob)[K],
+                                            const float2 ecb, float2 (&out)[2 * K - 1])
+{
+  constexpr int M = 2 * K - 1;
+#pragma unroll
+  for (int r = 0; r < K - 1; ++r) {
+    float2 e = pr_mul(fea[r * (K + 1) + K], eca), o = pr_mul(foa[r * K], Oa[0]);
+    e = pr_fma(feb[r * (K + 1) + K], ecb, e);
+    e = pr_fma(fea[r * (K + 1)], Ea[0], e);
+    e = pr_fma(feb[r * (K + 1)], Eb[0], e);
+    o = pr_fma(fob[r * K], Ob[0], o);
+#pragma unroll
+    for (int j = 1; j < K; ++j) {
+      e = pr_fma(fea[r * (K + 1) + j], Ea[j], e);
+      o = pr_fma(foa[r * K + j], Oa[j], o);
+      e = pr_fma(feb[r * (K + 1) + j], Eb[j], e);
+      o = pr_fma(fob[r * K + j], Ob[j], o);
+    }
+    out[r] = pr_add(e, o);
+    out[M - 1 - r] = pr_sub(e, o);
+  }
+  float2 sc = pr_mul(fea[(K - 1) * (K + 1) + K], eca);
+  sc = pr_fma(feb[(K - 1) * (K + 1) + K], ecb, sc);
+#pragma unroll
+  for (int j = 0; j < K; ++j) {
+    sc = pr_fma(fea[(K - 1) * (K + 1) + j], Ea[j], sc);
+    sc = pr_fma(feb[(K - 1) * (K + 1) + j], Eb[j], sc);
+  }
+  out[K - 1] = sc;
+}
+
+// S or S^T on a line of 2k-1 pairs (apply_evec_s, the same chains and order)
+template <int K, bool TRANSPOSE>
+__device__ __forceinline__ void pr_evec(const float2 (&in)[2 * K - 1], float2 (&out)[2 * K - 1])
+{
+  constexpr int M = 2 * K - 1, C = K - 1;
+  const DegreeTables<K, float> &tb = c_tables<K, float>;
+  if constexpr (TRANSPOSE) {
+    float2 ev[C > 0 ? C : 1], od[C > 0 ? C : 1];
+#pragma unroll
+    for (int j = 0; j < C; ++j) {
+      ev[j] = pr_add(in[j], in[M - 1 - j]);
+      od[j] = pr_sub(in[j], in[M - 1 - j]);
+    }
+    const float2 ec = in[C];
+#pragma unroll
+    for (int q = 0; q < C; ++q) {
+      float2 e = pr_mul(tb.evec[C * M + q], ec), o = pr_mul(tb.evec[C + 1 + q], od[0]);
+      e = pr_fma(tb.evec[q], ev[0], e);
+#pragma unroll
+      for (int j = 1; j < C; ++j) {
+        e = pr_fma(tb.evec[j * M + q], ev[j], e);
+        o = pr_fma(tb.evec[j * M + C + 1 + q], od[j], o);
+      }
+      out[q] = e;
+      out[C + 1 + q] = o;
+    }
+    float2 sc = pr_mul(tb.evec[C * M + C], ec);
+#pragma unroll
+    for (int j = 0; j < C; ++j) sc = pr_fma(tb.evec[j * M + C], ev[j], sc);
+    out[C] = sc;
+  } else {
+#pragma unroll
+    for (int i = 0; i < C; ++i) {
+      float2 e = pr_mul(tb.evec[i * M + C], in[C]), o = pr_mul(tb.evec[i * M + C + 1], in[C + 1]);
+      e = pr_fma(tb.evec[i * M], in[0], e);
+#pragma unroll
+      for (int q = 1; q < C; ++q) {
+        e = pr_fma(tb.evec[i * M + q], in[q], e);
+        o = pr_fma(tb.evec[i * M + C + 1 + q], in[C + 1 + q], o);
+      }
+      out[i] = pr_add(e, o);
+      out[M - 1 - i] = pr_sub(e, o);
+    }
+    float2 sc = pr_mul(tb.evec[C * M], in[0]);
+#pragma unroll
+    for (int q = 1; q <= C; ++q) sc = pr_fma(tb.evec[C * M + q], in[q], sc);
+    out[C] = sc;
+  }
+}
+
+// degrees with a compiled pair kernel (FP32; the scalar folded contractions
+// of degrees <= 5 are the ones it mirrors)
+template <int K>
+constexpr bool pp3_enabled()
+{
+  return K >= 2 && K <= 5;
+}
+
+template <int K, int WARPS>
+struct Pp3 {
+  using L = WpLayout<K, 8>;  // strides of the 8-byte pair elements
+  static constexpr int N1 = 2 * K + 1, M = 2 * K - 1;
+  static constexpr int A = Sm3<K, float>::A, W = Sm3<K, float>::W;  // TMA boxes as the FP32 kernels'
+  static constexpr int XBOX = N1 * N1 * W, BBOX = M * M * W;        // floats per patch
+  static constexpr int ALIGN = 32;                                   // floats (128 B: TMA destinations)
+  static constexpr int XBOX_A = wp_rup(XBOX, ALIGN), BBOX_A = wp_rup(BBOX, ALIGN);
+  // Z [zi][y][x] = M_z / L_z x~ and V [zi][yi][x] in "task-major" layouts:
+  // the next stage's task t (its line) is the fastest index, so its reads of
+  // element q are the consecutive words t + q * stride (conflict-free); the
+  // strides ZY (y of Z) and M * M (x of V) were chosen by a bank-conflict
+  // search over the writing stage's lane mappings
+  static constexpr int ZY = K == 2 ? 15 : K == 3 ? 36 : K == 4 ? 63 : 108;
+  static constexpr Str3 ZL{1, ZY, M}, VL{M, 1, M * M};  // {zi, y or yi, x} strides
+  static constexpr int ZEXT = (M - 1) * ZL.p + (N1 - 1) * ZL.r + (N1 - 1) * ZL.c + 1;
+  static constexpr int VEXT = (M - 1) * VL.p + (M - 1) * VL.r + (N1 - 1) * VL.c + 1;
+  static constexpr int NZP = (N1 * N1 - M * M + (M * M + 1) / 2 + 31) / 32;  // passes of the z stage
+  static constexpr int ext(Str3 s) { return (M - 1) * (s.p + s.r + s.c) + 1; }
+  static constexpr int QBUF1 = wp_max(ext(L::QA), ext(L::QC)), QBUF2 = wp_max(ext(L::QB), ext(L::QD));
+  // per warp (floats): [x box A | x box B, later V1 | V2] [b slab A | b slab B]
+  // [Z1 | Z2, later QA/QC | QB/QD]; pair arrays take 2 floats per element
+  static constexpr int BOFF = wp_rup(wp_max(2 * XBOX_A, 4 * VEXT), ALIGN);
+  static constexpr int ZOFF = BOFF + 2 * BBOX_A;
+  static constexpr int WARP_ELEMS = wp_rup(ZOFF + wp_max(4 * ZEXT, 2 * (QBUF1 + QBUF2)), ALIGN);
+  static constexpr int QSZ = M * M * M;
+  static constexpr int NT = 32 * WARPS;
+  static constexpr size_t OFF_RL = sizeof(float) * static_cast<size_t>(WARPS) * WARP_ELEMS;
+  static constexpr size_t OFF_BAR = (OFF_RL + sizeof(float) * QSZ + 7) / 8 * 8;
+  static constexpr size_t BYTES = OFF_BAR + 8 * WARPS;
+  static constexpr size_t bytes_for(int w)
+  {
+    return (sizeof(float) * (static_cast<size_t>(w) * WARP_ELEMS + QSZ) + 7) / 8 * 8 + 8 * static_cast<size_t>(w);
+  }
+  static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
+  static constexpr int NZT = RING + IPAIR, NYT = M * N1, NQT = M * M;
+};
+
+// Lane assignment of the z stage at degree 4 (positions y * 9 + x of the box
+// face, 255: idle): pass 0 the 32 ring lines, pass 1 two interior lines per
+// lane.  With the Z layout above (y stride 63, x stride 7, 8-byte words) every
+// half-warp's 16 stores of one instruction fall on 16 distinct bank pairs;
+// the assignment was found by a greedy search over the lines' residues
+// (y * 63 + 7 x) mod 16.
+static __device__ const unsigned char kPairRing4[32] = {0,  7,  78, 5,  76, 3,  74, 1,  8,  79, 6,  77, 4,  75, 2,  73,
+                                          80, 71, 62, 53, 44, 35, 26, 17, 72, 63, 54, 45, 36, 27, 18, 9};
+static __device__ const unsigned char kPairIn4[2][32] = {
+    {16, 10, 11, 12, 13, 14, 15, 19, 20, 21, 22, 23, 24, 25, 33, 34,
+     48, 58, 59, 61, 47, 68, 70, 56, 65, 255, 255, 255, 255, 255, 255, 255},
+    {32, 42, 43, 28, 29, 30, 31, 51, 52, 37, 38, 39, 40, 41, 49, 50,
+     64, 60, 46, 67, 69, 55, 57, 66, 255, 255, 255, 255, 255, 255, 255, 255}};
+
+// z-stage task of a lane in one pass: ring = one full z-line, else up to
+// two interior z-lines (their x box rows read at z = 0 and z = N1-1 only);
+// positions y * N1 + x, -1 = none
+struct PairZTask {
+  int ring, in0, in1;
+};
+
+template <int K>
+__device__ __forceinline__ PairZTask pair_ztask(int lane, int p)
+{
+  constexpr int N1 = 2 * K + 1, M = 2 * K - 1, RING = N1 * N1 - M * M, NZT = RING + (M * M + 1) / 2;
+  PairZTask r{-1, -1, -1};
+  if constexpr (K == 4) {
+    if (p == 0) {
+      r.ring = kPairRing4[lane];
+    } else {
+      const int a = kPairIn4[0][lane], b = kPairIn4[1][lane];
+      r.in0 = a == 255 ? -1 : a;
+      r.in1 = b == 255 ? -1 : b;
+    }
+  } else {
+    const int t = lane + 32 * p;
+    if (t < RING) {
+      int y, xx;
+      if (t < N1) {
+        y = 0;
+        xx = t;
+      } else if (t < 2 * N1) {
+        y = N1 - 1;
+        xx = t - N1;
+      } else {
+        const int q = t - 2 * N1;
+        y = 1 + (q >> 1);
+        xx = (q & 1) ? N1 - 1 : 0;
+      }
+      r.ring = y * N1 + xx;
+    } else if (t < NZT) {
+      const int r0 = 2 * (t - RING);
+      r.in0 = (1 + r0 / M) * N1 + 1 + r0 % M;
+      if (r0 + 1 < M * M) r.in1 = (1 + (r0 + 1) / M) * N1 + 1 + (r0 + 1) % M;
+    }
+  }
+  return r;
+}
+
+// warps per CTA with the most warps per SM (228 KB, 1 KB reserved per CTA),
+// at most 16 warps per SM so that a thread keeps 128 registers (the pair
+// contractions hold about 120 live values at degree 4)
+constexpr int kPairMaxWarpsPerSm = 16;
+template <int K>
+constexpr int pp3_ctas_for(int w)
+{
+  int ctas = static_cast<int>(233472 / (Pp3<K, 1>::bytes_for(w) + 1024));  // 0: does not fit
+  if (ctas * w > kPairMaxWarpsPerSm) ctas = kPairMaxWarpsPerSm / w;
+  return ctas > 32 ? 32 : ctas;
+}
+template <int K>
+constexpr int pp3_warps()
+{
+  int best = 1, best_w = 0;
+  for (int w = 1; w <= 8; ++w) {
+    const int ctas = pp3_ctas_for<K>(w);
+    if (ctas * w > best_w) {
+      best_w = ctas * w;
+      best = w;
+    }
+  }
+  return best;
+}
+
+template <int K>
+constexpr int pp3_ctas()
+{
+  const int c = pp3_ctas_for<K>(pp3_warps<K>());
+  return c < 1 ? 1 : c;
+}
+
+template <int K, int WARPS>
+__global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
+    smoother3d_pair_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
+                           float *__restrict__ x, const Sm3Args a, float scale, float fd_scale,
+                           int *__restrict__ err)
+{
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
+  using S = Pp3<K, WARPS>;
+  using Lo = typename S::L;
+  constexpr int N1 = S::N1, M = S::M, W = S::W, AL = S::A;
+  constexpr Str3 QA = Lo::QA, QB = Lo::QB, QC = Lo::QC, QD = Lo::QD;
+  const DegreeTables<K, float> &tb = c_tables<K, float>;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  float *RL = reinterpret_cast<float *>(smem_raw + S::OFF_RL);
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + S::OFF_BAR) + wid;
+  float *stage = reinterpret_cast<float *>(smem_raw) + static_cast<size_t>(wid) * S::WARP_ELEMS;
+  float2 *Z1 = reinterpret_cast<float2 *>(stage + S::ZOFF), *Z2 = Z1 + S::ZEXT;
+  float2 *V1 = reinterpret_cast<float2 *>(stage), *V2 = V1 + S::VEXT;
+  float2 *QAb = Z1, *QBb = Z1 + S::QBUF1;  // QA and QC share one buffer, QB and QD the other
+  const float *boxA = stage, *boxB = stage + S::XBOX_A;
+  const float *bslA = stage + S::BOFF, *bslB = bslA + S::BBOX_A;
+
+  for (int e = tid; e < S::QSZ; e += S::NT)
+    RL[e] = fd_scale / (tb.eval[e % M] + tb.eval[(e / M) % M] + tb.eval[e / (M * M)]);
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();  // the only CTA-wide barrier: RL and the mbarriers are ready
+  // this lane's eigenvalue scalings of the z stage of the solve (tasks t and
+  // t + 32, modes 0..M-1), kept in registers
+  float rl[(S::NQT + 31) / 32][M];
+#pragma unroll
+  for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
+    const int t = lane + 32 * p < S::NQT ? lane + 32 * p : lane % S::NQT;
+#pragma unroll
+    for (int jj = 0; jj < M; ++jj) rl[p][jj] = RL[jj * M * M + t];
+  }
+
+  const int n_pairs = (a.n_patches + 1) >> 1;
+  const int G = gridDim.x * WARPS;
+  int q = blockIdx.x * WARPS + wid;
+  // lane 0: both x boxes and b slabs of the pair with box origins (fA, fB)
+  auto issue = [&](int fxa, int fya, int fza, int fxb, int fyb, int fzb) {
+    mbar_arrive_expect_tx(bar, static_cast<uint32_t>(sizeof(float) * 2 * (S::BBOX + (a.zero_x ? 0 : S::XBOX))));
+    if (!a.zero_x) {
+      tma_load_3d(stage, &map_x, bar, fxa & ~(AL - 1), fya, fza);
+      tma_load_3d(stage + S::XBOX_A, &map_x, bar, fxb & ~(AL - 1), fyb, fzb);
+    }
+    tma_load_3d(stage + S::BOFF, &map_b, bar, fxa & ~(AL - 1), fya + 1, fza + 1);
+    tma_load_3d(stage + S::BOFF + S::BBOX_A, &map_b, bar, fxb & ~(AL - 1), fyb + 1, fzb + 1);
+  };
+  // pair q -> box origins of patches 2q and 2q+1 (the last patch twice for an odd count)
+  auto pair_xyz = [&](int qq, int &fxa, int &fya, int &fza, int &fxb, int &fyb, int &fzb) {
+    const int ja = 2 * qq, jb = ja + 1 < a.n_patches ? ja + 1 : ja;
+    wp_patch_xyz(a, ja, K, fxa, fya, fza);
+    wp_patch_xyz(a, jb, K, fxb, fyb, fzb);
+  };
+  PairZTask ztk[S::NZP];  // this lane's z-stage lines, per pass
+#pragma unroll
+  for (int p = 0; p < S::NZP; ++p) ztk[p] = pair_ztask<K>(lane, p);
+  int fxa = 0, fya = 0, fza = 0, fxb = 0, fyb = 0, fzb = 0;
+  if (q < n_pairs) {
+    pair_xyz(q, fxa, fya, fza, fxb, fyb, fzb);
+    if (lane == 0) issue(fxa, fya, fza, fxb, fyb, fzb);
+  }
+
+  for (int it = 0; q < n_pairs; q += G, ++it) {
+    const int xoa = fxa & (AL - 1), xob = fxb & (AL - 1);
+    const bool store_b = 2 * q + 1 < a.n_patches;
+    int nxa = 0, nya = 0, nza = 0, nxb = 0, nyb = 0, nzb = 0;  // the next pair of this warp
+    if (q + G < n_pairs) pair_xyz(q + G, nxa, nya, nza, nxb, nyb, nzb);
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, it & 1))) {
+      if (lane == 0) atomicExch(err, 1);
+      return;  // the only copies in flight were the ones waited for
+    }
+
+    if (!a.zero_x) {
+      // ---- z: Z1 = M_z x~, Z2 = L_z x~ (ring lines, then interior lines) ----
+      const float *ba = boxA + xoa, *bb = boxB + xob;
+#pragma unroll
+      for (int p = 0; p < S::NZP; ++p) {
+        const PairZTask tk = ztk[p];
+        if (tk.ring >= 0) {
+          const int y = tk.ring / N1, xx = tk.ring % N1;
+          const int o = y * W + xx;
+          float2 v[N1], E[K], O[K], ec, r1[M], r2[M];
+#pragma unroll
+          for (int z = 0; z < N1; ++z) v[z] = make_float2(ba[o + z * N1 * W], bb[o + z * N1 * W]);
+          pr_fold<K>(v, E, O, ec);
+          pr_rows<K>(tb.pmass_fe, tb.pmass_fo, E, O, ec, r1);
+          pr_rows<K>(tb.plap_fe, tb.plap_fo, E, O, ec, r2);
+          float2 *d1 = Z1 + y * S::ZL.r + xx * S::ZL.c, *d2 = Z2 + y * S::ZL.r + xx * S::ZL.c;
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            d1[i * S::ZL.p] = r1[i];
+            d2[i * S::ZL.p] = r2[i];
+          }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const int pos = h == 0 ? tk.in0 : tk.in1;
+          if (pos >= 0) {
+            const int y = pos / N1, xx = pos % N1;
+            const int o = y * W + xx;
+            const float2 v0 = make_float2(ba[o], bb[o]);
+            const float2 vn = make_float2(ba[o + (N1 - 1) * N1 * W], bb[o + (N1 - 1) * N1 * W]);
+            float2 *d1 = Z1 + y * S::ZL.r + xx * S::ZL.c, *d2 = Z2 + y * S::ZL.r + xx * S::ZL.c;
+#pragma unroll
+            for (int i = 0; i < M; ++i) {
+              d1[i * S::ZL.p] = pr_fma(tb.pmass[(i + 1) * N1 + N1 - 1], vn, pr_mul(tb.pmass[(i + 1) * N1], v0));
+              d2[i * S::ZL.p] = pr_fma(tb.plap[(i + 1) * N1 + N1 - 1], vn, pr_mul(tb.plap[(i + 1) * N1], v0));
+            }
+          }
+        }
+      }
+      __syncwarp();
+      // ---- y: V1 = M_y Z2 + L_y Z1, V2 = M_y Z1 (V overwrites the dead x boxes) ----
+      // task t = (zi, xx) = (t % M, t / M); lanes past the last task redo a
+      // valid task (lane mod the task count) and skip the stores, so every pass
+      // is straight-line code
+#pragma unroll
+      for (int p = 0; p < (S::NYT + 31) / 32; ++p) {
+        const int t0 = lane + 32 * p;
+        const bool act = t0 < S::NYT;
+        const int t = act ? t0 : lane % S::NYT;
+        const int zi = t % M, xx = t / M;
+        const float2 *s1 = Z1 + t, *s2 = Z2 + t;  // = zi * ZL.p + xx * ZL.c
+        float2 v[N1], E1[K], O1[K], ec1, E2[K], O2[K], ec2;
+#pragma unroll
+        for (int qq = 0; qq < N1; ++qq) v[qq] = s1[qq * S::ZL.r];
+        pr_fold<K>(v, E1, O1, ec1);
+#pragma unroll
+        for (int qq = 0; qq < N1; ++qq) v[qq] = s2[qq * S::ZL.r];
+        pr_fold<K>(v, E2, O2, ec2);
+        float2 ra[M], rc[M];
+        pr_rows_sum<K>(tb.pmass_fe, tb.pmass_fo, E2, O2, ec2, tb.plap_fe, tb.plap_fo, E1, O1, ec1, ra);
+        pr_rows<K>(tb.pmass_fe, tb.pmass_fo, E1, O1, ec1, rc);
+        if (act) {
+          float2 *d1 = V1 + zi * S::VL.p + xx * S::VL.c, *d2 = V2 + zi * S::VL.p + xx * S::VL.c;
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            d1[i * S::VL.r] = ra[i];
+            d2[i * S::VL.r] = rc[i];
+          }
+        }
+      }
+      __syncwarp();
+    }
+    // ---- x: r = b - s (M_x V1 + L_x V2), then S^T along x -> QA ----
+#pragma unroll
+    for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
+      const int t0 = lane + 32 * p;
+      const bool act = t0 < S::NQT;  // idle lanes redo task lane % NQT, stores skipped
+      const int t = act ? t0 : lane % S::NQT;
+      {
+        const int zi = t / M, yi = t % M;
+        float bv1[M], bv2[M];
+        if constexpr (K % 4 == 0 && W % 4 == 0) {
+          // the box origin is a multiple of 4 entries (x-offset 0): the row's
+          // interior is entries 1..M of two 16-byte vectors per group of 4;
+          // 8 lanes of rows 12 entries apart cover 32 distinct banks
+          const float4 *r1 = reinterpret_cast<const float4 *>(bslA + (zi * M + yi) * W);
+          const float4 *r2 = reinterpret_cast<const float4 *>(bslB + (zi * M + yi) * W);
+#pragma unroll
+          for (int g = 0; g < (M + 1) / 4; ++g) {
+            const float4 u1 = r1[g], u2 = r2[g];
+            const float e1[4] = {u1.x, u1.y, u1.z, u1.w}, e2[4] = {u2.x, u2.y, u2.z, u2.w};
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              const int i = 4 * g + c - 1;
+              if (i >= 0 && i < M) {
+                bv1[i] = e1[c];
+                bv2[i] = e2[c];
+              }
+            }
+          }
+        } else {
+          const float *b1 = bslA + (zi * M + yi) * W + xoa + 1, *b2 = bslB + (zi * M + yi) * W + xob + 1;
+#pragma unroll
+          for (int i = 0; i < M; ++i) {
+            bv1[i] = b1[i];
+            bv2[i] = b2[i];
+          }
+        }
+        float2 res[M];
+        if (!a.zero_x) {
+          const float2 *s1 = V1 + t, *s2 = V2 + t;  // = zi * VL.p + yi * VL.r
+          float2 v[N1], E1[K], O1[K], ec1, E2[K], O2[K], ec2;
+#pragma unroll
+          for (int qq = 0; qq < N1; ++qq) v[qq] = s1[qq * S::VL.c];
+          pr_fold<K>(v, E1, O1, ec1);
+#pragma unroll
+          for (int qq = 0; qq < N1; ++qq) v[qq] = s2[qq * S::VL.c];
+          pr_fold<K>(v, E2, O2, ec2);
+          float2 ra[M];
+          pr_rows_sum<K>(tb.pmass_fe, tb.pmass_fo, E1, O1, ec1, tb.plap_fe, tb.plap_fo, E2, O2, ec2, ra);
+#pragma unroll
+          for (int i = 0; i < M; ++i) res[i] = pr_fma(-scale, ra[i], make_float2(bv1[i], bv2[i]));
+        } else {
+#pragma unroll
+          for (int i = 0; i < M; ++i) res[i] = make_float2(bv1[i], bv2[i]);
+        }
+        float2 qv[M];
+        pr_evec<K, true>(res, qv);
+        float2 *d = QAb + zi * QA.p + yi * QA.r;
+        if (act) {
+#pragma unroll
+          for (int i = 0; i < M; ++i) d[i * QA.c] = qv[i];
+        }
+      }
+    }
+    __syncwarp();
+    // the staged boxes and slabs are consumed: fetch the next pair now
+    if (lane == 0 && q + G < n_pairs) {
+      fence_proxy_async_smem();
+      issue(nxa, nya, nza, nxb, nyb, nzb);
+    }
+    // ---- the four fast-diagonalisation stages: each lane's tasks of both
+    // passes side by side (all loads, then the independent contractions, then
+    // the stores), so the two chains interleave ----
+    constexpr int NP = (S::NQT + 31) / 32;
+    int tq[NP];
+    bool aq[NP];
+#pragma unroll
+    for (int p = 0; p < NP; ++p) {
+      aq[p] = lane + 32 * p < S::NQT;  // idle lanes redo task lane % NQT, stores skipped
+      tq[p] = aq[p] ? lane + 32 * p : lane % S::NQT;
+    }
+    // ---- S^T along y: QA -> QB ----
+    {
+      float2 v[NP][M], qv[NP][M];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const float2 *src = QAb + (tq[p] / M) * QA.p + (tq[p] % M) * QA.c;
+#pragma unroll
+        for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QA.r];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) pr_evec<K, true>(v[p], qv[p]);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        float2 *d = QBb + (tq[p] / M) * QB.p + (tq[p] % M) * QB.c;
+        if (aq[p]) {
+#pragma unroll
+          for (int jj = 0; jj < M; ++jj) d[jj * QB.r] = qv[p][jj];
+        }
+      }
+    }
+    __syncwarp();
+    // ---- S^T along z, eigenvalue scaling, S along z: QB -> QC ----
+    {
+      float2 v[NP][M], qv[NP][M];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const float2 *src = QBb + (tq[p] / M) * QB.r + (tq[p] % M) * QB.c;
+#pragma unroll
+        for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QB.p];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        pr_evec<K, true>(v[p], qv[p]);
+#pragma unroll
+        for (int jj = 0; jj < M; ++jj) qv[p][jj] = pr_mul(rl[p][jj], qv[p][jj]);
+        pr_evec<K, false>(qv[p], v[p]);
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        float2 *d = QAb + (tq[p] / M) * QC.r + (tq[p] % M) * QC.c;
+        if (aq[p]) {
+#pragma unroll
+          for (int jj = 0; jj < M; ++jj) d[jj * QC.p] = v[p][jj];
+        }
+      }
+    }
+    __syncwarp();
+    // ---- S along x: QC -> QD ----
+    {
+      float2 v[NP][M], qv[NP][M];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const float2 *src = QAb + (tq[p] / M) * QC.p + (tq[p] % M) * QC.r;
+#pragma unroll
+        for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QC.c];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) pr_evec<K, false>(v[p], qv[p]);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        float2 *d = QBb + (tq[p] / M) * QD.p + (tq[p] % M) * QD.r;
+        if (aq[p]) {
+#pragma unroll
+          for (int i = 0; i < M; ++i) d[i * QD.c] = qv[p][i];
+        }
+      }
+    }
+    __syncwarp();
+    // ---- S along y and store x_I of both patches ----
+    {
+      float *const xpa = x + (fxa + 1 + (fya + 1) * a.sy + (fza + 1) * a.sz);
+      float *const xpb = x + (fxb + 1 + (fyb + 1) * a.sy + (fzb + 1) * a.sz);
+      const int sy32 = static_cast<int>(a.sy), sz32 = static_cast<int>(a.sz);
+      float2 v[NP][M], qv[NP][M];
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const float2 *src = QBb + (tq[p] / M) * QD.p + (tq[p] % M) * QD.c;
+#pragma unroll
+        for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QD.r];
+      }
+#pragma unroll
+      for (int p = 0; p < NP; ++p) pr_evec<K, false>(v[p], qv[p]);
+#pragma unroll
+      for (int p = 0; p < NP; ++p) {
+        const int o = tq[p] % M + (tq[p] / M) * sz32;
+        if (aq[p]) {
+#pragma unroll
+          for (int jj = 0; jj < M; ++jj) xpa[o + jj * sy32] = qv[p][jj].x;
+        }
+        if (aq[p] && store_b) {
+#pragma unroll
+          for (int jj = 0; jj < M; ++jj) xpb[o + jj * sy32] = qv[p][jj].y;
+        }
+      }
+    }
+    __syncwarp();  // the Q buffers (inside the Z region) are read before the next z stage
+    fxa = nxa;
+    fya = nya;
+    fza = nza;
+    fxb = nxb;
+    fyb = nyb;
+    fzb = nzb;
+  }
+}
+
+}  // namespace tps

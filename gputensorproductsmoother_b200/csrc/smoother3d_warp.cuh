@@ -260,8 +260,8 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
               T *d1 = Z1 + y * Lo::RZ + xx, *d2 = Z2 + y * Lo::RZ + xx;
 #pragma unroll
               for (int i = 0; i < M; ++i) {
-                d1[i * Lo::PZ] = tb.pmass[(i + 1) * N1] * v0 + tb.pmass[(i + 1) * N1 + N1 - 1] * vn;
-                d2[i * Lo::PZ] = tb.plap[(i + 1) * N1] * v0 + tb.plap[(i + 1) * N1 + N1 - 1] * vn;
+                d1[i * Lo::PZ] = fmadd(tb.pmass[(i + 1) * N1 + N1 - 1], vn, tb.pmass[(i + 1) * N1] * v0);
+                d2[i * Lo::PZ] = fmadd(tb.plap[(i + 1) * N1 + N1 - 1], vn, tb.plap[(i + 1) * N1] * v0);
               }
             }
           }

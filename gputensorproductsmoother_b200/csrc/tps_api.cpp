@@ -410,19 +410,27 @@ VcycleVectors &vcycle_vectors(tps_handle *h, int p)
   return V;
 }
 
-// smoother variant of a level that was neither autotuned nor set: the
-// one-warp-per-patch kernel (variant 3) for degrees 3 and 4 when a colour
-// holds at least 4096 patches, else the default CTA batch.  Measured on B200
-// (us per sweep, best CTA batch vs one warp per patch): Q4 64^3 FP32 738 vs
-// 584, FP64 1166 vs 1052; Q4 32^3 FP32 132 vs 115; Q3 32^3 FP64 114 vs 105;
-// on 16^3 and coarser levels (latency-bound launches) and for degrees 2 and 5
-// (3x3 patch interiors leave lanes idle, 9^3 patches leave few warps per SM)
-// the CTA batches are as fast or faster.
+// smoother variant of a level that was neither autotuned nor set.  FP32,
+// degrees 2..4: two patches per warp in packed FP32 (variant 4) when a
+// colour holds at least 4096 patches, else one warp per patch (variant 3).
+// FP64 (and FP32 at other degrees): one warp per patch for degrees 3 and 4
+// from 4096 patches per colour, else the default CTA batch.  Measured on B200
+// (us per FP32 sweep, CTA batch / one warp per patch / two patches per warp):
+// Q4 64^3 724 / 566 / 506, Q4 32^3 118 / 97 / 94, Q3 64^3 344 / 316 / 269,
+// Q3 32^3 72 / 65 / 62, Q2 64^3 145 / 156 / 108, Q2 16^3 34 / 22 / 23;
+// degree 5 is fastest with the CTA batch (248 / 310 / 307 at 32^3: the larger
+// per-warp stages leave few warps per SM).  FP64: Q4 64^3 1166 vs 1052 (CTA
+// batch vs one warp per patch), Q3 32^3 114 vs 105; 16^3 and coarser levels
+// are launch-latency-bound and equal or faster with CTA batches.
 int default_variant(const tps_handle *h, int level, int p)
 {
-  if (h->dim != 3 || (h->k != 3 && h->k != 4) || h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 3) != -1) return 0;
+  if (h->dim != 3) return 0;
   const int64_t c = h->lv[level].n / 2;  // patches per direction of colour 0
-  return c * c * c >= 4096 ? 3 : 0;
+  const bool large = c * c * c >= 4096;
+  if (p == 1 && h->k >= 2 && h->k <= 4 && h->kt->smoother_ppb(3, 1, 4) == -2 && h->kt->smoother_ppb(3, 1, 3) == -1)
+    return large ? 4 : 3;
+  if ((h->k != 3 && h->k != 4) || h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 3) != -1) return 0;
+  return large ? 3 : 0;
 }
 
 // one coloured sweep; x_zero declares x == 0 on entry (the first colour then

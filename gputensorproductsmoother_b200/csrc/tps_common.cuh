@@ -42,6 +42,17 @@ struct Pair<double> {
   }
 };
 
+// a * b + c as one fused multiply-add in either precision: written out where
+// the sum of two products would otherwise leave the choice of the fused
+// product to the compiler, so that kernels of different shapes round alike
+__device__ __forceinline__ float fmadd(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmadd(double a, double b, double c) { return __fma_rn(a, b, c); }
+// a + b and a - b that the compiler may not fuse with a product operand
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+
 template <int K, typename T>
 struct DegreeTables {
   T pmass[Dims<K>::N1 * Dims<K>::N1];   // patch mass (reference cells)

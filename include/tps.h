@@ -245,10 +245,14 @@ int tps_solve_host_many(tps_handle *h, const tps_solve_opts *opts, int n, const 
  * (0 in 2D, -1 for the one-warp-per-patch kernel).  Batched solves tune their systems automatically. */
 int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
 /* The compiled variants of the 3D smoother, TPS_SMOOTHER_VARIANTS entries:
- * patches per CTA batch 0 default, 1 half, 2 quarter, and 3 one warp per
- * patch (reported as -1 where it is compiled, else as variant 0's value; 0 in
- * 2D), and the explicit choice of one for a level (what tps_autotune sets). */
-#define TPS_SMOOTHER_VARIANTS 4
+ * patches per CTA batch 0 default, 1 half, 2 quarter, 3 one warp per patch
+ * (reported as -1 where it is compiled) and 4 two patches per warp in packed
+ * FP32 arithmetic (FP32 only, degrees 2..5; reported as -2 where it is
+ * compiled); a variant that is not compiled reports variant 0's value, and
+ * 2D reports 0.  tps_set_smoother_variant makes the explicit choice of one
+ * for a level (what tps_autotune sets).  All variants give bit-identical
+ * sweeps. */
+#define TPS_SMOOTHER_VARIANTS 5
 int tps_smoother_variants(tps_handle *h, int dtype, int *ppb);
 int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant);
 /* The variant a level's sweeps use now: the one set or autotuned, else the

@@ -67,7 +67,7 @@ def test_autotune_keeps_results(cuda):
     x_def = x0.clone()
     tps.PatchSmoother(P).step(x_def, b)
     ppb = P.autotune("fp32")
-    assert len(ppb) == P.n_levels and all(v >= 1 or v == -1 for v in ppb)
+    assert len(ppb) == P.n_levels and all(v >= 1 or v in (-1, -2) for v in ppb)
     x_tuned = x0.clone()
     tps.PatchSmoother(P).step(x_tuned, b)
     torch.cuda.synchronize()

@@ -159,7 +159,8 @@ def test_vcycle(cuda, oracle, dim, k, n, precision, oprec, tol, symmetric):
 @pytest.mark.parametrize("precision,oprec,tol", [("fp64", 0, TOL64), ("fp32", 1, 1e-4)])
 def test_vcycle_smoother_variants(cuda, oracle, k, n, precision, oprec, tol):
     """Every compiled 3D smoother variant (patches per CTA batch P, P/2, P/4,
-    one warp per patch) gives the oracle's V-cycle; the variants only regroup
+    one warp per patch, two patches per warp in packed FP32) gives the
+    oracle's V-cycle; the variants only regroup
     the independent patches of a colour with the same per-patch arithmetic,
     so their V-cycles are bit-identical."""
     P = tps.PoissonProblem(3, k, n)
@@ -169,7 +170,7 @@ def test_vcycle_smoother_variants(cuda, oracle, k, n, precision, oprec, tol):
     ref = H.vcycle(src, precision=oprec, symmetric=True)
     dt = "fp64" if precision == "fp64" else "fp32"
     variants = P.smoother_variants(dt)
-    assert len(variants) == 4
+    assert len(variants) == 5
     outs = []
     for v in range(len(variants)):
         P.set_smoother_variant(v, dt)
@@ -235,3 +236,24 @@ def test_gmres_parity(cuda, oracle, dim, k, n):
                                                  max_iter=20, reduce=1e-9)
     assert rep.iterations == it_r
     assert relerr(x.cpu().numpy(), xr) < 1e-10
+
+
+@pytest.mark.parametrize("k,n", [(4, 32), (3, 16), (5, 8)])
+def test_pair_kernel_solve_bit_identical(cuda, k, n):
+    """The two-patches-per-warp packed-FP32 smoother (variant 4) and the
+    one-warp-per-patch kernel (variant 3, or the CTA batch where that is not
+    compiled) give bit-identical FP32-V-cycle CG solves: same residual
+    histories, same solution."""
+    P = tps.PoissonProblem(3, k, n)
+    b = dev(_rhs(3, n * k + 1, 31), torch.float64)
+    MG = tps.MultigridSolvers(P)
+    out = {}
+    for v in (3, 4):
+        P.set_smoother_variant(v, "fp32")
+        x, rep = MG.solve_cg(b, precision="fp32", rel_tol=1e-10)
+        torch.cuda.synchronize()
+        out[v] = (x.clone(), list(rep.history), rep.iterations)
+    assert out[3][2] == out[4][2]
+    assert out[3][1] == out[4][1]
+    assert torch.equal(out[3][0], out[4][0])
+    P.close()
