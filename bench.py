@@ -58,8 +58,9 @@ def parse():
     ap.add_argument("--variant", type=int, default=-1,
                     help="--mode smoother: 3D smoother variant (0-2 CTA batches P, P/2, P/4; 3 one warp "
                          "per patch; -1 the library default)")
-    ap.add_argument("--smoother", default="fp32", choices=["fp32", "tf32", "fp64"],
-                    help="--mode smoother: FP32 SIMT kernel, tensor-core (TF32) kernel or FP64")
+    ap.add_argument("--smoother", default="fp32", choices=["fp32", "tf32", "tf32x3", "fp64"],
+                    help="--mode smoother: FP32 SIMT kernel, tensor-core kernel (TF32, or the "
+                         "three-term TF32 split) or FP64")
     ap.add_argument("--directions", type=int, default=64,
                     help="--mode adjoint: random unit directions of the finite-difference check")
     ap.add_argument("--config", default=None,
@@ -117,14 +118,14 @@ def run_smoother_only(args):
     stream = torch.cuda.Stream()
     sp = ctypes.c_void_p(stream.cuda_stream)
     ms = ctypes.c_double()
-    code = {"fp32": L.TPS_F32, "tf32": L.TPS_TF32, "fp64": L.TPS_F64}[args.smoother]
-    if args.variant >= 0 and args.smoother != "tf32":
+    code = {"fp32": L.TPS_F32, "tf32": L.TPS_TF32, "tf32x3": L.TPS_TF32X3, "fp64": L.TPS_F64}[args.smoother]
+    if args.variant >= 0 and args.smoother in ("fp32", "fp64"):
         P.set_smoother_variant(args.variant, args.smoother, lf)
     if args.warmup > 0:
         L.check(L.lib().tps_time_smoother(P.handle, lf, code, args.warmup, ctypes.byref(ms), sp), P.handle)
     L.check(L.lib().tps_time_smoother(P.handle, lf, code, max(args.steps, 1), ctypes.byref(ms), sp), P.handle)
     total, per = smoother_bytes(dim, k, n, 8 if args.smoother == "fp64" else 4)
-    variant = P.smoother_variant(lf, args.smoother) if args.smoother != "tf32" else None
+    variant = P.smoother_variant(lf, args.smoother) if args.smoother in ("fp32", "fp64") else None
     print(json.dumps({"mode": "smoother", "smoother": args.smoother, "workload": args.workload,
                       "variant": variant, "ms_per_sweep": ms.value, "algorithmic_GBps": total / (ms.value * 1e-3) / 1e9}),
           flush=True)

@@ -17,8 +17,8 @@ STATUS_NAMES = {
     4: "TPS_ERR_NOT_CONVERGED", 5: "TPS_ERR_BREAKDOWN", 6: "TPS_ERR_NONFINITE",
     7: "TPS_ERR_UNSUPPORTED", 8: "TPS_ERR_TIMEOUT",
 }
-TPS_F64, TPS_F32, TPS_TF32 = 0, 1, 2
-VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32 = 0, 1, 2, 3
+TPS_F64, TPS_F32, TPS_TF32, TPS_TF32X3 = 0, 1, 2, 3
+VCYCLE_F64, VCYCLE_F32, VCYCLE_F64_ROUNDED, VCYCLE_TF32, VCYCLE_TF32X3 = 0, 1, 2, 3, 4
 DRIVER_CG, DRIVER_GMRES = 0, 1
 SMOOTHER_VARIANTS = 5  # TPS_SMOOTHER_VARIANTS
 SMOOTHER_FUSED, SMOOTHER_SEPARATE, SMOOTHER_GLOBAL, SMOOTHER_EXACT, SMOOTHER_ADDITIVE = 0, 1, 2, 3, 4

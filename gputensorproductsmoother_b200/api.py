@@ -26,7 +26,7 @@ from . import _lib as L
 
 _DTYPES = {torch.float64: L.TPS_F64, torch.float32: L.TPS_F32}
 _PRECISIONS = {"fp64": L.VCYCLE_F64, "fp32": L.VCYCLE_F32, "fp64_rounded": L.VCYCLE_F64_ROUNDED,
-               "tf32": L.VCYCLE_TF32}
+               "tf32": L.VCYCLE_TF32, "tf32x3": L.VCYCLE_TF32X3}
 
 
 def split_cells(n_cells: int) -> tuple[int, int]:
@@ -96,7 +96,7 @@ class PoissonProblem:
         """Milliseconds per coloured sweep on the level's V-cycle work vectors
         (CUDA events on the current stream); dtype "fp64", "fp32" or "tf32"
         (tensor-core patch solves)."""
-        codes = {"fp64": L.TPS_F64, "fp32": L.TPS_F32, "tf32": L.TPS_TF32}
+        codes = {"fp64": L.TPS_F64, "fp32": L.TPS_F32, "tf32": L.TPS_TF32, "tf32x3": L.TPS_TF32X3}
         ms = ctypes.c_double()
         lv = self.n_levels - 1 if level is None else level
         L.check(L.lib().tps_time_smoother(self.handle, lv, codes[dtype], sweeps, ctypes.byref(ms), _stream()),
@@ -237,8 +237,10 @@ class LaplaceOperator:
 class PatchSmoother:
     """PatchSmoother (PreconditionRelaxation over the coloured vertex-patch
     sweep): vmult zeroes dst and sweeps once, step sweeps once in place.
-    tensor_cores=True runs the 3D patch solves of FP32 vectors on the tensor
-    cores (TF32 operands, FP32 accumulation).  variant selects the
+    tensor_cores=True (or "tf32") runs the 3D patch solves of FP32 vectors on
+    the tensor cores (TF32 operands, FP32 accumulation); "tf32x3" forms every
+    product from a three-term TF32 split (about FP32 accuracy, degree 4 only).
+    variant selects the
     reference's SmootherVariant (include/patch_base.cuh:28-90): "fused" (the
     default kernels), or the separate-kernel cross-checks "separate" (patch
     residual kernel + fast-diagonalisation kernel), "global" (level operator
@@ -254,7 +256,9 @@ class PatchSmoother:
                  variant: str = "fused"):
         self.problem = problem
         self.level = problem.n_levels - 1 if level is None else level
-        self.tensor_cores = tensor_cores
+        if tensor_cores not in (False, True, "tf32", "tf32x3"):
+            raise ValueError(f"tensor_cores must be False, True, 'tf32' or 'tf32x3', not {tensor_cores!r}")
+        self.tensor_cores = "tf32" if tensor_cores is True else tensor_cores
         if variant not in self.VARIANTS:
             raise ValueError(f"unknown smoother variant {variant!r}")
         if tensor_cores and variant != "fused":
@@ -268,7 +272,7 @@ class PatchSmoother:
         if self.tensor_cores:
             if dst.dtype != torch.float32:
                 raise TypeError("the tensor-core smoother works on float32 vectors")
-            dt = L.TPS_TF32
+            dt = L.TPS_TF32X3 if self.tensor_cores == "tf32x3" else L.TPS_TF32
         if self.variant == "fused":
             L.check(L.lib().tps_smoother_step(p.handle, self.level, dt, dst.data_ptr(), src.data_ptr(),
                                               int(zero_init), int(reverse), _stream()), p.handle)

@@ -327,6 +327,11 @@ float round_tf32(double v)
 
 std::vector<float> patch_gemm_image(const DegreeData &D, int nbe, int nbo, int ck)
 {
+  return patch_gemm_image_ordered(D, nbe, nbo, ck, 0, false);
+}
+
+std::vector<float> patch_gemm_image_ordered(const DegreeData &D, int nbe, int nbo, int ck, int order, bool split)
+{
   const int k = D.k, n1 = 2 * k + 1, m = 2 * k - 1;
   const int nb = n1 * n1 * n1, ni = m * m * m, pl = n1 * n1, ipl = m * m;
   const std::vector<double> inv = dense_patch_inverse(D, 3);  // ni x ni
@@ -372,29 +377,58 @@ std::vector<float> patch_gemm_image(const DegreeData &D, int nbe, int nbo, int c
     const double a = in(grow(zp, r)), b = in(grow(m - 1 - zp, r));
     return odd_out ? 0.5 * (a - b) : 0.5 * (a + b);
   };
-  const int ce = (ke + ck - 1) / ck, co = (ko + ck - 1) / ck;
+  // K (column) order: 0 = p * (2k+1)^2 + s; 1 = the entries x < 2k of the box
+  // rows first (p * (2k+1) * 2k + y * 2k + x), then the x = 2k entries
+  // (rows_total + p * (2k+1) + y).  Returns false for a padding column.
+  const int rw = n1 - 1, rpp = n1 * rw;
+  auto colmap = [&](int col, int n_pp, int &p, int &s) {
+    if (order == 0) {
+      if (col >= n_pp * pl) return false;
+      p = col / pl;
+      s = col % pl;
+      return true;
+    }
+    if (col < n_pp * rpp) {
+      p = col / rpp;
+      const int r = col % rpp;
+      s = (r / rw) * n1 + r % rw;
+      return true;
+    }
+    const int c2 = col - n_pp * rpp;
+    if (c2 >= n_pp * n1) return false;
+    p = c2 / n1;
+    s = (c2 % n1) * n1 + rw;
+    return true;
+  };
+  const int ke_cols = (k + 1) * pl, ko_cols = k * pl;
+  const int ce = (ke_cols + ck - 1) / ck, co = (ko_cols + ck - 1) / ck;
   const size_t chunk_e = static_cast<size_t>(nbe) * ck, chunk_o = static_cast<size_t>(nbo) * ck;
-  std::vector<float> img(ce * chunk_e + co * chunk_o, 0.f);
-  auto put = [&](float *base, int n, int kk, float v) {
-    // K-major, no swizzle: 8-row groups of ck/4 core matrices (8 rows x 16 bytes)
-    base[((n >> 3) * (ck / 4) * 128 + (n & 7) * 16 + (kk >> 2) * 128 + (kk & 3) * 4) / 4] = v;
+  const size_t one = ce * chunk_e + co * chunk_o;
+  std::vector<float> img((split ? 2 : 1) * one, 0.f);
+  auto put = [&](float *base, int n, int kk, double v) {
+    // K-major, no swizzle: 8-row groups of ck/4 core matrices (8 rows x 16 bytes);
+    // with split, the TF32 residual v - tf32(v) goes to the second image
+    const size_t at = ((n >> 3) * (ck / 4) * 128 + (n & 7) * 16 + (kk >> 2) * 128 + (kk & 3) * 4) / 4;
+    const float hi = round_tf32(v);
+    base[at] = hi;
+    if (split) base[one + at] = round_tf32(v - static_cast<double>(hi));
   };
   for (int c = 0; c < ce; ++c)
     for (int n = 0; n < ne; ++n)
       for (int kk = 0; kk < ck; ++kk) {
-        const int col = c * ck + kk;
-        if (col >= ke) continue;
-        const int zp = n / ipl, r = n % ipl, p = col / pl, s = col % pl;
-        put(&img[c * chunk_e], n, kk, round_tf32(coef(false, false, zp, r, p, s)));
+        int p = 0, s = 0;
+        if (!colmap(c * ck + kk, k + 1, p, s)) continue;
+        const int zp = n / ipl, r = n % ipl;
+        put(&img[c * chunk_e], n, kk, coef(false, false, zp, r, p, s));
       }
   float *go = img.data() + ce * chunk_e;
   for (int c = 0; c < co; ++c)
     for (int n = 0; n < no; ++n)
       for (int kk = 0; kk < ck; ++kk) {
-        const int col = c * ck + kk;
-        if (col >= ko) continue;
-        const int zp = n / ipl, r = n % ipl, p = col / pl, s = col % pl;
-        put(go + c * chunk_o, n, kk, round_tf32(coef(true, true, zp, r, p, s)));
+        int p = 0, s = 0;
+        if (!colmap(c * ck + kk, k, p, s)) continue;
+        const int zp = n / ipl, r = n % ipl;
+        put(go + c * chunk_o, n, kk, coef(true, true, zp, r, p, s));
       }
   return img;
 }

@@ -52,6 +52,14 @@ std::vector<double> dense_patch_inverse(const DegreeData &D, int dim);
 // of ck/4 core matrices of 8 rows x 16 bytes), values rounded to nearest TF32.
 // Returns G_E's chunks followed by G_O's as FP32 words.
 std::vector<float> patch_gemm_image(const DegreeData &D, int nbe, int nbo, int ck);
+// The same blocks with a choice of column order and precision: order 0 as
+// above; order 1 lists, per box plane pair p, the entries x = 0..2k-1 of the
+// rows y = 0..2k (column p (2k+1) 2k + y 2k + x) and after all plane pairs
+// the x = 2k entries (column (pairs) (2k+1) 2k + p (2k+1) + y), so that a
+// chunk of 3 * 2k columns is three box rows of one plane pair.  With split,
+// a second image of the same size follows with the TF32 residuals
+// tf32(v - tf32(v)) (the low parts of a three-product TF32 split).
+std::vector<float> patch_gemm_image_ordered(const DegreeData &D, int nbe, int nbo, int ck, int order, bool split);
 
 // Inverse of the symmetric positive definite n x n matrix A (row-major,
 // overwritten): Cholesky factorisation A = L L^T, W = L^{-1}, A^{-1} = W^T W,

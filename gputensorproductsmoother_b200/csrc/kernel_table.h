@@ -80,9 +80,11 @@ struct KernelTable {
   cudaError_t (*cell_energy[2])(const LevelGeomH &, const VecLayout &, double *e, const double *u,
                                 const double *lam, cudaStream_t);
   // 3D colour step on the tensor cores (FP32 vectors, TF32 operands, FP32
-  // accumulation); null for degree 1; needs maps->tc_valid
+  // accumulation; passes 3: three-term TF32 split, degree 4 only); null for
+  // degree 1; needs maps->tc_valid
   cudaError_t (*smoother_tc)(const LevelGeomH &, const VecLayout &, void *x, const void *b, int colour,
-                             double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t);
+                             double omega, int zero_x, const SmootherMaps *maps, int passes, int *err,
+                             cudaStream_t);
   // the rank-4 TMA views of FP32 x and b (sets tc_valid when the layout allows them)
   cudaError_t (*encode_tc_maps)(const VecLayout &l, void *x, const void *b, SmootherMaps *out);
   // patches per CTA batch of smoother variant v (dtype 0 FP64, 1 FP32; 0 in

@@ -12,6 +12,7 @@
 #include "smoother3d.cuh"
 #include "smoother3d_gemm.cuh"
 #include "smoother3d_pair.cuh"
+#include "smoother3d_pgemm.cuh"
 #include "smoother3d_tc.cuh"
 #include "smoother3d_warp.cuh"
 #include "smoother_variants.cuh"
@@ -126,6 +127,12 @@ cudaError_t set_attributes()
   if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_tc_kernel<K>), (Tc3<K>::BYTES));
 #if TPS_DEGREE <= 4
   if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_gemm_kernel<K>), (Pg3<K>::BYTES));
+#if TPS_DEGREE == 4
+  if constexpr (sizeof(T) == 4) {
+    TPS_SET((smoother3d_pgemm_kernel<K, 1>), (Pgv<K, 1>::BYTES));
+    TPS_SET((smoother3d_pgemm_kernel<K, 3>), (Pgv<K, 3>::BYTES));
+  }
+#endif
 #endif
 #endif
 #undef TPS_SET
@@ -142,6 +149,20 @@ cudaError_t upload(const DegreeData &D)
     static const std::vector<float> img = patch_gemm_image(D, Pg3<K>::NBE, Pg3<K>::NBO, Pg3<K>::CK);
     if (e == cudaSuccess && img.size() != static_cast<size_t>(Pg3<K>::IMG_FLOATS)) e = cudaErrorInvalidValue;
     if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_pg3_image<K>, img.data(), sizeof(float) * img.size());
+  }
+#endif
+#if TPS_DEGREE == 4
+  {
+    // the row-ordered images of the vector-producer kernel: TF32, and TF32 hi/lo
+    static const std::vector<float> im1 = patch_gemm_image_ordered(D, Pgv<K, 1>::NBE, Pgv<K, 1>::NBO,
+                                                                   Pgv<K, 1>::CK, 1, false);
+    static const std::vector<float> im3 = patch_gemm_image_ordered(D, Pgv<K, 3>::NBE, Pgv<K, 3>::NBO,
+                                                                   Pgv<K, 3>::CK, 1, true);
+    if (e == cudaSuccess && (im1.size() != static_cast<size_t>(Pgv<K, 1>::IMG_FLOATS) ||
+                             im3.size() != static_cast<size_t>(Pgv<K, 3>::IMG_FLOATS)))
+      e = cudaErrorInvalidValue;
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_pgv_image<K, 1>, im1.data(), sizeof(float) * im1.size());
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_pgv_image<K, 3>, im3.data(), sizeof(float) * im3.size());
   }
 #endif
   if (e == cudaSuccess) e = set_attributes<double>();
@@ -351,8 +372,11 @@ int tc_grid(int n_units)
 }
 
 cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const void *b, int colour,
-                        double omega, int zero_x, const SmootherMaps *maps, int *err, cudaStream_t s)
+                        double omega, int zero_x, const SmootherMaps *maps, int passes, int *err, cudaStream_t s)
 {
+#if TPS_DEGREE != 4
+  if (passes != 1) return cudaErrorNotSupported;
+#endif
 #if TPS_DEGREE <= 4
   {
     // degrees 2..4: the patch step as one GEMM over the colour's patches
@@ -380,7 +404,29 @@ cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const 
       return cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && n > 0 ? n : 1;
     }();
     const int tiles = static_cast<int>(ceil_div(count, 128));
-    TPS_LAUNCH((smoother3d_gemm_kernel<K>), tiles < n_sm ? tiles : n_sm, Pg3<K>::NT, Pg3<K>::BYTES, s,
+    const int grid = tiles < n_sm ? tiles : n_sm;
+#if TPS_DEGREE == 4
+    // the vector-producer kernel reads box rows as 16-byte vectors: vectors
+    // and pitches aligned to 4 entries (always true for the V-cycle's padded
+    // work vectors)
+    const bool vec_ok = (reinterpret_cast<uintptr_t>(x) % 16 == 0) && (reinterpret_cast<uintptr_t>(b) % 16 == 0) &&
+                        l.sy % 4 == 0 && l.sz % 4 == 0;
+    if (passes == 3 && !vec_ok) return cudaErrorNotSupported;
+    // one TF32 pass: the gather kernel below measured faster (0.511 vs 0.763 ms
+    // per Q4 64^3 sweep); the vector-producer kernel serves the three-pass split
+    if (vec_ok && passes == 3) {
+      if (passes == 3)
+        TPS_LAUNCH((smoother3d_pgemm_kernel<K, 3>), grid, (Pgv<K, 3>::NT), (Pgv<K, 3>::BYTES), s,
+            static_cast<float *>(x), static_cast<const float *>(b), a, static_cast<float>(sc),
+            static_cast<float>(omega / sc), err);
+      else
+        TPS_LAUNCH((smoother3d_pgemm_kernel<K, 1>), grid, (Pgv<K, 1>::NT), (Pgv<K, 1>::BYTES), s,
+            static_cast<float *>(x), static_cast<const float *>(b), a, static_cast<float>(sc),
+            static_cast<float>(omega / sc), err);
+      return cudaGetLastError();
+    }
+#endif
+    TPS_LAUNCH((smoother3d_gemm_kernel<K>), grid, Pg3<K>::NT, Pg3<K>::BYTES, s,
         static_cast<float *>(x), static_cast<const float *>(b), a, static_cast<float>(sc),
         static_cast<float>(omega / sc), err);
     (void)maps;

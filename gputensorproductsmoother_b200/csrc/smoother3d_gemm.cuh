@@ -98,7 +98,7 @@ constexpr bool pg3_enabled()
 // the B operand image of degree K (G_E chunks, then G_O chunks), written by
 // the per-degree upload
 template <int K>
-__device__ float g_pg3_image[Pg3<K>::IMG_FLOATS];
+__device__ __align__(128) float g_pg3_image[Pg3<K>::IMG_FLOATS];  // bulk-copy sources: 16-byte aligned
 
 // one interior row of a patch (M = 2K-1 entries from box x = 1).  For K = 4
 // the box origin is a multiple of 4 entries and so are the row pitches, so

@@ -206,6 +206,7 @@ struct tps_handle {
   // CUDA graph of one CG iteration
   cudaGraphExec_t graph = nullptr;
   int graph_key = -1;
+  int tc_passes = 1;  // tensor-core smoother: 1 TF32 pass, 3 the three-term TF32 split
   cudaStream_t graph_stream = nullptr;
   const double *graph_x = nullptr;  // the captured graph updates this solution vector
   cudaStream_t own_stream = nullptr;  // used by tps_solve_host
@@ -453,7 +454,7 @@ void smoother_sweep(tps_handle *h, int level, int p, const VecLayout &lay, void 
                                                     h->kappa_dev[p][level]->p, c, h->omega, s));
     else if (use_tc)
       TPS_CUDA(h->kt->smoother_tc(h->lv[level], lay, x, b, c, h->omega, (x_zero && i == 0) ? 1 : 0, maps,
-                                  h->err_flag.as<int>(), s));
+                                  h->tc_passes, h->err_flag.as<int>(), s));
     else
       TPS_CUDA(h->kt->smoother[h->dim - 2][p](h->lv[level], lay, x, b, c, h->omega,
                                               (x_zero && i == 0) ? 1 : 0, variant, maps,
@@ -598,7 +599,7 @@ void level_smooth(tps_handle *h, int level, int p, const VecLayout &lay, void *x
 // Smaller levels are latency-bound and keep the SIMT smoother.
 bool tc_pays(const tps_handle *h, int level)
 {
-  if (h->dim != 3 || h->k > 4) return false;
+  if (h->dim != 3 || h->k > 4 || (h->tc_passes == 3 && h->k != 4)) return false;
   const int64_t c = h->lv[level].n / 2;
   return c * c * c >= 128 * static_cast<int64_t>(h->n_sm);
 }
@@ -633,18 +634,25 @@ void vcycle_rec(tps_handle *h, int level, int p, bool symmetric, cudaStream_t s,
 
 int vprec_index(int precision)
 {
-  if (precision < 0 || precision > 3) throw ApiError(TPS_ERR_INVALID, "bad V-cycle precision");
-  return precision == TPS_VCYCLE_F32 || precision == TPS_VCYCLE_TF32 ? 1 : 0;
+  if (precision < 0 || precision > 4) throw ApiError(TPS_ERR_INVALID, "bad V-cycle precision");
+  return precision == TPS_VCYCLE_F32 || precision == TPS_VCYCLE_TF32 || precision == TPS_VCYCLE_TF32X3 ? 1 : 0;
 }
 // conversion of the FP64 input into the V-cycle vectors: 0 f64, 1 f32, 2 f64-rounded
-int input_kind(int precision) { return precision == TPS_VCYCLE_TF32 ? 1 : precision; }
-bool vprec_tc(int precision) { return precision == TPS_VCYCLE_TF32; }
+int input_kind(int precision)
+{
+  return precision == TPS_VCYCLE_TF32 || precision == TPS_VCYCLE_TF32X3 ? 1 : precision;
+}
+bool vprec_tc(int precision) { return precision == TPS_VCYCLE_TF32 || precision == TPS_VCYCLE_TF32X3; }
+// tensor-core passes of a V-cycle precision (only read where vprec_tc holds)
+int vprec_passes(int precision) { return precision == TPS_VCYCLE_TF32X3 ? 3 : 1; }
 
-// the tensor-core smoother exists for 3D, degree >= 2, constant coefficient
-void check_tc(tps_handle *h)
+// the tensor-core smoother exists for 3D, degree >= 2, constant coefficient;
+// records the passes (1 TF32, 3 the three-term split) for the sweeps that follow
+void check_tc(tps_handle *h, int passes = 1)
 {
   if (h->dim != 3 || !h->kt->smoother_tc || h->has_kappa)
     throw ApiError(TPS_ERR_UNSUPPORTED, "the tensor-core (TF32) smoother needs 3D, degree >= 2 and no kappa");
+  h->tc_passes = passes;
 }
 
 
@@ -750,7 +758,7 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
 {
   TPS_RANGE("tps_solve CG");
   const int p = vprec_index(o.precision);
-  if (vprec_tc(o.precision)) check_tc(h);
+  if (vprec_tc(o.precision)) check_tc(h, vprec_passes(o.precision));
   vcycle_vectors(h, p);
   ensure_krylov(h);
   const int L = h->n_levels - 1;
@@ -873,7 +881,7 @@ void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, c
                     cudaStream_t s)
 {
   const int p = vprec_index(precision);
-  if (vprec_tc(precision)) check_tc(h);
+  if (vprec_tc(precision)) check_tc(h, vprec_passes(precision));
   VcycleVectors &V = vcycle_vectors(h, p);
   const int L = h->n_levels - 1;
   const int64_t N = h->fine().N;
@@ -922,10 +930,12 @@ void autotune_levels(tps_handle *h, int p, cudaStream_t s)
 
 // tps_smoother_step with TPS_TF32 on caller vectors (FP32, lexicographic):
 // the sweep runs on the padded, TMA-addressable V-cycle vectors of the level
-void tc_smoother_step(tps_handle *h, int level, void *x, const void *b, bool zero_init, bool reverse,
+void tc_smoother_step(tps_handle *h, int level, void *x, const void *b, bool zero_init, bool reverse, int passes,
                       cudaStream_t s)
 {
-  check_tc(h);
+  check_tc(h, passes);
+  if (passes == 3 && h->k != 4)
+    throw ApiError(TPS_ERR_UNSUPPORTED, "the three-term TF32 tensor-core smoother needs degree 4");
   VcycleVectors &V = vcycle_vectors(h, 1);
   const VecLayout &l = V.layout[level];
   const size_t row = sizeof(float) * l.N1, pitch = sizeof(float) * l.sy;
@@ -947,7 +957,7 @@ void fmg(tps_handle *h, int precision, int n_cycles, const double *const *rhs, c
   TPS_RANGE("tps_fmg");
   const int p = vprec_index(precision), L = h->n_levels - 1, dim = h->dim;
   const bool tc = vprec_tc(precision);
-  if (tc) check_tc(h);
+  if (tc) check_tc(h, vprec_passes(precision));
   VcycleVectors &V = vcycle_vectors(h, p);
   ensure_krylov(h);
   if (h->fmg_sol.size() != static_cast<size_t>(h->n_levels)) {
@@ -1249,8 +1259,8 @@ int tps_smoother_step(tps_handle *h, int level, int dtype, void *x, const void *
     if (x == b) throw ApiError(TPS_ERR_INVALID, "x and b must not alias");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     const LevelGeomH &g = h->lv[level];
-    if (dtype == TPS_TF32) {
-      tc_smoother_step(h, level, x, b, zero_init != 0, reverse != 0, s);
+    if (dtype == TPS_TF32 || dtype == TPS_TF32X3) {
+      tc_smoother_step(h, level, x, b, zero_init != 0, reverse != 0, dtype == TPS_TF32X3 ? 3 : 1, s);
       return;
     }
     const int p = dt_index(dtype);
@@ -1516,8 +1526,10 @@ int tps_time_smoother(tps_handle *h, int level, int dtype, int sweeps, double *m
 {
   return guarded(h, [&] {
     check_level(h, level);
-    const bool tc = dtype == TPS_TF32;
-    if (tc) check_tc(h);
+    const bool tc = dtype == TPS_TF32 || dtype == TPS_TF32X3;
+    if (tc) check_tc(h, dtype == TPS_TF32X3 ? 3 : 1);
+    if (dtype == TPS_TF32X3 && h->k != 4)
+      throw ApiError(TPS_ERR_UNSUPPORTED, "the three-term TF32 tensor-core smoother needs degree 4");
     const int p = tc ? 1 : dt_index(dtype);
     if (sweeps < 1 || !ms_per_sweep) throw ApiError(TPS_ERR_INVALID, "sweeps >= 1 and an output are required");
     ensure_krylov(h);
@@ -2038,7 +2050,7 @@ int tps_batch_solve(tps_batch *B, const tps_solve_opts *opts, const double *cons
     const int n = static_cast<int>(B->sys.size());
     for (int i = 0; i < n; ++i) {
       if (!rhs[i] || !x[i]) throw ApiError(TPS_ERR_INVALID, "null vector");
-      if (vprec_tc(opts->precision)) check_tc(B->sys[i]);
+      if (vprec_tc(opts->precision)) check_tc(B->sys[i], vprec_passes(opts->precision));
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (!s) {  // capture needs a non-default stream

@@ -35,9 +35,12 @@ typedef enum {
 typedef enum {
   TPS_F64 = 0,
   TPS_F32 = 1,
-  TPS_TF32 = 2 /* FP32 vectors; the 3D patch solves run on the tensor cores (TF32
+  TPS_TF32 = 2, /* FP32 vectors; the 3D patch solves run on the tensor cores (TF32
                   operands, FP32 accumulation).  tps_smoother_step and
                   tps_time_smoother only. */
+  TPS_TF32X3 = 3 /* as TPS_TF32 with every product formed from a three-term TF32
+                    split (a_hi b_hi + a_hi b_lo + a_lo b_hi): about FP32 accuracy
+                    per product, FP32 accumulation.  Degree 4 only. */
 } tps_dtype;
 
 typedef struct tps_handle tps_handle;
@@ -127,11 +130,14 @@ typedef enum {
   TPS_VCYCLE_F32 = 1,        /* FP32 smoother/operator/transfer inside the V-cycle */
   TPS_VCYCLE_F64_ROUNDED = 2, /* FP64 V-cycle fed with FP32-rounded input: the
                                 reference's "double" V-cycle (include/solver.cuh:64-78) */
-  TPS_VCYCLE_TF32 = 3         /* as TPS_VCYCLE_F32, with the 3D patch solves on the tensor
+  TPS_VCYCLE_TF32 = 3,        /* as TPS_VCYCLE_F32, with the 3D patch solves on the tensor
                                 cores (TF32 operands, FP32 accumulation) on the levels
                                 where that is faster: degrees 2..4, colours of at least
                                 128 patches per multiprocessor; the other levels use the
                                 FP32 smoother */
+  TPS_VCYCLE_TF32X3 = 4       /* as TPS_VCYCLE_TF32 with the three-term TF32 split of
+                                TPS_TF32X3 (FP32-accurate products) on the same levels,
+                                degree 4 only; other degrees run TPS_VCYCLE_F32 */
 } tps_vcycle_precision;
 
 /* MultigridSolvers::vmult (include/solver.cuh:1915-1930): dst = V-cycle(src) on the

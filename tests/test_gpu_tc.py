@@ -68,3 +68,60 @@ def test_tc_timing_hook(cuda):
     P = tps.PoissonProblem(3, 4, 16)
     ms = P.time_smoother(dtype="tf32", sweeps=3)
     assert ms > 0.0
+
+
+# three-term TF32 split (a_hi b_hi + a_hi b_lo + a_lo b_hi, FP32 accumulation):
+# products to about FP32 accuracy, so a sweep meets the FP32 sweep tolerance
+TF32X3_SWEEP_TOL = 2e-5
+
+
+@pytest.mark.parametrize("n", [4, 8, 16])
+@pytest.mark.parametrize("zero_init", [False, True])
+def test_tf32x3_sweep_matches_oracle_at_fp32_accuracy(cuda, oracle, n, zero_init):
+    """Degree 4 (the vector-producer patch-GEMM kernel): the three-pass
+    tensor-core sweep agrees with the FP64 oracle sweep and with the FP32 SIMT
+    sweep to the FP32 tolerance; the one-pass TF32 sweep of the same kernel
+    stays within the TF32 tolerance."""
+    k = 4
+    P = tps.PoissonProblem(3, k, n)
+    N1 = n * k + 1
+    x0, b = interior_random(N1, 11), interior_random(N1, 12)
+    ref = oracle.smoother_step(3, k, n, x0, b, zero_init=zero_init)
+    bd = torch.tensor(b, dtype=torch.float32, device="cuda")
+    out = {}
+    for mode in ("tf32x3", "tf32", False):
+        x = torch.tensor(x0, dtype=torch.float32, device="cuda")
+        S = tps.PatchSmoother(P, tensor_cores=mode)
+        (S.vmult if zero_init else S.step)(x, bd)
+        torch.cuda.synchronize()
+        out[mode] = x.cpu().numpy()
+    assert np.all(np.isfinite(out["tf32x3"]))
+    assert relerr(out["tf32x3"], ref) < TF32X3_SWEEP_TOL, relerr(out["tf32x3"], ref)
+    assert relerr(out["tf32x3"], out[False]) < TF32X3_SWEEP_TOL
+    assert relerr(out["tf32"], ref) < TF32_SWEEP_TOL
+
+
+def test_tf32x3_vcycle_cg_matches_fp32_iterations(cuda):
+    """The three-pass tensor-core V-cycle (degree 4) preconditions the FP64 CG
+    like the FP32 V-cycle: same iteration count, solution within 1e-8 of the
+    FP64-V-cycle solve."""
+    P = tps.PoissonProblem(3, 4, 32)
+    b = torch.tensor(interior_random(4 * 32 + 1, 13), device="cuda")
+    MG = tps.MultigridSolvers(P)
+    x64, r64 = MG.solve_cg(b, precision="fp64", rel_tol=1e-10)
+    x32, r32 = MG.solve_cg(b, precision="fp32", rel_tol=1e-10)
+    x3, r3 = MG.solve_cg(b, precision="tf32x3", rel_tol=1e-10)
+    assert r3.converged and r3.final_residual <= 1e-10
+    assert r3.iterations == r32.iterations
+    assert relerr(x3.cpu().numpy(), x64.cpu().numpy()) < 1e-8
+
+
+def test_tf32x3_other_degrees_unsupported(cuda):
+    P = tps.PoissonProblem(3, 3, 8)
+    x = P.new_vector(dtype=torch.float32)
+    with pytest.raises(tps.TpsError):
+        tps.PatchSmoother(P, tensor_cores="tf32x3").step(x, P.new_vector(dtype=torch.float32))
+    # the V-cycle precision falls back to the FP32 smoother at other degrees
+    b = torch.tensor(interior_random(3 * 8 + 1, 14), device="cuda")
+    x3, r3 = tps.MultigridSolvers(P).solve_cg(b, precision="tf32x3", rel_tol=1e-10)
+    assert r3.converged
