@@ -66,7 +66,7 @@ def test_invalid_arguments_leave_the_handle_usable(cuda):
     x = torch.zeros_like(b)
     assert raw_solve(P, b, x, max_iter=0)[0] == INVALID
     assert raw_solve(P, b, x, driver=5)[0] == INVALID
-    assert raw_solve(P, b, x, precision=4)[0] == INVALID
+    assert raw_solve(P, b, x, precision=5)[0] == INVALID
     assert x.abs().max().item() == 0.0  # nothing ran
     st, rep = raw_solve(P, b, x)
     assert st == L.TPS_OK and rep.converged
