@@ -51,7 +51,7 @@ def parse():
                     help="skip the sub-records of the other configurations (2D Q2 64^2, Q7 32^3, "
                          "batched Q3, adjoint Q4 48^3) that follow the headline measurement")
     ap.add_argument("--mode", default="solve",
-                    choices=["solve", "smoother", "operator", "batch", "adjoint", "micro"],
+                    choices=["solve", "smoother", "operator", "batch", "adjoint", "micro", "solves"],
                     help="smoother / operator: only time the finest-level smoother "
                          "sweeps / FP64 operator applications (small commands for kernel "
                          "profiling)")
@@ -102,6 +102,28 @@ def run_operator_only(args):
     ms = e0.elapsed_time(e1) / max(args.steps, 1)
     print(json.dumps({"mode": "operator", "workload": args.workload, "ms_per_apply": ms,
                       "algorithmic_GBps": 2 * 8 * P.n_dofs() / (ms * 1e-3) / 1e9}), flush=True)
+    P.close()
+
+
+def run_solves_once(args):
+    """--mode solves: one FP32-V-cycle and one FP64-V-cycle solve of the
+    workload after one warm-up solve of each (the small command for launch
+    lists of whole solves); prints their iteration counts and times."""
+    import torch
+    import gputensorproductsmoother_b200 as tps
+    from gputensorproductsmoother_b200 import problems
+    dim, k, n, _ = problems.WORKLOADS[args.workload]
+    P = tps.PoissonProblem(dim, k, n)
+    S = tps.MultigridSolvers(P)
+    b = problems.make_rhs(args.workload)
+    x = torch.zeros_like(b)
+    out = {}
+    for prec in ("fp32", "fp64", "fp32", "fp64"):
+        x.zero_()
+        _, rep = S.solve_cg(b, x, precision=prec, rel_tol=1e-10)
+        torch.cuda.synchronize()
+        out[prec] = {"iterations": rep.iterations, "ms": rep.time_ms}
+    print(json.dumps({"mode": "solves", "workload": args.workload, **out}), flush=True)
     P.close()
 
 
@@ -591,6 +613,9 @@ def main():
         return
     if args.mode == "operator":
         run_operator_only(args)
+        return
+    if args.mode == "solves":
+        run_solves_once(args)
         return
     if args.mode == "batch":
         run_batch(args)

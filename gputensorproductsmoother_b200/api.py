@@ -152,6 +152,45 @@ class PoissonProblem:
         L.check(L.lib().tps_mass_vmult(self.handle, dst.data_ptr(), src.data_ptr(), _stream()),
                 self.handle)
 
+    def quadrature_points(self, level: int | None = None):
+        """Coordinates of the QGauss(k+1) points of every cell of the level, in
+        the order tps_assemble_rhs expects: cells lexicographic (x fastest),
+        then the points of a cell lexicographic (x fastest).  Returns dim
+        float64 CUDA tensors (x, y[, z]) of shape (cells, (k+1)^dim)."""
+        import numpy as np
+        lv = self.n_levels - 1 if level is None else level
+        n, k, d = self.cells(lv), self.degree, self.dim
+        xq = 0.5 * (np.polynomial.legendre.leggauss(k + 1)[0] + 1.0)
+        dev = torch.device("cuda", self.device)
+        c = torch.arange(n, dtype=torch.float64, device=dev)
+        q = torch.tensor(xq, dtype=torch.float64, device=dev)
+        t = (c[:, None] + q[None, :]) / n  # (cell, point) per direction
+        if d == 2:
+            xs = t[None, :, None, :].expand(n, n, k + 1, k + 1)
+            ys = t[:, None, :, None].expand(n, n, k + 1, k + 1)
+            return xs.reshape(n * n, -1), ys.reshape(n * n, -1)
+        xs = t[None, None, :, None, None, :].expand(n, n, n, k + 1, k + 1, k + 1)
+        ys = t[None, :, None, None, :, None].expand(n, n, n, k + 1, k + 1, k + 1)
+        zs = t[:, None, None, :, None, None].expand(n, n, n, k + 1, k + 1, k + 1)
+        return xs.reshape(n ** 3, -1), ys.reshape(n ** 3, -1), zs.reshape(n ** 3, -1)
+
+    def assemble_rhs(self, f, level: int | None = None) -> torch.Tensor:
+        """b_i = sum over cells and QGauss(k+1) points of f(x_q) phi_i(x_q) JxW_q
+        on the device (tps_assemble_rhs; the right-hand-side loop of
+        LaplaceOperator::compute_residual, include/laplace_operator.cuh:118-181),
+        Dirichlet rows zero.  f: a callable of the point coordinates
+        (quadrature_points) returning a tensor of the same shape, or the values
+        at the points themselves."""
+        lv = self.n_levels - 1 if level is None else level
+        fq = f if isinstance(f, torch.Tensor) else f(*self.quadrature_points(lv))
+        fq = fq.to(torch.float64).contiguous()
+        nq = (self.degree + 1) ** self.dim * self.cells(lv) ** self.dim
+        if not fq.is_cuda or fq.numel() != nq:
+            raise ValueError(f"f needs {nq} values on the device (cells x Gauss points)")
+        b = self.new_vector(lv)
+        L.check(L.lib().tps_assemble_rhs(self.handle, lv, fq.data_ptr(), b.data_ptr(), _stream()), self.handle)
+        return b
+
     def cell_energy(self, u: torch.Tensor, lam: torch.Tensor) -> torch.Tensor:
         """Per finest-level cell: lambda_c^T A_cell u_c (FP64)."""
         lvl = self.n_levels - 1

@@ -197,9 +197,13 @@ DegreeData make_degree_data(int k)
   gauss_legendre(k + 1, xq, wq);
   D.cmass.assign(np * np, 0.0);
   D.clap.assign(np * np, 0.0);
+  D.qpoint = xq;
+  D.qweight = wq;
+  D.qshape.assign(np * np, 0.0);
   for (int q = 0; q < k + 1; ++q) {
     std::vector<double> v(np), dv(np);
     for (int i = 0; i < np; ++i) lagrange(D.nodes, i, xq[q], v[i], dv[i]);
+    for (int i = 0; i < np; ++i) D.qshape[q * np + i] = v[i];
     for (int i = 0; i < np; ++i)
       for (int j = 0; j < np; ++j) {
         D.cmass[i * np + j] += wq[q] * v[i] * v[j];

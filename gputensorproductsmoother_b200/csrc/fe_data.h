@@ -26,6 +26,9 @@ struct DegreeData {
   std::vector<double> evec;   // m^2, m = 2k-1
   std::vector<double> eval;   // m, ordered like the columns of evec
   std::vector<double> prol;   // (2k+1) x (k+1): coarse basis at child nodes
+  // QGauss(k+1) on [0,1]: points, weights, and the basis at the points
+  // (qshape[q * (k+1) + i] = phi_i(xq_q)), for right-hand-side assembly
+  std::vector<double> qpoint, qweight, qshape;
 };
 
 // Builds every table above for degree k (1 <= k <= kMaxDegree).

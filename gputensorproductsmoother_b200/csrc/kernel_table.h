@@ -79,6 +79,9 @@ struct KernelTable {
                          cudaStream_t);
   cudaError_t (*cell_energy[2])(const LevelGeomH &, const VecLayout &, double *e, const double *u,
                                 const double *lam, cudaStream_t);
+  // b = sum over cells and QGauss(k+1) points of f phi_i JxW, interior rows
+  // (FP64; f at the cells' Gauss points, cells then points lexicographic)
+  cudaError_t (*assemble_rhs[2])(const LevelGeomH &, const VecLayout &, double *b, const double *fq, cudaStream_t);
   // 3D colour step on the tensor cores (FP32 vectors, TF32 operands, FP32
   // accumulation; passes 3: three-term TF32 split, degree 4 only); null for
   // degree 1; needs maps->tc_valid

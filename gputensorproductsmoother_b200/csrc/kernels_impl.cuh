@@ -5,6 +5,7 @@
 
 #include <vector>
 
+#include "assemble.cuh"
 #include "kappa.cuh"
 #include "kernel_table.h"
 #include "laplace.cuh"
@@ -40,6 +41,8 @@ cudaError_t upload_one(const DegreeData &D)
   for (int i = 0; i < M * M; ++i) t.evec[i] = static_cast<T>(D.evec[i]);
   for (int i = 0; i < M; ++i) t.eval[i] = static_cast<T>(D.eval[i]);
   for (int i = 0; i < N1 * NP; ++i) t.prol[i] = static_cast<T>(D.prol[i]);
+  for (int q = 0; q < NP; ++q)
+    for (int i = 0; i < NP; ++i) t.qwshape[q * NP + i] = static_cast<T>(D.qweight[q] * D.qshape[q * NP + i]);
   // folded interior rows of the centro-symmetric patch matrices (FP64, then rounded)
   auto fold = [&](const std::vector<double> &A, T *fe, T *fo) {
     for (int r = 0; r < K; ++r) {
@@ -649,6 +652,28 @@ cudaError_t mass(const LevelGeomH &g, const VecLayout &l, double *dst, const dou
   return cell_sweep<DIM, double, true>(g, l, dst, src, nullptr, hd, st);
 }
 
+// b = sum over cells and Gauss points of f phi_i JxW (interior rows; b zeroed first)
+template <int DIM>
+cudaError_t assemble_rhs(const LevelGeomH &g, const VecLayout &l, double *b, const double *fq, cudaStream_t st)
+{
+  const int64_t n = DIM == 3 ? l.sz * g.N1 : l.sy * g.N1;
+  cudaError_t e = cudaMemsetAsync(b, 0, sizeof(double) * n, st);
+  if (e != cudaSuccess) return e;
+  double hd = 1.0;
+  for (int d = 0; d < DIM; ++d) hd *= g.h;
+  for (int c = 0; c < (1 << DIM); ++c) {
+    const int cx = c & 1, cy = (c >> 1) & 1, cz = (c >> 2) & 1;
+    const int nx = (g.n - cx + 1) / 2, ny = (g.n - cy + 1) / 2, nz = DIM == 3 ? (g.n - cz + 1) / 2 : 1;
+    const int count = nx * ny * nz;
+    if (count == 0) continue;
+    TPS_LAUNCH((assemble_rhs_kernel<DIM, K>), static_cast<unsigned>(ceil_div(count, 128)), 128, 0, st, b, fq, g.n,
+        l.sy, l.sz, cx, cy, cz, nx, ny, count, hd);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
 template <int DIM>
 cudaError_t cell_energy(const LevelGeomH &g, const VecLayout &l, double *e, const double *u,
                         const double *lam, cudaStream_t st)
@@ -733,6 +758,7 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
      {&deg_impl::kappa_smoother<3, double>, &deg_impl::kappa_smoother<3, float>}},
     {&deg_impl::mass<2>, &deg_impl::mass<3>},
     {&deg_impl::cell_energy<2>, &deg_impl::cell_energy<3>},
+    {&deg_impl::assemble_rhs<2>, &deg_impl::assemble_rhs<3>},
 #if TPS_DEGREE >= 2
     &deg_impl::smoother_tc,
 #else

@@ -1438,6 +1438,16 @@ int tps_mass_vmult(tps_handle *h, double *dst, const double *src, void *stream)
   });
 }
 
+int tps_assemble_rhs(tps_handle *h, int level, const double *f_quad, double *b, void *stream)
+{
+  return guarded(h, [&] {
+    check_level(h, level);
+    if (!f_quad || !b) throw ApiError(TPS_ERR_INVALID, "null vector");
+    TPS_CUDA(h->kt->assemble_rhs[h->dim - 2](h->lv[level], lex_layout(h, level), b, f_quad,
+                                             static_cast<cudaStream_t>(stream)));
+  });
+}
+
 int tps_cell_energy(tps_handle *h, const double *u, const double *lam, double *energy, void *stream)
 {
   return guarded(h, [&] {

@@ -62,6 +62,7 @@ struct DegreeTables {
   T evec[Dims<K>::M * Dims<K>::M];      // interior eigenvectors (columns)
   T eval[Dims<K>::M];                   // interior eigenvalues (reference scaling)
   T prol[Dims<K>::N1 * Dims<K>::NP];    // 1D prolongation (child node x coarse basis)
+  T qwshape[Dims<K>::NP * Dims<K>::NP]; // QGauss(k+1) weight times basis: w_q phi_i(x_q), [q][i]
   // even/odd folded interior rows of the centro-symmetric patch matrices A:
   // row r < k-1 (A row r+1, paired with row 2k-1-r):
   //   fe[r][j] = (A[r+1][j] + A[r+1][2k-j])/2 (j < k), fe[r][k] = A[r+1][k]

@@ -205,6 +205,17 @@ int tps_set_kappa(tps_handle *h, const double *kappa_host, int rebuild_coarse);
 /* dst = M src with the finest-level mass matrix (all rows), FP64, device
  * buffers.  Used for b = M f and the gradient dJ/df = M lambda. */
 int tps_mass_vmult(tps_handle *h, double *dst, const double *src, void *stream);
+/* Right-hand-side assembly on the device, the loop of
+ * LaplaceOperator::compute_residual (include/laplace_operator.cuh:118-181, a
+ * host loop over deal.II FEValues there) for a general f:
+ * b_i = sum over the level's cells and their QGauss(k+1) points of
+ * f(x_q) phi_i(x_q) JxW_q, Dirichlet rows zero.  f_quad (FP64 device array)
+ * holds f at the Gauss points: cells lexicographic (x fastest), then the
+ * (k+1)^dim points of the cell lexicographic (x fastest); the Gauss points of
+ * [0,1] are those of orc_gauss/QGauss(k+1) mapped to the cell.  b: FP64,
+ * lexicographic, n_dofs(level) entries.  Deterministic (cells added colour
+ * by colour, no atomics). */
+int tps_assemble_rhs(tps_handle *h, int level, const double *f_quad, double *b, void *stream);
 
 /* energy[c] = lambda_c^T A_cell u_c = int_c grad(lambda).grad(u) for every
  * finest-level cell c (lexicographic cells), FP64: dJ/dkappa_c = -energy[c]

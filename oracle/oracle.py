@@ -334,3 +334,48 @@ def adjoint_gradients(dim, k, n_coarse, n_levels, kappa, f, u_target, rel_tol=1e
     lam, _, _ = H.solve_cg(g, precision=0, symmetric=True, rel_tol=rel_tol, max_it=400)
     lam = zero_dirichlet(lam, dim, N1)
     return u, mass_vmult(dim, k, n, lam), -cell_energy(dim, k, n, u, lam)
+
+
+# ---- right-hand-side assembly (include/laplace_operator.cuh:118-181) ----------
+# b_i = sum over cells and QGauss(k+1) points of f(x_q) phi_i(x_q) JxW_q with
+# f given at the points (cells lexicographic x fastest, then the points of a
+# cell lexicographic x fastest), Dirichlet rows zero.  Restated with numpy from
+# the definitions: Lagrange basis on the Gauss-Lobatto nodes, Gauss rule on [0,1].
+
+
+def _shape_at_gauss(k):
+    nodes = gauss_lobatto_nodes(k)
+    xq, wq = gauss(k + 1)
+    V = np.ones((k + 1, k + 1))
+    for i, xi in enumerate(nodes):
+        for m, xm in enumerate(nodes):
+            if m != i:
+                V[:, i] *= (xq - xm) / (xi - xm)
+    return V, wq
+
+
+def gauss_lobatto_nodes(k):
+    nodes, _, _, _ = fe1d(k)
+    return nodes
+
+
+def assemble_rhs(dim, k, n, fq):
+    V, wq = _shape_at_gauss(k)
+    W = V * wq[:, None]  # [q][i] = w_q phi_i(x_q)
+    N1 = n * k + 1
+    np1 = k + 1
+    h = 1.0 / n
+    f = np.asarray(fq, dtype=np.float64).reshape((n,) * dim + (np1,) * dim)
+    b = np.zeros((N1,) * dim)
+    if dim == 2:
+        loc = np.einsum("qi,pj,yxpq->yxji", W, W, f) * h ** 2  # [cy, cx, iy, ix]
+        for iy in range(np1):
+            for ix in range(np1):
+                b[iy:iy + n * k:k, ix:ix + n * k:k] += loc[:, :, iy, ix]
+    else:
+        loc = np.einsum("qi,pj,rl,zyxrpq->zyxlji", W, W, W, f) * h ** 3
+        for iz in range(np1):
+            for iy in range(np1):
+                for ix in range(np1):
+                    b[iz:iz + n * k:k, iy:iy + n * k:k, ix:ix + n * k:k] += loc[:, :, :, iz, iy, ix]
+    return zero_dirichlet(b.reshape(-1), dim, N1)

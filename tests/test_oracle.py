@@ -234,3 +234,53 @@ def test_oracle_cell_energy_and_mass(oracle, dim, k, n):
         M = np.kron(M, M1)
     f = rng.uniform(-1, 1, N1 ** dim)
     assert np.abs(M @ f - oracle.mass_vmult(dim, k, n, f)).max() <= 1e-15
+
+
+def _quad_points_np(dim, k, n):
+    xq = 0.5 * (np.polynomial.legendre.leggauss(k + 1)[0] + 1.0)
+    t = (np.arange(n)[:, None] + xq[None, :]) / n
+    if dim == 2:
+        xs = np.broadcast_to(t[None, :, None, :], (n, n, k + 1, k + 1))
+        ys = np.broadcast_to(t[:, None, :, None], (n, n, k + 1, k + 1))
+        return xs.reshape(n * n, -1), ys.reshape(n * n, -1)
+    sh = (n, n, n, k + 1, k + 1, k + 1)
+    xs = np.broadcast_to(t[None, None, :, None, None, :], sh)
+    ys = np.broadcast_to(t[None, :, None, None, :, None], sh)
+    zs = np.broadcast_to(t[:, None, None, :, None, None], sh)
+    return xs.reshape(n ** 3, -1), ys.reshape(n ** 3, -1), zs.reshape(n ** 3, -1)
+
+
+@pytest.mark.parametrize("dim,k,n", [(2, 2, 3), (2, 5, 2), (3, 2, 2), (3, 4, 2)])
+def test_oracle_assemble_rhs_pinned(oracle, dim, k, n):
+    """The assembly restatement is pinned twice: for f in Q_k (given at the
+    Gauss points by interpolating nodal values) QGauss(k+1) is exact and
+    b = M f; for the sine-mode right-hand side it equals the 1D-factorised
+    assembly the benchmark inputs use."""
+    import torch
+    from gputensorproductsmoother_b200 import problems
+    N1 = n * k + 1
+    rng = np.random.default_rng(dim * 100 + k)
+    fn = rng.uniform(-1, 1, N1 ** dim)
+    V, _ = oracle._shape_at_gauss(k)
+    F = fn.reshape((N1,) * dim)
+    blocks = []
+    for c in np.ndindex(*((n,) * dim)):
+        sl = tuple(slice(ci * k, ci * k + k + 1) for ci in c)
+        blk = F[sl]
+        if dim == 2:
+            blocks.append(np.einsum("qj,pi,ji->qp", V, V, blk).reshape(-1))
+        else:
+            blocks.append(np.einsum("rl,qj,pi,lji->rqp", V, V, V, blk).reshape(-1))
+    b = oracle.assemble_rhs(dim, k, n, np.stack(blocks))
+    ref = oracle.zero_dirichlet(oracle.mass_vmult(dim, k, n, fn), dim, N1)
+    assert np.abs(b - ref).max() <= 1e-14 * max(1.0, np.abs(ref).max())
+    # sine modes: f = sum_j a_j prod_d sin(f_jd pi x_d), same seed as sine_modes_rhs
+    rs = np.random.default_rng(5)
+    amps = rs.uniform(-1.0, 1.0, 4)
+    freqs = rs.integers(1, 9, size=(4, dim))
+    pts = _quad_points_np(dim, k, n)
+    fq = sum(a * np.prod([np.sin(int(fr[d]) * np.pi * pts[d]) for d in range(dim)], axis=0)
+             for a, fr in zip(amps, freqs))
+    bs = oracle.assemble_rhs(dim, k, n, fq)
+    ref = problems.sine_modes_rhs(dim, k, n, 5, 4, device="cpu").numpy()
+    assert np.abs(bs - ref).max() <= 1e-14 * max(1.0, np.abs(ref).max())
