@@ -9,6 +9,7 @@
 #include "kappa.cuh"
 #include "kernel_table.h"
 #include "laplace.cuh"
+#include "laplace3d_march.cuh"
 #include "smoother.cuh"
 #include "smoother3d.cuh"
 #include "smoother3d_gemm.cuh"
@@ -108,13 +109,13 @@ cudaError_t set_attributes()
     TPS_SET((smoother3d_pair_kernel<K, pp3_warps<K>()>), (Pp3<K, pp3_warps<K>()>::BYTES));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Vmult>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Residual>), (laplace_smem<2, T>()));
-  TPS_SET((laplace3d_stream_kernel<K, T, OpMode::Vmult>), (sizeof(T) * OpStream<K, T>::ELEMS));
-  TPS_SET((laplace3d_stream_kernel<K, T, OpMode::Residual>), (sizeof(T) * OpStream<K, T>::ELEMS));
-  // the streaming operator is shared-memory heavy: prefer the largest carveout
-  e = cudaFuncSetAttribute(laplace3d_stream_kernel<K, T, OpMode::Vmult>,
+  TPS_SET((laplace3d_march_kernel<K, T, OpMode::Vmult>), (sizeof(T) * OpMarch<K, T>::ELEMS));
+  TPS_SET((laplace3d_march_kernel<K, T, OpMode::Residual>), (sizeof(T) * OpMarch<K, T>::ELEMS));
+  // the marching operator is shared-memory heavy: prefer the largest carveout
+  e = cudaFuncSetAttribute(laplace3d_march_kernel<K, T, OpMode::Vmult>,
                            cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(laplace3d_stream_kernel<K, T, OpMode::Residual>,
+  e = cudaFuncSetAttribute(laplace3d_march_kernel<K, T, OpMode::Residual>,
                            cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
   TPS_SET((restrict_xy_kernel<K, T, XYOut::AddInterior>), (restrict_smem<T>()));
@@ -179,19 +180,20 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
 {
   const T scale = static_cast<T>(stiffness_scale(DIM, g.h));
   if constexpr (DIM == 3) {
-    using Sz = OpStream<K, T>;
+    using Sz = OpMarch<K, T>;
     // at least one CTA per SM of a 148-SM part: 8 layers per CTA on 32^3 and
-    // larger Q4 levels, 1 on 16^3 and smaller (measured, us per FP64 apply
-    // with 8 layers vs 1: 16^3 24.7 vs 19.5, 8^3 23.0 vs 19.6; with 2 layers
-    // on 32^3 the recomputed leading layers made it 33.0 -> 39.6)
-    const int cz = opstream_layers<K, T>(g.n, 148);
+    // larger Q4 levels, 1 on 16^3 and smaller (measured with the earlier
+    // streaming kernel, us per FP64 apply with 8 layers vs 1: 16^3 24.7 vs
+    // 19.5, 8^3 23.0 vs 19.6; with 2 layers on 32^3 the recomputed leading
+    // layers made it 33.0 -> 39.6)
+    const int cz = opmarch_layers<K, T>(g.n, 148);
     const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, cz));
     const size_t smem = sizeof(T) * Sz::ELEMS;
     if (mode == 0)
-      TPS_LAUNCH((laplace3d_stream_kernel<K, T, OpMode::Vmult>), grid, Sz::NT, smem, s,
+      TPS_LAUNCH((laplace3d_march_kernel<K, T, OpMode::Vmult>), grid, Sz::NT, smem, s,
           static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, l.sy, l.sz, scale, cz);
     else
-      TPS_LAUNCH((laplace3d_stream_kernel<K, T, OpMode::Residual>), grid, Sz::NT, smem, s,
+      TPS_LAUNCH((laplace3d_march_kernel<K, T, OpMode::Residual>), grid, Sz::NT, smem, s,
           static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1, g.n, l.sy,
           l.sz, scale, cz);
   } else {

@@ -206,213 +206,4 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT, 2)
   (void)OZ;
 }
 
-// ---------------------------------------------------------------------------
-// 3D operator, z-streaming form.  A CTA owns TX x TY cells in x, y and marches
-// through a range of cell layers in z.  Each input plane (with a one-cell xy
-// halo) is contracted once in x (M, L) and once in y, giving the planes
-// T1 = M_y M_x u and T2 = (L_y M_x + M_y L_x) u of the output tile; the z
-// direction is then applied cell by cell: for cell layer c the (k+1)x(k+1)
-// cell matrices act on the k+1 planes ck..(c+1)k of T1 (stiffness) and T2
-// (mass), the k+1 results go to planes ck..(c+1)k, and the last one -- the
-// vertex plane shared with cell c+1 -- is carried in a register to the next
-// layer.  A CTA starts one layer early to form the carry of its first plane,
-// so every input plane is read from memory about (1 + 1/CZ) times in z (xy
-// halo: ((T+1)k+1)^2/(Tk)^2) instead of the brick kernel's full halo in all
-// three directions.  The next layer's k input planes are loaded into
-// registers while the current layer is contracted; each thread's staged xy
-// offsets are computed once, so a prefetched entry costs one add and a load.
-// CTAs per SM the register budget must allow: two (at most 128 registers for
-// 256 threads), which doubles the resident warps of this latency-bound kernel
-// (measured on B200, ms per apply, one CTA vs two: Q4 64^3 FP64 0.255 vs
-// 0.198, FP32 0.136 vs 0.131; Q3 32^3 FP64 0.038 vs 0.024; Q7 32^3 FP64 0.321
-// vs 0.296), except Q7 FP32, which spills 444 bytes under the cap (0.169 vs
-// 0.388 ms) and keeps one
-template <int K, typename T>
-constexpr int opstream_minb()
-{
-#ifdef TPS_OPSTREAM_MINB
-  return TPS_OPSTREAM_MINB(K);
-#else
-  return (K == 7 && sizeof(T) == 4) ? 1 : 2;
-#endif
-}
-template <int K, typename T>
-struct OpStream {
-  static constexpr int TX = K == 1 ? 16 : K == 2 ? 8 : K <= 4 ? 4 : K == 5 ? 3 : 2, TY = TX;  // cells per CTA in x, y
-  static constexpr int OX = TX * K, OY = TY * K;      // output tile
-  static constexpr int WX = (TX + 1) * K + 1, WY = (TY + 1) * K + 1;  // staged plane
-  static constexpr int NT = (OX * OY + 31) / 32 * 32;
-  static constexpr int CZ = 8;                        // cell layers per CTA (at most; see opstream_layers)
-  static constexpr int PL = WX * WY;                  // one staged input plane
-  static constexpr int XS = WY * OX;                  // one x-contracted plane (per product)
-  static constexpr int TS = OY * OX;                  // one xy-contracted plane (per product)
-  // shared memory (elements): IN[K][PL] | X1[K][XS] | X2[K][XS] | T1[K+1][TS] | T2[K+1][TS]
-  static constexpr int OFF_X1 = K * PL, OFF_X2 = OFF_X1 + K * XS, OFF_T1 = OFF_X2 + K * XS;
-  static constexpr int OFF_T2 = OFF_T1 + (K + 1) * TS;
-  static constexpr int ELEMS = OFF_T2 + (K + 1) * TS;
-  static constexpr int EPT = (PL + NT - 1) / NT;      // staged xy entries per thread and plane
-  static constexpr int MINB = opstream_minb<K, T>();   // CTAs per SM the registers must allow
-};
-
-// cell layers per CTA for a level of n cells per direction: the most (up to
-// CZ, fewer leading layers recomputed) that still gives at least `want` CTAs;
-// one on small levels, where a CTA's layer march is the latency
-template <int K, typename T>
-inline int opstream_layers(int n, int want)
-{
-  using S = OpStream<K, T>;
-  const int xy = ((n + S::TX - 1) / S::TX) * ((n + S::TY - 1) / S::TY);
-  for (int cz = S::CZ; cz > 1; cz /= 2)
-    if (xy * ((n + cz - 1) / cz) >= want) return cz;
-  return 1;
-}
-
-template <int K, typename T, OpMode MODE>
-__global__ void __launch_bounds__(OpStream<K, T>::NT, OpStream<K, T>::MINB)
-    laplace3d_stream_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs,
-                            int N1g, int n_cells, int64_t sy, int64_t sz, T scale, int cz)
-{
-  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
-  using S = OpStream<K, T>;
-  constexpr int NT = S::NT, WX = S::WX, WY = S::WY, OX = S::OX, OY = S::OY, PL = S::PL;
-  constexpr int XS = S::XS, TS = S::TS, EPT = S::EPT;
-  const DegreeTables<K, T> &tb = c_tables<K, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sm = reinterpret_cast<T *>(smem_raw);
-  T *IN = sm, *X1 = sm + S::OFF_X1, *X2 = sm + S::OFF_X2, *T1 = sm + S::OFF_T1, *T2 = sm + S::OFF_T2;
-  const int tid = threadIdx.x;
-  const int cx0 = blockIdx.x * S::TX, cy0 = blockIdx.y * S::TY;
-  const int gx0 = (cx0 - 1) * K, gy0 = (cy0 - 1) * K;  // staged plane origin
-  const int cz_begin = blockIdx.z * cz;  // cz cell layers per CTA
-  const int cz_end = min(cz_begin + cz, n_cells);
-  const int c_first = cz_begin > 0 ? cz_begin - 1 : 0;  // leading layer: carry only
-
-  // this thread's staged xy entries (fixed for every plane): global xy offset
-  // and whether the entry lies in the mesh
-  int64_t xoff[EPT];
-  bool xok[EPT];
-#pragma unroll
-  for (int j = 0; j < EPT; ++j) {
-    const int l = tid + j * NT, lx = l % WX, ly = l / WX;
-    const int gx = gx0 + lx, gy = gy0 + ly;
-    xok[j] = l < PL && gx >= 0 && gx < N1g && gy >= 0 && gy < N1g;
-    xoff[j] = xok[j] ? gx + gy * sy : 0;
-  }
-  // load planes z0 .. z0+np-1 (np <= K) of the staged tile into registers
-  T pre[K][EPT];
-  auto prefetch = [&](int z0, int np) {
-#pragma unroll
-    for (int p = 0; p < K; ++p) {
-      const int gz = z0 + p;
-      const bool zok = p < np && gz >= 0 && gz < N1g;
-#pragma unroll
-      for (int j = 0; j < EPT; ++j) pre[p][j] = (zok && xok[j]) ? __ldg(&src[xoff[j] + gz * sz]) : T(0);
-    }
-  };
-  auto commit = [&]() {
-#pragma unroll
-    for (int p = 0; p < K; ++p)
-#pragma unroll
-      for (int j = 0; j < EPT; ++j) {
-        const int l = tid + j * NT;
-        if (l < PL) IN[p * PL + l] = pre[p][j];
-      }
-  };
-  // x then y contraction of staged planes 0..np-1 into T slots slot0.. (mod K+1)
-  auto contract_xy = [&](int np, int slot0) {
-    for (int t = tid; t < np * WY * S::TX; t += NT) {
-      const int c = t % S::TX, r = t / S::TX;  // r = p * WY + y
-      const T *s = IN + (r / WY) * PL + (r % WY) * WX + c * K;
-      T v[2 * K + 1], o1[K], o2[K];
-#pragma unroll
-      for (int j = 0; j <= 2 * K; ++j) v[j] = s[j];
-      band_apply<K, T>(tb.cmass, v, o1);
-      band_apply<K, T>(tb.clap, v, o2);
-      T *d1 = X1 + r * OX + c * K, *d2 = X2 + r * OX + c * K;
-#pragma unroll
-      for (int a = 0; a < K; ++a) {
-        d1[a] = o1[a];
-        d2[a] = o2[a];
-      }
-    }
-    __syncthreads();
-    for (int t = tid; t < np * OX * S::TY; t += NT) {
-      const int xo = t % OX, r = t / OX;  // r = p * TY + cell row
-      const int p = r / S::TY, c = r % S::TY;
-      const T *s1 = X1 + p * XS + c * K * OX + xo, *s2 = X2 + p * XS + c * K * OX + xo;
-      T v1[2 * K + 1], v2[2 * K + 1], o1[K], o2[K], o3[K];
-#pragma unroll
-      for (int j = 0; j <= 2 * K; ++j) {
-        v1[j] = s1[j * OX];
-        v2[j] = s2[j * OX];
-      }
-      band_apply<K, T>(tb.cmass, v1, o1);
-      band_apply<K, T>(tb.clap, v1, o2);
-      band_apply<K, T>(tb.cmass, v2, o3);
-      const int slot = (slot0 + p) % (K + 1);
-      T *d1 = T1 + slot * TS + c * K * OX + xo, *d2 = T2 + slot * TS + c * K * OX + xo;
-#pragma unroll
-      for (int a = 0; a < K; ++a) {
-        d1[a * OX] = o1[a];
-        d2[a * OX] = o2[a] + o3[a];
-      }
-    }
-    __syncthreads();
-  };
-
-  // prime: plane c_first*K into slot 0
-  int base = 0;  // slot of plane c*K
-  prefetch(c_first * K, 1);
-  commit();
-  __syncthreads();
-  contract_xy(1, base);
-  prefetch(c_first * K + 1, K);  // the first layer's new planes
-  const int tx = tid % OX, ty = tid / OX;
-  const bool owner = tid < OX * OY;
-  const int gx = cx0 * K + tx, gy = cy0 * K + ty;
-  const bool xy_in = owner && gx > 0 && gx < N1g - 1 && gy > 0 && gy < N1g - 1;
-  T carry = T(0);
-  for (int c = c_first; c < cz_end; ++c) {
-    commit();
-    __syncthreads();
-    if (c + 1 < cz_end) prefetch((c + 1) * K + 1, K);  // next layer, overlapped with the contractions
-    contract_xy(K, base + 1);
-    // z: cell matrices on planes cK..(c+1)K
-    if (owner) {
-      T u1[K + 1], u2[K + 1];
-#pragma unroll
-      for (int b = 0; b <= K; ++b) {
-        const int slot = (base + b) % (K + 1);
-        u1[b] = T1[slot * TS + ty * OX + tx];
-        u2[b] = T2[slot * TS + ty * OX + tx];
-      }
-      T out[K + 1];
-#pragma unroll
-      for (int a = 0; a <= K; ++a) {
-        T acc = T(0);
-#pragma unroll
-        for (int b = 0; b <= K; ++b) acc += tb.clap[a * (K + 1) + b] * u1[b] + tb.cmass[a * (K + 1) + b] * u2[b];
-        out[a] = acc;
-      }
-      out[0] += carry;
-      carry = out[K];
-      if (c >= cz_begin && xy_in) {
-#pragma unroll
-        for (int a = 0; a < K; ++a) {
-          const int gz = c * K + a;
-          if (gz < 1 || gz > N1g - 2) continue;
-          const int64_t gi = gx + gy * sy + gz * sz;
-          const T val = scale * out[a];
-          if constexpr (MODE == OpMode::Vmult)
-            dst[gi] = val;
-          else
-            dst[gi] = rhs[gi] - val;
-        }
-      }
-    }
-    base = (base + K) % (K + 1);
-    __syncthreads();  // the T slots of this layer's first planes are refilled next
-  }
-}
-
 }  // namespace tps

@@ -235,4 +235,28 @@ __device__ __forceinline__ float to_tf32(float v)
   return __uint_as_float(r);
 }
 
+// ---- asynchronous global -> shared element copies (cp.async) -----------------
+
+// copy BYTES (4 or 8) from gmem to smem, or write zeros when !valid (the
+// source is then not read; callers still pass an address inside the buffer)
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill(void *smem, const void *gmem, bool valid)
+{
+  static_assert(BYTES == 4 || BYTES == 8 || BYTES == 16, "cp.async size");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(smem_u32(smem)), "l"(gmem), "n"(BYTES),
+               "r"(valid ? BYTES : 0)
+               : "memory");
+}
+// the same with the shared address as a 32-bit shared-window offset and the
+// number of source bytes (BYTES, or 0 for zero fill) precomputed by the caller
+template <int BYTES>
+__device__ __forceinline__ void cp_async_zfill_s(uint32_t saddr, const void *gmem, uint32_t src_bytes)
+{
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;" ::"r"(saddr), "l"(gmem), "n"(BYTES), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+// this thread's copies of all committed groups have landed in shared memory
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 }  // namespace tps
