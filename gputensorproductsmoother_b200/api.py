@@ -104,13 +104,23 @@ class PoissonProblem:
         return ms.value
 
     def autotune(self, dtype: str = "fp32") -> list[int]:
-        """Time the 3D smoother's kernel variants on every level and keep the
-        fastest; returns the chosen patches per batch per level (-1: the
-        one-warp-per-patch kernel, -2: two patches per warp in packed FP32)."""
+        """Time the 3D smoother's kernel variants and the operator's tile
+        depths on every level and keep the fastest; returns the chosen patches
+        per batch per level (-1: the one-warp-per-patch kernel, -2: two
+        patches per warp in packed FP32)."""
         out = (ctypes.c_int * self.n_levels)()
         L.check(L.lib().tps_autotune(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], out),
                 self.handle)
         return list(out)
+
+    def operator_layers(self, level: int | None = None, dtype: str = "fp32") -> int:
+        """Cell layers per CTA of the 3D operator on a level (set by autotune;
+        0 = the library's rule)."""
+        lv = self.n_levels - 1 if level is None else level
+        out = ctypes.c_int()
+        L.check(L.lib().tps_get_operator_layers(self.handle, {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype], lv,
+                                                ctypes.byref(out)), self.handle)
+        return out.value
 
     def smoother_variants(self, dtype: str = "fp32") -> list[int]:
         """Patches per batch of each compiled 3D smoother variant (index =

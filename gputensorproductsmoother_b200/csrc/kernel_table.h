@@ -46,9 +46,10 @@ struct KernelTable {
   // copy the 1D tables of this degree into constant memory of the current device
   cudaError_t (*upload)(const DegreeData &);
   // dst = A src on interior rows (mode 0) or dst = rhs - A src (mode 1);
-  // boundary rows of dst are not written
+  // boundary rows of dst are not written; layers (3D): cell layers per CTA
+  // of the z-marching kernel, 1, 2, 4 or 8, or 0 for the default rule
   cudaError_t (*laplace[2][2])(const LevelGeomH &, const VecLayout &, void *dst, const void *src,
-                               const void *rhs, int mode, cudaStream_t);
+                               const void *rhs, int mode, int layers, cudaStream_t);
   // one colour of the patch sweep; maps (3D, TMA path) may be null; zero_x
   // declares x == 0 on entry; variant selects the 3D kernel shape
   // (0 default, 1 half, 2 quarter batch, 3 one warp per patch; see

@@ -176,7 +176,7 @@ cudaError_t upload(const DegreeData &D)
 
 template <int DIM, typename T>
 cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const void *src,
-                    const void *rhs, int mode, cudaStream_t s)
+                    const void *rhs, int mode, int layers, cudaStream_t s)
 {
   const T scale = static_cast<T>(stiffness_scale(DIM, g.h));
   if constexpr (DIM == 3) {
@@ -186,7 +186,7 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
     // streaming kernel, us per FP64 apply with 8 layers vs 1: 16^3 24.7 vs
     // 19.5, 8^3 23.0 vs 19.6; with 2 layers on 32^3 the recomputed leading
     // layers made it 33.0 -> 39.6)
-    const int cz = opmarch_layers<K, T>(g.n, 148);
+    const int cz = layers > 0 ? layers : opmarch_layers<K, T>(g.n, 148);
     const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, cz));
     const size_t smem = sizeof(T) * Sz::ELEMS;
     if (mode == 0)

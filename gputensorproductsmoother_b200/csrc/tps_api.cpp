@@ -194,6 +194,7 @@ struct tps_handle {
   std::vector<int> coarse_coord;        // (x, y, z) of each interior coarse DoF
   VcycleVectors vc[2];  // [0] FP64, [1] FP32
   std::vector<int> sm_variant[2];  // per level: 3D smoother patches-per-batch variant (autotuned)
+  std::vector<int> op_layers[2];   // per level: 3D operator cell layers per CTA (autotuned; 0 default)
   DevBuf err_flag;      // set by a kernel whose bounded wait gave up
   Mailbox mbox;         // small device results (CG scalars, dots, the error flag) for the host
   // variable coefficient: per-level per-cell kappa (fine given, coarse = mean of children)
@@ -428,10 +429,16 @@ int default_variant(const tps_handle *h, int level, int p)
   if (h->dim != 3) return 0;
   const int64_t c = h->lv[level].n / 2;  // patches per direction of colour 0
   const bool large = c * c * c >= 4096;
+  // levels whose colours hold fewer patches are latency-bound: half CTA
+  // batches in FP32 and, at degree 3, quarter batches in FP64 (measured on
+  // B200, us per sweep, default / half / quarter batch / warp per patch:
+  // Q4 FP32 16^3 37.0 / 36.9 / 39.3 / 40.5, 8^3 35.3 / 31.2 / 33.7 / 37.4,
+  // 4^3 33.6 / 29.6 / 31.8 / 35.4; Q3 FP64 16^3 33.0 / 32.1 / 31.8 / 34.9)
+  if (!large) return p == 1 ? 1 : (h->k == 3 ? 2 : 0);
   if (p == 1 && h->k >= 2 && h->k <= 4 && h->kt->smoother_ppb(3, 1, 4) == -2 && h->kt->smoother_ppb(3, 1, 3) == -1)
-    return large ? 4 : 3;
+    return 4;
   if ((h->k != 3 && h->k != 4) || h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 3) != -1) return 0;
-  return large ? 3 : 0;
+  return 3;
 }
 
 // one coloured sweep; x_zero declares x == 0 on entry (the first colour then
@@ -470,7 +477,10 @@ void level_laplace(tps_handle *h, int level, int p, const VecLayout &lay, void *
     TPS_CUDA(h->kt->kappa_laplace[h->dim - 2][p](h->lv[level], lay, dst, src, rhs,
                                                  h->kappa_dev[p][level]->p, mode, s));
   else
-    TPS_CUDA(h->kt->laplace[h->dim - 2][p](h->lv[level], lay, dst, src, rhs, mode, s));
+    TPS_CUDA(h->kt->laplace[h->dim - 2][p](h->lv[level], lay, dst, src, rhs, mode,
+                                           level < static_cast<int>(h->op_layers[p].size())
+                                               ? h->op_layers[p][level] : 0,
+                                           s));
 }
 
 // per-level coefficients from the finest-level kappa (coarse = mean of the 2^d
@@ -892,32 +902,59 @@ void apply_vcycle64(tps_handle *h, int precision, bool symmetric, double *dst, c
 }
 
 
-// Patches-per-batch autotuner of the 3D smoother: every level of precision p
-// times each compiled variant on the V-cycle work vectors (one warm-up sweep,
-// then the best of three timed sweeps) and keeps the fastest.
+// best of three timed runs of fn on stream s (after one untimed run), ms
+template <class F>
+float best_of_three(tps_handle *h, cudaStream_t s, F &&fn)
+{
+  fn();
+  float t = 1e30f;
+  for (int r = 0; r < 3; ++r) {
+    TPS_CUDA(cudaEventRecord(h->ev0, s));
+    fn();
+    TPS_CUDA(cudaEventRecord(h->ev1, s));
+    TPS_CUDA(cudaEventSynchronize(h->ev1));
+    float ms = 0.f;
+    TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+    t = ms < t ? ms : t;
+  }
+  return t;
+}
+
+// Autotuner of the 3D level kernels of precision p, on the V-cycle work
+// vectors: per level, the smoother's patches-per-batch variant (one sweep per
+// candidate) and the operator's tile depth in z (cell layers per CTA of the
+// z-marching kernel, one residual per candidate); the fastest of each is kept.
 void autotune_levels(tps_handle *h, int p, cudaStream_t s)
 {
   VcycleVectors &V = vcycle_vectors(h, p);
   ensure_krylov(h);
   h->sm_variant[p].assign(h->n_levels, 0);
+  h->op_layers[p].assign(h->n_levels, 0);
   if (h->dim != 3 || h->has_kappa) return;
+  for (int l = 0; l < h->n_levels; ++l) {
+    float best_op = 1e30f;
+    int bz = 0;
+    for (int cz = 1; cz <= 8 && cz <= h->lv[l].n; cz *= 2) {
+      h->op_layers[p][l] = cz;
+      const float t = best_of_three(h, s, [&] {
+        level_laplace(h, l, p, V.layout[l], V.t[l]->p, V.su[l]->p, V.d[l]->p, 1, s);
+      });
+      if (t < best_op) {
+        best_op = t;
+        bz = cz;
+      }
+    }
+    h->op_layers[p][l] = bz;
+  }
   for (int l = 0; l < h->n_levels; ++l) {
     float best = 1e30f;
     int bv = 0;
     for (int v = 0; v < kSmootherVariants; ++v) {
       if (v > 0 && h->kt->smoother_ppb(3, p == 0 ? 0 : 1, v) == h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 0)) continue;
       h->sm_variant[p][l] = v;
-      smoother_sweep(h, l, p, V.layout[l], V.su[l]->p, V.d[l]->p, false, false, &V.maps[l], s);
-      float t = 1e30f;
-      for (int r = 0; r < 3; ++r) {
-        TPS_CUDA(cudaEventRecord(h->ev0, s));
+      const float t = best_of_three(h, s, [&] {
         smoother_sweep(h, l, p, V.layout[l], V.su[l]->p, V.d[l]->p, false, false, &V.maps[l], s);
-        TPS_CUDA(cudaEventRecord(h->ev1, s));
-        TPS_CUDA(cudaEventSynchronize(h->ev1));
-        float ms = 0.f;
-        TPS_CUDA(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
-        t = ms < t ? ms : t;
-      }
+      });
       if (t < best) {
         best = t;
         bv = v;
@@ -1514,6 +1551,16 @@ int tps_get_smoother_variant(tps_handle *h, int dtype, int level, int *variant)
   });
 }
 
+int tps_get_operator_layers(tps_handle *h, int dtype, int level, int *layers)
+{
+  return guarded(h, [&] {
+    const int p = dt_index(dtype);
+    check_level(h, level);
+    if (!layers) throw ApiError(TPS_ERR_INVALID, "null output");
+    *layers = level < static_cast<int>(h->op_layers[p].size()) ? h->op_layers[p][level] : 0;
+  });
+}
+
 int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level)
 {
   return guarded(h, [&] {
@@ -1854,7 +1901,8 @@ void batch_build(tps_batch *B, const tps_solve_opts &o, const double *const *b, 
     vcycle_vectors(h, p);
     ensure_krylov(h);
   }
-  // patches-per-batch autotuning, once per distinct hierarchy of the batch
+  // autotuning (smoother variants, operator tile depth), once per distinct
+  // hierarchy of the batch
   for (int i = 0; i < n; ++i) {
     tps_handle *h = B->sys[i];
     if (static_cast<int>(h->sm_variant[p].size()) == h->n_levels) continue;
@@ -1865,9 +1913,10 @@ void batch_build(tps_batch *B, const tps_solve_opts &o, const double *const *b, 
           static_cast<int>(o2->sm_variant[p].size()) == o2->n_levels)
         break;
     }
-    if (j < i)
+    if (j < i) {
       h->sm_variant[p] = B->sys[j]->sm_variant[p];
-    else
+      h->op_layers[p] = B->sys[j]->op_layers[p];
+    } else
       autotune_levels(h, p, s);
   }
   std::vector<CGScalars *> scp(n);

@@ -254,13 +254,21 @@ int tps_solve_host_guess(tps_handle *h, const tps_solve_opts *opts, const double
 int tps_solve_host_many(tps_handle *h, const tps_solve_opts *opts, int n, const double *const *b_host,
                         double *const *x_host, tps_report *reports);
 
-/* Patches-per-batch autotuner of the 3D smoother (the reference's
- * AdditionalData::patch_per_block, include/patch_smoother.cuh:101-118, chosen
- * by timing): every level of the dtype's V-cycle times each compiled variant
- * and keeps the fastest for later sweeps and V-cycles of this handle.
- * ppb_per_level (n_levels entries, may be null) receives the chosen values
- * (0 in 2D, -1 for the one-warp-per-patch kernel).  Batched solves tune their systems automatically. */
+/* Autotuner of the 3D level kernels (the reference's
+ * AdditionalData::patch_per_block, include/patch_smoother.cuh:101-118, fixed
+ * there, chosen here by timing): on every level of the dtype's V-cycle it times
+ * each compiled smoother variant (patches per CTA batch, one warp per patch,
+ * two patches per warp) and each tile depth of the operator (1, 2, 4 or 8
+ * cell layers per CTA of the z-marching kernel), and keeps the fastest of each
+ * for later sweeps, operator applications and V-cycles of this handle.
+ * ppb_per_level (n_levels entries, may be null) receives the chosen smoother
+ * values (0 in 2D, -1 for one warp per patch, -2 for two patches per warp).
+ * Batched solves tune their systems automatically. */
 int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
+/* The operator tile depth a level of the dtype's V-cycle uses: the cell layers
+ * per CTA that tps_autotune chose, or 0 for the library's rule (8 layers, fewer
+ * where a level would have fewer than 148 CTAs). */
+int tps_get_operator_layers(tps_handle *h, int dtype, int level, int *layers);
 /* The compiled variants of the 3D smoother, TPS_SMOOTHER_VARIANTS entries:
  * patches per CTA batch 0 default, 1 half, 2 quarter, 3 one warp per patch
  * (reported as -1 where it is compiled) and 4 two patches per warp in packed
@@ -273,8 +281,10 @@ int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
 int tps_smoother_variants(tps_handle *h, int dtype, int *ppb);
 int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant);
 /* The variant a level's sweeps use now: the one set or autotuned, else the
- * library default (one warp per patch for degrees 3 and 4 when a colour
- * holds at least 4096 patches, else the default CTA batch). */
+ * library default: where a colour holds at least 4096 patches, two patches
+ * per warp (FP32, degrees 2..4) or one warp per patch (FP64, degrees 3 and
+ * 4), else the default CTA batch; on smaller levels half CTA batches in FP32
+ * and, at degree 3, quarter batches in FP64. */
 int tps_get_smoother_variant(tps_handle *h, int dtype, int level, int *variant);
 
 /* ---- batched solves (no reference counterpart) ----------------------------

@@ -77,3 +77,26 @@ def test_autotune_keeps_results(cuda):
     x, rep = MG.solve_cg(bb, precision="fp32", rel_tol=1e-10)
     assert rep.converged
     assert P.autotune("fp64")[0] in (-1, 1, 2, 4, 8, 16)
+
+
+def test_autotune_operator_tile_depth_keeps_results(cuda):
+    """The autotuner also picks the operator's cell layers per CTA (1, 2, 4 or
+    8, at most the level's cells); every output is formed by the same
+    arithmetic whatever the tile depth, so mixed and FP64 solves after tuning
+    are bit-identical to the untuned ones."""
+    P = tps.PoissonProblem(3, 4, 16)
+    N1 = 65
+    bb = interior_random(3, N1, 4)
+    MG = tps.MultigridSolvers(P)
+    ref = {p: MG.solve_cg(bb, precision=p, rel_tol=1e-10) for p in ("fp32", "fp64")}
+    assert all(P.operator_layers(lv, dt) == 0 for lv in range(P.n_levels) for dt in ("fp32", "fp64"))
+    P.autotune("fp32")
+    P.autotune("fp64")
+    for dt in ("fp32", "fp64"):
+        for lv in range(P.n_levels):
+            cz = P.operator_layers(lv, dt)
+            assert cz in (1, 2, 4, 8) and cz <= P.cells(lv), (dt, lv, cz)
+    for p in ("fp32", "fp64"):
+        x, rep = MG.solve_cg(bb, precision=p, rel_tol=1e-10)
+        assert rep.iterations == ref[p][1].iterations
+        assert torch.equal(x, ref[p][0]), p
