@@ -177,6 +177,19 @@ __global__ void __launch_bounds__(kRedThreads) finalize_kernel(const double *par
   if (threadIdx.x == 0) op(sc, v);
 }
 
+// sums `count` partial values in a fixed order in one CTA and applies `op`
+template <typename Op>
+__global__ void __launch_bounds__(kRedThreads) finalize_count_kernel(const double *partial, int count,
+                                                                     CGScalars *sc, Op op)
+{
+  griddep_wait();  // programmatic launch: the previous kernel's writes are visible
+  __shared__ double sh[32];
+  double s = 0.0;
+  for (int i = threadIdx.x; i < count; i += kRedThreads) s += partial[i];
+  double v[1] = {block_sum<kRedThreads>(s, sh)};
+  if (threadIdx.x == 0) op(sc, v);
+}
+
 struct OpInit {
   __device__ void operator()(CGScalars *sc, const double *v) const
   {
@@ -407,6 +420,11 @@ cudaError_t launch_cg_first_direction(double *p, const void *z, int z_kind, PadM
 cudaError_t launch_cg_finalize_rz(const double *partial, CGScalars *sc, cudaStream_t s)
 {
   TPS_LAUNCH((finalize_kernel<1, OpRz>), 1, kRedThreads, 0, s, partial, sc, OpRz{});
+  return cudaGetLastError();
+}
+cudaError_t launch_cg_alpha_partials(const double *partial, int count, CGScalars *sc, cudaStream_t s)
+{
+  TPS_LAUNCH((finalize_count_kernel<OpAlpha>), 1, kRedThreads, 0, s, partial, count, sc, OpAlpha{});
   return cudaGetLastError();
 }
 cudaError_t launch_cg_alpha(const double *p, const double *q, int64_t n, double *partial,

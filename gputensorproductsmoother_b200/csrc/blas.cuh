@@ -76,6 +76,9 @@ cudaError_t launch_cg_first_direction(double *p, const void *z, int z_kind, PadM
                                       const double *r, int64_t n, double *partial, cudaStream_t s);
 cudaError_t launch_cg_finalize_rz(const double *partial, CGScalars *sc, cudaStream_t s);
 // partial(p.q) then alpha = rz / pq
+// alpha from `count` partial sums of p.q formed elsewhere (the fused
+// operator kernel), summed in a fixed order
+cudaError_t launch_cg_alpha_partials(const double *partial, int count, CGScalars *sc, cudaStream_t s);
 cudaError_t launch_cg_alpha(const double *p, const double *q, int64_t n, double *partial,
                             CGScalars *sc, cudaStream_t s);
 // x += alpha p, r -= alpha q, d = conv(r), partial(r.r)

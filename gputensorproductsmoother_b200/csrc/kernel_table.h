@@ -83,6 +83,12 @@ struct KernelTable {
   // b = sum over cells and QGauss(k+1) points of f phi_i JxW, interior rows
   // (FP64; f at the cells' Gauss points, cells then points lexicographic)
   cudaError_t (*assemble_rhs[2])(const LevelGeomH &, const VecLayout &, double *b, const double *fq, cudaStream_t);
+  // 3D FP64 q = A p (z-marching kernel) with the p.q partial sums of a CG step
+  // fused: one per CTA into partial (at most capacity), *ctas = their count
+  cudaError_t (*laplace3d_dot)(const LevelGeomH &, const VecLayout &, void *dst, const void *src,
+                               double *partial, int capacity, int layers, int *ctas, cudaStream_t);
+  // the most CTAs laplace3d_dot launches on a level of n cells
+  int (*laplace3d_ctas)(int n);
   // 3D colour step on the tensor cores (FP32 vectors, TF32 operands, FP32
   // accumulation; passes 3: three-term TF32 split, degree 4 only); null for
   // degree 1; needs maps->tc_valid

@@ -109,15 +109,21 @@ cudaError_t set_attributes()
     TPS_SET((smoother3d_pair_kernel<K, pp3_warps<K>()>), (Pp3<K, pp3_warps<K>()>::BYTES));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Vmult>), (laplace_smem<2, T>()));
   TPS_SET((laplace_kernel<2, K, T, OpMode::Residual>), (laplace_smem<2, T>()));
-  TPS_SET((laplace3d_march_kernel<K, T, OpMode::Vmult>), (sizeof(T) * OpMarch<K, T>::ELEMS));
-  TPS_SET((laplace3d_march_kernel<K, T, OpMode::Residual>), (sizeof(T) * OpMarch<K, T>::ELEMS));
+  TPS_SET((laplace3d_march_kernel<K, T, OpMode::Vmult, false>), (sizeof(T) * OpMarch<K, T>::ELEMS));
+  TPS_SET((laplace3d_march_kernel<K, T, OpMode::Residual, false>), (sizeof(T) * OpMarch<K, T>::ELEMS));
   // the marching operator is shared-memory heavy: prefer the largest carveout
-  e = cudaFuncSetAttribute(laplace3d_march_kernel<K, T, OpMode::Vmult>,
+  e = cudaFuncSetAttribute(laplace3d_march_kernel<K, T, OpMode::Vmult, false>,
                            cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(laplace3d_march_kernel<K, T, OpMode::Residual>,
+  e = cudaFuncSetAttribute(laplace3d_march_kernel<K, T, OpMode::Residual, false>,
                            cudaFuncAttributePreferredSharedMemoryCarveout, 100);
   if (e != cudaSuccess) return e;
+  if constexpr (sizeof(T) == 8) {
+    TPS_SET((laplace3d_march_kernel<K, T, OpMode::Vmult, true>), (sizeof(T) * OpMarch<K, T>::ELEMS));
+    e = cudaFuncSetAttribute(laplace3d_march_kernel<K, T, OpMode::Vmult, true>,
+                             cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (e != cudaSuccess) return e;
+  }
   TPS_SET((restrict_xy_kernel<K, T, XYOut::AddInterior>), (restrict_smem<T>()));
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetInterior>), (restrict_smem<T>()));
   TPS_SET((restrict_xy_kernel<K, T, XYOut::SetAll>), (restrict_smem<T>()));
@@ -190,12 +196,13 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
     const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, cz));
     const size_t smem = sizeof(T) * Sz::ELEMS;
     if (mode == 0)
-      TPS_LAUNCH((laplace3d_march_kernel<K, T, OpMode::Vmult>), grid, Sz::NT, smem, s,
-          static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, l.sy, l.sz, scale, cz);
+      TPS_LAUNCH((laplace3d_march_kernel<K, T, OpMode::Vmult, false>), grid, Sz::NT, smem, s,
+          static_cast<T *>(dst), static_cast<const T *>(src), nullptr, g.N1, g.n, l.sy, l.sz, scale, cz,
+          nullptr);
     else
-      TPS_LAUNCH((laplace3d_march_kernel<K, T, OpMode::Residual>), grid, Sz::NT, smem, s,
+      TPS_LAUNCH((laplace3d_march_kernel<K, T, OpMode::Residual, false>), grid, Sz::NT, smem, s,
           static_cast<T *>(dst), static_cast<const T *>(src), static_cast<const T *>(rhs), g.N1, g.n, l.sy,
-          l.sz, scale, cz);
+          l.sz, scale, cz, nullptr);
   } else {
     using Tl = OpTile<DIM, K>;
     const dim3 grid(ceil_div(g.n, Tl::CX), ceil_div(g.n, Tl::CY), 1);
@@ -655,6 +662,30 @@ cudaError_t mass(const LevelGeomH &g, const VecLayout &l, double *dst, const dou
 }
 
 // b = sum over cells and Gauss points of f phi_i JxW (interior rows; b zeroed first)
+// 3D FP64 q = A p with the CG's p.q partial sums fused (one per CTA into
+// partial, at most `capacity`; *ctas receives their count)
+cudaError_t laplace3d_dot(const LevelGeomH &g, const VecLayout &l, void *dst, const void *src, double *partial,
+                          int capacity, int layers, int *ctas, cudaStream_t s)
+{
+  using Sz = OpMarch<K, double>;
+  const int cz = layers > 0 ? layers : opmarch_layers<K, double>(g.n, 148);
+  const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, cz));
+  const int64_t count = int64_t(grid.x) * grid.y * grid.z;
+  if (count > capacity) return cudaErrorInvalidValue;
+  *ctas = static_cast<int>(count);
+  TPS_LAUNCH((laplace3d_march_kernel<K, double, OpMode::Vmult, true>), grid, Sz::NT, sizeof(double) * Sz::ELEMS,
+      s, static_cast<double *>(dst), static_cast<const double *>(src), nullptr, g.N1, g.n, l.sy, l.sz,
+      stiffness_scale(3, g.h), cz, partial);
+  return cudaGetLastError();
+}
+
+// the most CTAs laplace3d_dot launches on a level of n cells (one layer per CTA)
+int laplace3d_ctas(int n)
+{
+  using Sz = OpMarch<K, double>;
+  return ceil_div(n, Sz::TX) * ceil_div(n, Sz::TY) * n;
+}
+
 template <int DIM>
 cudaError_t assemble_rhs(const LevelGeomH &g, const VecLayout &l, double *b, const double *fq, cudaStream_t st)
 {
@@ -761,6 +792,8 @@ const KernelTable TPS_CAT(kernel_table_k, TPS_DEGREE) = {
     {&deg_impl::mass<2>, &deg_impl::mass<3>},
     {&deg_impl::cell_energy<2>, &deg_impl::cell_energy<3>},
     {&deg_impl::assemble_rhs<2>, &deg_impl::assemble_rhs<3>},
+    &deg_impl::laplace3d_dot,
+    &deg_impl::laplace3d_ctas,
 #if TPS_DEGREE >= 2
     &deg_impl::smoother_tc,
 #else

@@ -78,11 +78,11 @@ struct OpMarch {
 };
 
 // CTAs per SM the registers must allow (no spills at these caps; the FP64
-// residual holds b of the layer's outputs as well)
-template <int K, typename T, OpMode MODE>
+// residual and the fused dot hold b or p of the layer's outputs as well)
+template <int K, typename T, OpMode MODE, bool DOT>
 constexpr int march_minb()
 {
-  if constexpr (sizeof(T) == 8) return K <= 3 ? 4 : K == 4 ? (MODE == OpMode::Vmult ? 4 : 3) : 2;
+  if constexpr (sizeof(T) == 8) return K <= 3 ? 4 : K == 4 ? (MODE == OpMode::Vmult && !DOT ? 4 : 3) : 2;
   return K <= 6 ? 4 : 3;
 }
 
@@ -240,11 +240,15 @@ __device__ __forceinline__ void march_y_task(const T *X1, const T *X2, T *T1, T 
   }
 }
 
-template <int K, typename T, OpMode MODE>
-__global__ void __launch_bounds__(OpMarch<K, T>::NT, march_minb<K, T, MODE>())
+// DOT (Vmult only): every CTA also forms the sum of src * dst over the
+// outputs it writes and stores it to dotp[CTA index]: the p.q of a CG step
+// without a second pass over both vectors (fixed summation order)
+template <int K, typename T, OpMode MODE, bool DOT>
+__global__ void __launch_bounds__(OpMarch<K, T>::NT, march_minb<K, T, MODE, DOT>())
     laplace3d_march_kernel(T *__restrict__ dst, const T *__restrict__ src, const T *__restrict__ rhs, int N1g,
-                           int n_cells, int64_t sy, int64_t sz, T scale, int cz)
+                           int n_cells, int64_t sy, int64_t sz, T scale, int cz, double *__restrict__ dotp)
 {
+  static_assert(!DOT || MODE == OpMode::Vmult, "the fused dot belongs to q = A p");
   griddep_wait();  // programmatic launch: the previous kernel's writes are visible
   using S = OpMarch<K, T>;
   using P = Pair<T>;
@@ -324,6 +328,7 @@ __global__ void __launch_bounds__(OpMarch<K, T>::NT, march_minb<K, T, MODE>())
   }
 
   V2 carry = P::make(T(0), T(0));
+  double dsum = 0.0;  // DOT: this thread's src * dst
   for (int c = c_first; c < cz_end; ++c) {
     cp_async_wait_all();
     __syncthreads();  // IN holds planes cK+1..cK+K; X and the slots are free
@@ -334,13 +339,14 @@ __global__ void __launch_bounds__(OpMarch<K, T>::NT, march_minb<K, T, MODE>())
     __syncthreads();  // slots 0..K-1 hold planes cK+1 .. (c+1)K
     const bool store = c >= cz_begin && row_in;
     if (owner) {
-      V2 rv[K];  // residual: b at this layer's outputs, loaded before the contraction
-      if constexpr (MODE == OpMode::Residual) {
+      V2 rv[K];  // residual: b at this layer's outputs (DOT: src), loaded before the contraction
+      if constexpr (MODE == OpMode::Residual || DOT) {
+        const T *vin = DOT ? src : rhs;
 #pragma unroll
         for (int a = 0; a < K; ++a) {
           const int gz = c * K + a;
           const bool zin = store && gz > 0 && gz < N1g - 1;
-          const T *rp = rhs + gxy + int64_t(gz) * sz;
+          const T *rp = vin + gxy + int64_t(gz) * sz;
           rv[a].x = zin && in0 ? rp[0] : T(0);
           rv[a].y = zin && in1 ? rp[1] : T(0);
         }
@@ -379,13 +385,29 @@ __global__ void __launch_bounds__(OpMarch<K, T>::NT, march_minb<K, T, MODE>())
         if (!store || gz < 1 || gz > N1g - 2) continue;
         T *dp = dst + gxy + int64_t(gz) * sz;
         if constexpr (MODE == OpMode::Vmult) {
-          if (in0) dp[0] = scale * acc.x;
-          if (in1) dp[1] = scale * acc.y;
+          const T q0 = scale * acc.x, q1 = scale * acc.y;
+          if (in0) dp[0] = q0;
+          if (in1) dp[1] = q1;
+          if constexpr (DOT) dsum += double(rv[a].x) * double(q0) + double(rv[a].y) * double(q1);
         } else {
           if (in0) dp[0] = rv[a].x - scale * acc.x;
           if (in1) dp[1] = rv[a].y - scale * acc.y;
         }
       }
+    }
+  }
+  if constexpr (DOT) {
+    // fixed-order CTA sum: warp shuffles, then the warp sums in order
+    __syncthreads();  // the stages' shared memory is free
+    double *red = reinterpret_cast<double *>(smem_raw);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, o);
+    if ((tid & 31) == 0) red[tid >> 5] = dsum;
+    __syncthreads();
+    if (tid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NT / 32; ++w) t += red[w];
+      dotp[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
     }
   }
 }

@@ -195,6 +195,8 @@ struct tps_handle {
   VcycleVectors vc[2];  // [0] FP64, [1] FP32
   std::vector<int> sm_variant[2];  // per level: 3D smoother patches-per-batch variant (autotuned)
   std::vector<int> op_layers[2];   // per level: 3D operator cell layers per CTA (autotuned; 0 default)
+  DevBuf dot_part;                 // 3D: per-CTA p.q partial sums of the fused CG operator
+  int dot_cap = 0;                 // their capacity
   DevBuf err_flag;      // set by a kernel whose bounded wait gave up
   Mailbox mbox;         // small device results (CG scalars, dots, the error flag) for the host
   // variable coefficient: per-level per-cell kappa (fine given, coarse = mean of children)
@@ -727,9 +729,31 @@ void ensure_krylov(tps_handle *h)
   if (!h->q.p) h->q.alloc(sizeof(double) * N);
   if (!h->partial.p) h->partial.alloc(sizeof(double) * kRedBlocks * 4);
   if (!h->scalars.p) h->scalars.alloc(sizeof(CGScalars) + 64);
+  if (h->dim == 3 && !h->dot_part.p) {
+    h->dot_cap = h->kt->laplace3d_ctas(h->fine().n);
+    h->dot_part.alloc(sizeof(double) * h->dot_cap);
+  }
   if (!h->ev0) {
     TPS_CUDA(cudaEventCreate(&h->ev0));
     TPS_CUDA(cudaEventCreate(&h->ev1));
+  }
+}
+
+// q = A p on the finest level and alpha = rz / p.q; in 3D without a
+// coefficient the operator kernel forms the p.q partial sums itself
+void cg_q_alpha(tps_handle *h, const VecLayout &lex, cudaStream_t s)
+{
+  const int L = h->n_levels - 1;
+  CGScalars *sc = h->scalars.as<CGScalars>();
+  if (h->dim == 3 && !h->has_kappa && h->dot_part.p) {
+    int ctas = 0;
+    const int layers = L < static_cast<int>(h->op_layers[0].size()) ? h->op_layers[0][L] : 0;
+    TPS_CUDA(h->kt->laplace3d_dot(h->lv[L], lex, h->q.p, h->p.p, h->dot_part.as<double>(), h->dot_cap, layers,
+                                  &ctas, s));
+    TPS_CUDA(launch_cg_alpha_partials(h->dot_part.as<double>(), ctas, sc, s));
+  } else {
+    level_laplace(h, L, 0, lex, h->q.p, h->p.p, nullptr, 0, s);
+    TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), h->fine().N, h->partial.as<double>(), sc, s));
   }
 }
 
@@ -749,8 +773,7 @@ void cg_iteration_body(tps_handle *h, int prec, bool symmetric, double *x, cudaS
   vcycle_rec(h, L, p, symmetric, s, vprec_tc(prec));
   TPS_CUDA(launch_cg_beta(V.su[L]->p, zk, pm, h->q.as<double>(), h->r.as<double>(), N, part, sc, s));
   TPS_CUDA(launch_cg_update_p(h->p.as<double>(), V.su[L]->p, zk, pm, N, sc, s));
-  level_laplace(h, L, 0, lex, h->q.p, h->p.p, nullptr, 0, s);
-  TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
+  cg_q_alpha(h, lex, s);
   TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
                                V.d[L]->p, input_kind(prec), pm, N, part, sc, s));
   TPS_CUDA(launch_cg_finalize_rr(part, sc, s));
@@ -805,8 +828,7 @@ int solve_cg(tps_handle *h, const tps_solve_opts &o, const double *b, double *x,
     TPS_CUDA(launch_cg_first_direction(h->p.as<double>(), V.su[L]->p, zk, pm, h->r.as<double>(), N,
                                        part, s));
     TPS_CUDA(launch_cg_finalize_rz(part, sc, s));
-    level_laplace(h, L, 0, lex, h->q.p, h->p.p, nullptr, 0, s);
-    TPS_CUDA(launch_cg_alpha(h->p.as<double>(), h->q.as<double>(), N, part, sc, s));
+    cg_q_alpha(h, lex, s);
     TPS_CUDA(launch_cg_update_xr(x, h->r.as<double>(), h->p.as<double>(), h->q.as<double>(),
                                  V.d[L]->p, input_kind(o.precision), pm, N, part, sc, s));
     TPS_CUDA(launch_cg_finalize_rr(part, sc, s));
