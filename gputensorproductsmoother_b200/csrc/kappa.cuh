@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(KSm<DIM, K, T>::NT)
   using S = KSm<DIM, K, T>;
   constexpr int NP = S::NP, N1 = S::N1, M = S::M, NT = S::NT, NC = S::NC, CELL = S::CELL;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ T kps[NC];  // the patch cells' coefficients (indexed by run-time cell)
   T *X = reinterpret_cast<T *>(smem_raw);
   T *TA = X + S::BOX, *TB = TA + NC * CELL, *UA = TB + NC * CELL, *UB = UA + NC * CELL;

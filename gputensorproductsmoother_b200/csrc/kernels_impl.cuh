@@ -295,7 +295,7 @@ void smoother3d_pair_launch(const Sm3Args &a, const SmootherMaps *maps, void *x,
     using S = Pp3<K, WA>;
     static_assert(S::BYTES + 1024 <= 233472, "pair smoother: one CTA must fit an SM");
     static const Residency r = residency(smoother3d_pair_kernel<K, WA>, S::NT, S::BYTES);
-    const int need = static_cast<int>(ceil_div(ceil_div(a.n_patches, 2), WA));
+    const int need = static_cast<int>(ceil_div(a.n_patches, 2));  // one pair at a time per CTA
     const int grid = need < r.per_sm * r.n_sm ? need : r.per_sm * r.n_sm;
     TPS_LAUNCH((smoother3d_pair_kernel<K, WA>), grid, S::NT, S::BYTES, s,
         *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),

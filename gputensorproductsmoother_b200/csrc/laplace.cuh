@@ -78,7 +78,7 @@ __global__ void __launch_bounds__(OpTile<DIM, K>::NT, 2)
   constexpr int NT = Tl::NT, WX = Tl::WX, WY = Tl::WY, WZ = Tl::WZ;
   constexpr int OX = Tl::OX, OY = Tl::OY, OZ = Tl::OZ, RX = Tl::RX;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *sIn = reinterpret_cast<T *>(smem_raw);
   T *U1 = sIn, *U2 = sIn + Tl::US;
   T *T1 = sIn + Tl::REGION0, *T2 = T1 + Tl::TS;

@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(OpMarch<K, T>::NT, march_minb<K, T, MODE, DOT>
   using P = Pair<T>;
   using V2 = typename P::type;
   constexpr int NT = S::NT, EPT = S::EPT, WX = S::WX, PL = S::PL, HX = S::HX;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *sm = reinterpret_cast<T *>(smem_raw);
   T *IN = sm, *X1 = sm + S::OFF_X1, *X2 = sm + S::OFF_X2, *T1 = sm + S::OFF_T1, *T2 = sm + S::OFF_T2;
   const int tid = threadIdx.x;

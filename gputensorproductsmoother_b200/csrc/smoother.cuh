@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(SmootherShape<DIM, K>::NT)
   using S = SmootherShape<DIM, K>;
   constexpr int N1 = S::N1, M = S::M, PPB = S::PPB, NT = S::NT;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *smem = reinterpret_cast<T *>(smem_raw);
 
   const int p0 = blockIdx.x * PPB;

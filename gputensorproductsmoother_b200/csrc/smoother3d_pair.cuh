@@ -19,12 +19,17 @@
 // arithmetic and the loop/TMA skeleton; only the raw box and b-slab reads
 // and the global stores stay per patch.
 //
-// Execution model as in smoother3d_warp_kernel: every warp owns its pairs of
-// patches (patches 2q and 2q+1 of the colour, q = pair index), its stage and
-// its mbarrier; stages are separated by __syncwarp only; the next pair's two
-// x boxes and two b slabs are fetched by TMA (4 copies on one mbarrier) as
-// soon as the x stage has consumed the current ones.  An odd last patch is
-// paired with itself and stored once.  Every wait is bounded.
+// Execution model: a team of warps -- one CTA, two warps from degree 4 on --
+// owns its pairs of patches (patches 2q and 2q+1 of the colour, q = pair
+// index), one stage and one mbarrier.  Every stage's work is a list of 32-lane
+// passes; warp w of the team takes passes w, w + TEAM, ..., so a pair moves
+// through its stages with the team's warps side by side and twice the warps
+// per SM share the same shared memory (the kernel is latency-bound: more
+// resident warps, not fewer instructions, is what it lacks).  Stages are
+// separated by the team's barrier; the next pair's two x boxes and two b
+// slabs are fetched by TMA (4 copies on one mbarrier) as soon as the x stage
+// has consumed the current ones.  An odd last patch is paired with itself
+// and stored once.  Every wait is bounded.
 //
 // Shared memory (8-byte pair elements): the z- and y-stage outputs Z and V
 // are stored task-major for the stage that reads them (conflict-free
@@ -183,7 +188,7 @@ constexpr bool pp3_enabled()
   return K >= 2 && K <= 5;
 }
 
-template <int K, int WARPS>
+template <int K, int TEAM>
 struct Pp3 {
   using L = WpLayout<K, 8>;  // strides of the 8-byte pair elements
   static constexpr int N1 = 2 * K + 1, M = 2 * K - 1;
@@ -203,22 +208,21 @@ struct Pp3 {
   static constexpr int NZP = (N1 * N1 - M * M + (M * M + 1) / 2 + 31) / 32;  // passes of the z stage
   static constexpr int ext(Str3 s) { return (M - 1) * (s.p + s.r + s.c) + 1; }
   static constexpr int QBUF1 = wp_max(ext(L::QA), ext(L::QC)), QBUF2 = wp_max(ext(L::QB), ext(L::QD));
-  // per warp (floats): [x box A | x box B, later V1 | V2] [b slab A | b slab B]
+  // per team (floats): [x box A | x box B, later V1 | V2] [b slab A | b slab B]
   // [Z1 | Z2, later QA/QC | QB/QD]; pair arrays take 2 floats per element
   static constexpr int BOFF = wp_rup(wp_max(2 * XBOX_A, 4 * VEXT), ALIGN);
   static constexpr int ZOFF = BOFF + 2 * BBOX_A;
   static constexpr int WARP_ELEMS = wp_rup(ZOFF + wp_max(4 * ZEXT, 2 * (QBUF1 + QBUF2)), ALIGN);
   static constexpr int QSZ = M * M * M;
-  static constexpr int NT = 32 * WARPS;
-  static constexpr size_t OFF_RL = sizeof(float) * static_cast<size_t>(WARPS) * WARP_ELEMS;
+  static constexpr int NT = 32 * TEAM;  // one team = one CTA, one pair of patches at a time
+  static constexpr size_t OFF_RL = sizeof(float) * static_cast<size_t>(WARP_ELEMS);
   static constexpr size_t OFF_BAR = (OFF_RL + sizeof(float) * QSZ + 7) / 8 * 8;
-  static constexpr size_t BYTES = OFF_BAR + 8 * WARPS;
-  static constexpr size_t bytes_for(int w)
-  {
-    return (sizeof(float) * (static_cast<size_t>(w) * WARP_ELEMS + QSZ) + 7) / 8 * 8 + 8 * static_cast<size_t>(w);
-  }
+  static constexpr size_t BYTES = OFF_BAR + 8;
   static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
   static constexpr int NZT = RING + IPAIR, NYT = M * N1, NQT = M * M;
+  // 32-lane passes of each stage; warp w of the team takes passes w, w + TEAM, ...
+  static constexpr int NYP = (NYT + 31) / 32, NP = (NQT + 31) / 32;
+  static constexpr int NZPW = (NZP + TEAM - 1) / TEAM, NYPW = (NYP + TEAM - 1) / TEAM, NPW = (NP + TEAM - 1) / TEAM;
 };
 
 // Lane assignment of the z stage at degree 4 (positions y * 9 + x of the box
@@ -280,55 +284,52 @@ __device__ __forceinline__ PairZTask pair_ztask(int lane, int p)
   return r;
 }
 
-// warps per CTA with the most warps per SM (228 KB, 1 KB reserved per CTA),
-// at most 16 warps per SM so that a thread keeps 128 registers (the pair
-// contractions hold about 120 live values at degree 4)
+// Warps per pair of patches (the team, one CTA): two from degree 4 on, where
+// every stage has at least two 32-lane passes, so the warps split a pair's
+// passes and twice the warps per SM share the staged boxes' shared memory;
+// one below.  CTAs per SM: as many as shared memory holds, at most 16 warps
+// per SM so that a thread keeps 128 registers (the pair contractions hold
+// about 120 live values at degree 4).
 constexpr int kPairMaxWarpsPerSm = 16;
-template <int K>
-constexpr int pp3_ctas_for(int w)
-{
-  int ctas = static_cast<int>(233472 / (Pp3<K, 1>::bytes_for(w) + 1024));  // 0: does not fit
-  if (ctas * w > kPairMaxWarpsPerSm) ctas = kPairMaxWarpsPerSm / w;
-  return ctas > 32 ? 32 : ctas;
-}
 template <int K>
 constexpr int pp3_warps()
 {
-  int best = 1, best_w = 0;
-  for (int w = 1; w <= 8; ++w) {
-    const int ctas = pp3_ctas_for<K>(w);
-    if (ctas * w > best_w) {
-      best_w = ctas * w;
-      best = w;
-    }
-  }
-  return best;
+  return K >= 4 ? 2 : 1;
 }
-
 template <int K>
 constexpr int pp3_ctas()
 {
-  const int c = pp3_ctas_for<K>(pp3_warps<K>());
-  return c < 1 ? 1 : c;
+  constexpr int w = pp3_warps<K>();
+  int ctas = static_cast<int>(233472 / (Pp3<K, w>::BYTES + 1024));  // 0: does not fit
+  if (ctas * w > kPairMaxWarpsPerSm) ctas = kPairMaxWarpsPerSm / w;
+  ctas = ctas > 32 ? 32 : ctas;
+  return ctas < 1 ? 1 : ctas;
 }
 
-template <int K, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
+template <int K, int TEAM>
+__global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
     smoother3d_pair_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
                            float *__restrict__ x, const Sm3Args a, float scale, float fd_scale,
                            int *__restrict__ err)
 {
   griddep_wait();  // programmatic launch: the previous kernel's writes are visible
-  using S = Pp3<K, WARPS>;
+  using S = Pp3<K, TEAM>;
   using Lo = typename S::L;
   constexpr int N1 = S::N1, M = S::M, W = S::W, AL = S::A;
   constexpr Str3 QA = Lo::QA, QB = Lo::QB, QC = Lo::QC, QD = Lo::QD;
   const DegreeTables<K, float> &tb = c_tables<K, float>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, wt = tid >> 5;  // wt: warp within the team
   float *RL = reinterpret_cast<float *>(smem_raw + S::OFF_RL);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + S::OFF_BAR) + wid;
-  float *stage = reinterpret_cast<float *>(smem_raw) + static_cast<size_t>(wid) * S::WARP_ELEMS;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + S::OFF_BAR);
+  float *stage = reinterpret_cast<float *>(smem_raw);
+  // the team's barrier between stages (one warp: the warp's own)
+  auto team_sync = [&]() {
+    if constexpr (TEAM == 1)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
   float2 *Z1 = reinterpret_cast<float2 *>(stage + S::ZOFF), *Z2 = Z1 + S::ZEXT;
   float2 *V1 = reinterpret_cast<float2 *>(stage), *V2 = V1 + S::VEXT;
   float2 *QAb = Z1, *QBb = Z1 + S::QBUF1;  // QA and QC share one buffer, QB and QD the other
@@ -337,25 +338,27 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
 
   for (int e = tid; e < S::QSZ; e += S::NT)
     RL[e] = fd_scale / (tb.eval[e % M] + tb.eval[(e / M) % M] + tb.eval[e / (M * M)]);
-  if (lane == 0) {
+  if (tid == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
   }
-  __syncthreads();  // the only CTA-wide barrier: RL and the mbarriers are ready
-  // this lane's eigenvalue scalings of the z stage of the solve (tasks t and
-  // t + 32, modes 0..M-1), kept in registers
-  float rl[(S::NQT + 31) / 32][M];
+  __syncthreads();  // RL and the mbarrier are ready
+  // this lane's eigenvalue scalings of the z stage of the solve (the tasks of
+  // this warp's passes, modes 0..M-1), kept in registers
+  constexpr int NPW = S::NPW;
+  float rl[NPW][M];
 #pragma unroll
-  for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
-    const int t = lane + 32 * p < S::NQT ? lane + 32 * p : lane % S::NQT;
+  for (int j = 0; j < NPW; ++j) {
+    const int t0 = lane + 32 * (wt + TEAM * j);
+    const int t = t0 < S::NQT ? t0 : lane % S::NQT;
 #pragma unroll
-    for (int jj = 0; jj < M; ++jj) rl[p][jj] = RL[jj * M * M + t];
+    for (int jj = 0; jj < M; ++jj) rl[j][jj] = RL[jj * M * M + t];
   }
 
   const int n_pairs = (a.n_patches + 1) >> 1;
-  const int G = gridDim.x * WARPS;
-  int q = blockIdx.x * WARPS + wid;
-  // lane 0: both x boxes and b slabs of the pair with box origins (fA, fB)
+  const int G = gridDim.x;
+  int q = blockIdx.x;
+  // thread 0: both x boxes and b slabs of the pair with box origins (fA, fB)
   auto issue = [&](int fxa, int fya, int fza, int fxb, int fyb, int fzb) {
     mbar_arrive_expect_tx(bar, static_cast<uint32_t>(sizeof(float) * 2 * (S::BBOX + (a.zero_x ? 0 : S::XBOX))));
     if (!a.zero_x) {
@@ -371,22 +374,26 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
     wp_patch_xyz(a, ja, K, fxa, fya, fza);
     wp_patch_xyz(a, jb, K, fxb, fyb, fzb);
   };
-  PairZTask ztk[S::NZP];  // this lane's z-stage lines, per pass
+  PairZTask ztk[S::NZPW];  // this lane's z-stage lines, per pass of this warp
 #pragma unroll
-  for (int p = 0; p < S::NZP; ++p) ztk[p] = pair_ztask<K>(lane, p);
+  for (int j = 0; j < S::NZPW; ++j) {
+    const int p = wt + TEAM * j;
+    ztk[j] = p < S::NZP ? pair_ztask<K>(lane, p) : PairZTask{-1, -1, -1};
+  }
   int fxa = 0, fya = 0, fza = 0, fxb = 0, fyb = 0, fzb = 0;
   if (q < n_pairs) {
     pair_xyz(q, fxa, fya, fza, fxb, fyb, fzb);
-    if (lane == 0) issue(fxa, fya, fza, fxb, fyb, fzb);
+    if (tid == 0) issue(fxa, fya, fza, fxb, fyb, fzb);
   }
 
   for (int it = 0; q < n_pairs; q += G, ++it) {
     const int xoa = fxa & (AL - 1), xob = fxb & (AL - 1);
     const bool store_b = 2 * q + 1 < a.n_patches;
-    int nxa = 0, nya = 0, nza = 0, nxb = 0, nyb = 0, nzb = 0;  // the next pair of this warp
+    int nxa = 0, nya = 0, nza = 0, nxb = 0, nyb = 0, nzb = 0;  // the next pair of this team
     if (q + G < n_pairs) pair_xyz(q + G, nxa, nya, nza, nxb, nyb, nzb);
-    if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, it & 1))) {
-      if (lane == 0) atomicExch(err, 1);
+    const bool ok = mbar_wait_bounded(bar, it & 1);
+    if (TEAM == 1 ? !__all_sync(0xffffffffu, ok) : !__syncthreads_and(ok)) {
+      if (tid == 0) atomicExch(err, 1);
       return;  // the only copies in flight were the ones waited for
     }
 
@@ -394,8 +401,8 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
       // ---- z: Z1 = M_z x~, Z2 = L_z x~ (ring lines, then interior lines) ----
       const float *ba = boxA + xoa, *bb = boxB + xob;
 #pragma unroll
-      for (int p = 0; p < S::NZP; ++p) {
-        const PairZTask tk = ztk[p];
+      for (int j = 0; j < S::NZPW; ++j) {
+        const PairZTask tk = ztk[j];
         if (tk.ring >= 0) {
           const int y = tk.ring / N1, xx = tk.ring % N1;
           const int o = y * W + xx;
@@ -429,14 +436,14 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
           }
         }
       }
-      __syncwarp();
+      team_sync();
       // ---- y: V1 = M_y Z2 + L_y Z1, V2 = M_y Z1 (V overwrites the dead x boxes) ----
       // task t = (zi, xx) = (t % M, t / M); lanes past the last task redo a
       // valid task (lane mod the task count) and skip the stores, so every pass
       // is straight-line code
 #pragma unroll
-      for (int p = 0; p < (S::NYT + 31) / 32; ++p) {
-        const int t0 = lane + 32 * p;
+      for (int j = 0; j < S::NYPW; ++j) {
+        const int t0 = lane + 32 * (wt + TEAM * j);
         const bool act = t0 < S::NYT;
         const int t = act ? t0 : lane % S::NYT;
         const int zi = t % M, xx = t / M;
@@ -460,12 +467,12 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
           }
         }
       }
-      __syncwarp();
+      team_sync();
     }
     // ---- x: r = b - s (M_x V1 + L_x V2), then S^T along x -> QA ----
 #pragma unroll
-    for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
-      const int t0 = lane + 32 * p;
+    for (int j = 0; j < NPW; ++j) {
+      const int t0 = lane + 32 * (wt + TEAM * j);
       const bool act = t0 < S::NQT;  // idle lanes redo task lane % NQT, stores skipped
       const int t = act ? t0 : lane % S::NQT;
       {
@@ -525,36 +532,36 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
         }
       }
     }
-    __syncwarp();
+    team_sync();
     // the staged boxes and slabs are consumed: fetch the next pair now
-    if (lane == 0 && q + G < n_pairs) {
+    if (tid == 0 && q + G < n_pairs) {
       fence_proxy_async_smem();
       issue(nxa, nya, nza, nxb, nyb, nzb);
     }
-    // ---- the four fast-diagonalisation stages: each lane's tasks of both
-    // passes side by side (all loads, then the independent contractions, then
-    // the stores), so the two chains interleave ----
-    constexpr int NP = (S::NQT + 31) / 32;
-    int tq[NP];
-    bool aq[NP];
+    // ---- the four fast-diagonalisation stages: each lane's tasks of this
+    // warp's passes side by side (all loads, then the independent
+    // contractions, then the stores), so their chains interleave ----
+    int tq[NPW];
+    bool aq[NPW];
 #pragma unroll
-    for (int p = 0; p < NP; ++p) {
-      aq[p] = lane + 32 * p < S::NQT;  // idle lanes redo task lane % NQT, stores skipped
-      tq[p] = aq[p] ? lane + 32 * p : lane % S::NQT;
+    for (int j = 0; j < NPW; ++j) {
+      const int t0 = lane + 32 * (wt + TEAM * j);
+      aq[j] = t0 < S::NQT;  // idle lanes redo task lane % NQT, stores skipped
+      tq[j] = aq[j] ? t0 : lane % S::NQT;
     }
     // ---- S^T along y: QA -> QB ----
     {
-      float2 v[NP][M], qv[NP][M];
+      float2 v[NPW][M], qv[NPW][M];
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         const float2 *src = QAb + (tq[p] / M) * QA.p + (tq[p] % M) * QA.c;
 #pragma unroll
         for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QA.r];
       }
 #pragma unroll
-      for (int p = 0; p < NP; ++p) pr_evec<K, true>(v[p], qv[p]);
+      for (int p = 0; p < NPW; ++p) pr_evec<K, true>(v[p], qv[p]);
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         float2 *d = QBb + (tq[p] / M) * QB.p + (tq[p] % M) * QB.c;
         if (aq[p]) {
 #pragma unroll
@@ -562,25 +569,25 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
         }
       }
     }
-    __syncwarp();
+    team_sync();
     // ---- S^T along z, eigenvalue scaling, S along z: QB -> QC ----
     {
-      float2 v[NP][M], qv[NP][M];
+      float2 v[NPW][M], qv[NPW][M];
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         const float2 *src = QBb + (tq[p] / M) * QB.r + (tq[p] % M) * QB.c;
 #pragma unroll
         for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QB.p];
       }
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         pr_evec<K, true>(v[p], qv[p]);
 #pragma unroll
         for (int jj = 0; jj < M; ++jj) qv[p][jj] = pr_mul(rl[p][jj], qv[p][jj]);
         pr_evec<K, false>(qv[p], v[p]);
       }
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         float2 *d = QAb + (tq[p] / M) * QC.r + (tq[p] % M) * QC.c;
         if (aq[p]) {
 #pragma unroll
@@ -588,20 +595,20 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
         }
       }
     }
-    __syncwarp();
+    team_sync();
     // ---- S along x: QC -> QD ----
     {
-      float2 v[NP][M], qv[NP][M];
+      float2 v[NPW][M], qv[NPW][M];
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         const float2 *src = QAb + (tq[p] / M) * QC.p + (tq[p] % M) * QC.r;
 #pragma unroll
         for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QC.c];
       }
 #pragma unroll
-      for (int p = 0; p < NP; ++p) pr_evec<K, false>(v[p], qv[p]);
+      for (int p = 0; p < NPW; ++p) pr_evec<K, false>(v[p], qv[p]);
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         float2 *d = QBb + (tq[p] / M) * QD.p + (tq[p] % M) * QD.r;
         if (aq[p]) {
 #pragma unroll
@@ -609,23 +616,23 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
         }
       }
     }
-    __syncwarp();
+    team_sync();
     // ---- S along y and store x_I of both patches ----
     {
       float *const xpa = x + (fxa + 1 + (fya + 1) * a.sy + (fza + 1) * a.sz);
       float *const xpb = x + (fxb + 1 + (fyb + 1) * a.sy + (fzb + 1) * a.sz);
       const int sy32 = static_cast<int>(a.sy), sz32 = static_cast<int>(a.sz);
-      float2 v[NP][M], qv[NP][M];
+      float2 v[NPW][M], qv[NPW][M];
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         const float2 *src = QBb + (tq[p] / M) * QD.p + (tq[p] % M) * QD.c;
 #pragma unroll
         for (int jj = 0; jj < M; ++jj) v[p][jj] = src[jj * QD.r];
       }
 #pragma unroll
-      for (int p = 0; p < NP; ++p) pr_evec<K, false>(v[p], qv[p]);
+      for (int p = 0; p < NPW; ++p) pr_evec<K, false>(v[p], qv[p]);
 #pragma unroll
-      for (int p = 0; p < NP; ++p) {
+      for (int p = 0; p < NPW; ++p) {
         const int o = tq[p] % M + (tq[p] / M) * sz32;
         if (aq[p]) {
 #pragma unroll
@@ -637,7 +644,7 @@ __global__ void __launch_bounds__(32 * WARPS, pp3_ctas<K>())
         }
       }
     }
-    __syncwarp();  // the Q buffers (inside the Z region) are read before the next z stage
+    team_sync();  // the Q buffers (inside the Z region) are read before the next z stage
     fxa = nxa;
     fya = nya;
     fza = nza;

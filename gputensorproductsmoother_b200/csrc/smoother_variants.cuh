@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(PVar<DIM, K>::NT)
   using S = PVar<DIM, K>;
   constexpr int N1 = S::N1, M = S::M, NT = S::NT;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *Pm = reinterpret_cast<T *>(smem_raw), *Pl = Pm + N1 * N1, *X = Pl + N1 * N1;
   T *Z1 = X + S::BOX, *Z2 = Z1 + S::ZS, *V1 = Z2 + S::ZS, *V2 = V1 + S::VS;
   const int tid = threadIdx.x;
@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(PVar<DIM, K>::NT)
   using S = PVar<DIM, K>;
   constexpr int M = S::M, NT = S::NT, INT = S::INT;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *Ev = reinterpret_cast<T *>(smem_raw), *Lm = Ev + M * M, *Q0 = Lm + M, *Q1 = Q0 + INT;
   const int tid = threadIdx.x;
   const int64_t o = pv_origin<DIM, K>(c, blockIdx.x);

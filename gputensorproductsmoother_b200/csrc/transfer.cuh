@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
   constexpr int C = XYTile<K>::C, NT = XYTile<K>::NT;
   constexpr int WI = 2 * K * (C + 1) + 1;  // fine inputs per direction
   constexpr int WO = C * K;                // coarse outputs per direction
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   T *sIn = reinterpret_cast<T *>(smem_raw);
   T *sX = sIn + WI * WI;
   const int plane = plane0 + blockIdx.z;
