@@ -71,10 +71,15 @@ struct Tc3 {
   static constexpr int NBF = rup(M, 16), SBOF = (KF / 4) * 128 + 16;
   static constexpr int AF = cdiv(RF, 8) * SBOF;
   static constexpr int BBOX = M * M * XW * 4;  // b interior, [zi][yi][box x]
-  // one slot: work region (x box, then the operands of S2..S9) + b box
+  // one slot: work region (x box, then the operands of S2..S9) + b box.
+  // Two slots per unit (the patch being solved and the TMA prefetch of its
+  // next patch) up to degree 4; one from degree 5 on, where a slot is 17-40 KB
+  // and the units that fit instead (8, 7 and 5 per SM at degrees 5, 6 and 7
+  // against 6, 3 and 2 with prefetch slots) overlap one another's stages
   static constexpr int WORK = rup(mx(mx(XBOX, A2), mx(A3, AF)), 128);
   static constexpr int SLOT = WORK + rup(BBOX, 128);
-  static constexpr int UNIT = 2 * SLOT;
+  static constexpr int SLOTS = K >= 5 ? 1 : 2;
+  static constexpr int UNIT = SLOTS * SLOT;
   static constexpr int COLS = mx(mx(T1 * NB1, T2 * NB2), mx(T3 * NB3, TF * NBF));  // TMEM columns
   // furthest byte an MMA may read, relative to its slot (16 groups of 8 rows per tile)
   static constexpr int EXT = mx(mx(T1 * 16 * SBO1 + KS1 * 256, T2 * 16 * SBO2 + KS2 * 256),
@@ -267,15 +272,15 @@ __global__ void __launch_bounds__(Tc3<K>::NT, Tc3<K>::MINB)
   const int first = blockIdx.x * U + u;
   if (leader && first < a.n_patches) issue(first, 0);
   for (int pp = first; pp < a.n_patches; pp += gstride, ++it) {
-    const int sl = it & 1;
+    const int sl = C::SLOTS == 2 ? (it & 1) : 0;
     unsigned char *work = slots + sl * C::SLOT;
     const float *bbox = reinterpret_cast<const float *>(work + C::WORK);
     const uint32_t wsa = smem_u32(work);
-    if (leader && pp + gstride < a.n_patches) issue(pp + gstride, sl ^ 1);
+    if (C::SLOTS == 2 && leader && pp + gstride < a.n_patches) issue(pp + gstride, sl ^ 1);
     int fx, fy, fz;
     patch_xyz(pp, fx, fy, fz);
     const int xo = fx & 3;
-    if (!mbar_wait_bounded(&tbar[sl], (it >> 1) & 1)) {
+    if (!mbar_wait_bounded(&tbar[sl], C::SLOTS == 2 ? (it >> 1) & 1 : it & 1)) {
       atomicExch(err, 1);
       s_abort[u] = 1;
     }
@@ -436,9 +441,15 @@ __global__ void __launch_bounds__(Tc3<K>::NT, Tc3<K>::MINB)
     // before the unit's next MMAs and TMA loads
     tc_fence_before();
     named_bar(1 + u, 128);
+    // one slot: the next patch is fetched once this one has left the slot
+    if (C::SLOTS == 1 && leader && pp + gstride < a.n_patches) {
+      fence_proxy_async_smem();
+      issue(pp + gstride, 0);
+    }
   }
   // a unit that stopped early waits (bounded) for its prefetch still in flight
-  if (leader && s_abort[u]) {
+  // (with one slot no load is issued ahead of the patch being solved)
+  if (C::SLOTS == 2 && leader && s_abort[u]) {
     const int pp = first + it * gstride;
     if (pp + gstride < a.n_patches) (void)mbar_wait_bounded(&tbar[(it & 1) ^ 1], ((it + 1) >> 1) & 1);
   }
