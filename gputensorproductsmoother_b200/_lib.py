@@ -81,6 +81,8 @@ SIGNATURES = [
     ("tps_set_kappa", ctypes.c_int, [_VP, _VP, ctypes.c_int]),
     ("tps_mass_vmult", ctypes.c_int, [_VP, _VP, _VP, _VP]),
     ("tps_assemble_rhs", ctypes.c_int, [_VP, ctypes.c_int, _VP, _VP, _VP]),
+    ("tps_adjoint", ctypes.c_int, [_VP, ctypes.POINTER(TpsSolveOpts), _VP, _VP, _VP, _VP,
+                                   ctypes.POINTER(TpsReport), _VP]),
     ("tps_cell_energy", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
     ("tps_restrict_add_noalloc", ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                 ctypes.c_int, _VP, _VP, _VP]),

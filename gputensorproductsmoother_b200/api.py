@@ -447,6 +447,29 @@ class MultigridSolvers:
         return self._solve(L.DRIVER_CG, b, x, precision, symmetric, max_iter, rel_tol, 1e-300,
                            use_graph, raise_on_fail)
 
+    def adjoint(self, u: torch.Tensor, g: torch.Tensor, precision: str = "fp64", rel_tol: float = 1e-13,
+                max_iter: int = 400, kappa_gradient: bool = True, raise_on_fail: bool = True):
+        """Adjoint gradients of J(u(f, kappa)) through tps_adjoint: given the
+        forward solution u and g = dJ/du, solves A lambda = g (Dirichlet rows
+        of g taken as zero) and returns (dJ/df = M lambda, dJ/dkappa =
+        -lambda_c^T A_c u_c per cell or None, SolveReport)."""
+        p = self.problem
+        lv = p.n_levels - 1
+        p._check_vec(u, lv, torch.float64)
+        p._check_vec(g, lv, torch.float64)
+        dJdf = torch.empty_like(u)
+        dk = None
+        if kappa_gradient and p.has_kappa:
+            n = p.cells(lv)
+            dk = torch.empty(n ** p.dim, dtype=torch.float64, device=u.device)
+        o = L.TpsSolveOpts(L.DRIVER_CG, _PRECISIONS[precision], 1, max_iter, rel_tol, 1e-300, 1)
+        rep = L.TpsReport()
+        st = L.lib().tps_adjoint(p.handle, ctypes.byref(o), u.data_ptr(), g.data_ptr(), dJdf.data_ptr(),
+                                 None if dk is None else dk.data_ptr(), ctypes.byref(rep), _stream())
+        if st != L.TPS_OK and (raise_on_fail or st != 4):
+            L.check(st, p.handle)
+        return dJdf, dk, _report(rep)
+
     def solve_host_many(self, bs, xs=None, precision: str = "fp32", symmetric: bool = True,
                         max_iter: int = 100, rel_tol: float = 1e-10, raise_on_fail: bool = True):
         """CG solves (each from x = 0) of a sequence of HOST right-hand sides

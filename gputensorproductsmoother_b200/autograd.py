@@ -2,11 +2,12 @@
 
 ``PoissonSolve.apply(problem, f, kappa)`` returns u with A(kappa) u = M f
 (M the finite-element mass matrix, f nodal values, homogeneous Dirichlet
-data).  The backward pass is the hand-written adjoint: one MG-preconditioned
-CG solve A(kappa) lambda = dJ/du (A is symmetric on the interior), then
+data).  The backward pass is the hand-written adjoint, one call of
+tps_adjoint: an MG-preconditioned CG solve A(kappa) lambda = dJ/du (A is
+symmetric on the interior), then
 
-    dJ/df     = M lambda                       (tps_mass_vmult)
-    dJ/dkappa = -lambda_c^T A_cell u_c per cell  (tps_cell_energy)
+    dJ/df     = M lambda
+    dJ/dkappa = -lambda_c^T A_cell u_c per cell
 
 No reference counterpart (the reference has no differentiable path).  Both
 solves use the FP64 V-cycle by default and a tight tolerance so that the
@@ -41,14 +42,9 @@ class PoissonSolve(torch.autograd.Function):
     def backward(ctx, grad_u):
         (u,) = ctx.saved_tensors
         P = ctx.problem
-        g = grad_u.detach().to(torch.float64).contiguous().clone()
-        _zero_dirichlet(g, P)
-        lam, _ = MultigridSolvers(P).solve_cg(g, precision=ctx.precision, rel_tol=ctx.rel_tol,
-                                              max_iter=400)
-        _zero_dirichlet(lam, P)
-        grad_f = torch.empty_like(lam)
-        P.mass_vmult(grad_f, lam)
-        grad_k = -P.cell_energy(u, lam)
+        g = grad_u.detach().to(torch.float64).contiguous()
+        grad_f, grad_k, _ = MultigridSolvers(P).adjoint(u, g, precision=ctx.precision, rel_tol=ctx.rel_tol,
+                                                        max_iter=400)
         return None, grad_f.to(ctx.f_dtype), grad_k.to(ctx.k_dtype), None, None
 
 

@@ -220,6 +220,7 @@ struct tps_handle {
   cudaEvent_t pipe_in[2] = {nullptr, nullptr}, pipe_done[2] = {nullptr, nullptr}, pipe_out[2] = {nullptr, nullptr};
   std::vector<std::unique_ptr<DevBuf>> fmg_sol, fmg_res;  // FMG: FP64 per level (lexicographic)
   DevBuf fmg_tmp;                                        // FMG: FP64 transfer scratch
+  DevBuf adj_g, adj_lam;                                 // tps_adjoint: its right-hand side and lambda
   DevBuf var_r[2];      // separate-kernel smoother variants: residual of the finest-level size
   DevBuf var_acc[2];    // additive step: the summed patch solves
   int sm_kind = TPS_SMOOTHER_FUSED;  // V-cycle smoothing on levels >= 1
@@ -1505,6 +1506,45 @@ int tps_assemble_rhs(tps_handle *h, int level, const double *f_quad, double *b, 
     TPS_CUDA(h->kt->assemble_rhs[h->dim - 2](h->lv[level], lex_layout(h, level), b, f_quad,
                                              static_cast<cudaStream_t>(stream)));
   });
+}
+
+int tps_adjoint(tps_handle *h, const tps_solve_opts *opts, const double *u, const double *g, double *dJdf,
+                double *dJdkappa, tps_report *report, void *stream)
+{
+  int status = TPS_OK;
+  int rc = guarded(h, [&] {
+    if (!opts || !u || !g || !dJdf || !report) throw ApiError(TPS_ERR_INVALID, "null argument");
+    if (opts->driver != TPS_DRIVER_CG) throw ApiError(TPS_ERR_INVALID, "the adjoint solve uses the CG driver");
+    if (opts->max_iter < 1) throw ApiError(TPS_ERR_INVALID, "max_iter must be >= 1");
+    if (dJdkappa && !h->has_kappa) throw ApiError(TPS_ERR_INVALID, "dJ/dkappa needs a handle created with kappa");
+    if (dJdf == g || dJdf == u) throw ApiError(TPS_ERR_INVALID, "dJ/df must not alias u or g");
+    std::memset(report, 0, sizeof(*report));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int L = h->n_levels - 1;
+    const LevelGeomH &gf = h->fine();
+    const int64_t N = gf.N;
+    if (!h->adj_g.p) h->adj_g.alloc(sizeof(double) * N);
+    if (!h->adj_lam.p) h->adj_lam.alloc(sizeof(double) * N);
+    double *gb = h->adj_g.as<double>(), *lam = h->adj_lam.as<double>();
+    // adjoint right-hand side: g with its Dirichlet rows zeroed, so lambda = 0 there
+    TPS_CUDA(cudaMemsetAsync(lam, 0, sizeof(double) * N, s));
+    TPS_CUDA(cudaMemcpyAsync(gb, g, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
+    TPS_CUDA(launch_copy_boundary(gb, lam, h->dim, gf.N1, 8, s));
+    status = solve_cg(h, *opts, gb, lam, report, s);
+    TPS_CUDA(h->kt->mass[h->dim - 2](gf, lex_layout(h, L), dJdf, lam, s));
+    if (dJdkappa) {
+      TPS_CUDA(h->kt->cell_energy[h->dim - 2](gf, lex_layout(h, L), dJdkappa, u, lam, s));
+      const int64_t nc = h->dim == 3 ? int64_t(gf.n) * gf.n * gf.n : int64_t(gf.n) * gf.n;
+      TPS_CUDA(launch_scale_f64(dJdkappa, -1.0, nc, s));
+    }
+    if (take_timeout_flag(h, s)) {
+      status = TPS_ERR_TIMEOUT;
+      report->converged = 0;
+    }
+  });
+  if (rc != TPS_OK) return rc;
+  h->err = status_message(status);
+  return status;
 }
 
 int tps_cell_energy(tps_handle *h, const double *u, const double *lam, double *energy, void *stream)

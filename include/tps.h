@@ -217,6 +217,21 @@ int tps_mass_vmult(tps_handle *h, double *dst, const double *src, void *stream);
  * by colour, no atomics). */
 int tps_assemble_rhs(tps_handle *h, int level, const double *f_quad, double *b, void *stream);
 
+/* Adjoint of the solve u = A(kappa)^{-1} M f for a loss J(u) (no reference
+ * counterpart; the reference has no differentiable path): given the forward
+ * solution u and g = dJ/du (FP64 device vectors, finest level,
+ * lexicographic), solves A(kappa) lambda = g with the MG-preconditioned CG of
+ * opts (driver TPS_DRIVER_CG; g's Dirichlet rows are taken as zero, so
+ * lambda vanishes there) and returns
+ *   dJdf[i]     = (M lambda)_i                      (all rows, as tps_mass_vmult)
+ *   dJdkappa[c] = -lambda_c^T A_cell u_c per cell   (as -tps_cell_energy; may be
+ *                 NULL, and needs a handle created with kappa)
+ * report: the adjoint solve's.  Returns the adjoint solve's status (a gradient
+ * of a solve that did not converge is returned with TPS_ERR_NOT_CONVERGED).
+ * The handle keeps two more N-vectors between calls. */
+int tps_adjoint(tps_handle *h, const tps_solve_opts *opts, const double *u, const double *g, double *dJdf,
+                double *dJdkappa, tps_report *report, void *stream);
+
 /* energy[c] = lambda_c^T A_cell u_c = int_c grad(lambda).grad(u) for every
  * finest-level cell c (lexicographic cells), FP64: dJ/dkappa_c = -energy[c]
  * for J(u(kappa)) with adjoint state lambda. */

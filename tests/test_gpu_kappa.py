@@ -164,8 +164,9 @@ def test_adjoint_48cubed_q4(cuda):
 
 @pytest.mark.parametrize("dim,k,n", [(3, 2, 6), (3, 4, 12)])
 def test_adjoint_matches_fp64_oracle_adjoint(cuda, oracle, dim, k, n):
-    """GPU adjoint gradients (autograd.PoissonSolve backward: MG-CG adjoint
-    solve, tps_mass_vmult, tps_cell_energy) against the FP64 oracle adjoint
+    """GPU adjoint gradients (autograd.PoissonSolve backward: one tps_adjoint
+    call, i.e. the MG-CG adjoint solve, M lambda and the per-cell energies)
+    against the FP64 oracle adjoint
     (oracle.adjoint_gradients: the oracle's MG-CG, a dense-Kronecker mass apply
     and per-cell energies restated from the definitions) on the same seeded
     kappa, f and target: u, dJ/df and dJ/dkappa within 1e-10 (max-norm,
@@ -191,4 +192,60 @@ def test_adjoint_matches_fp64_oracle_adjoint(cuda, oracle, dim, k, n):
     df = relerr(fv.grad.cpu().numpy(), gfo)
     dk = relerr(kv.grad.cpu().numpy(), gko)
     assert du <= 1e-10 and df <= 1e-10 and dk <= 1e-10, (du, df, dk)
+    P.close()
+
+
+def test_adjoint_abi_equals_the_composition(cuda):
+    """tps_adjoint is the adjoint solve of the CG driver followed by the mass
+    apply and the negated per-cell energies: bit-identical to composing
+    tps_solve, tps_mass_vmult and tps_cell_energy by hand; g's Dirichlet rows
+    are ignored (g is not modified); dJ/dkappa may be skipped."""
+    dim, k, n = 3, 3, 8
+    N1 = n * k + 1
+    kap = torch.tensor(kappa_field(dim, n, 21), device="cuda")
+    P = tps.PoissonProblem(dim, k, n, kappa=kap)
+    MG = tps.MultigridSolvers(P)
+    u, _ = MG.solve_cg(torch.tensor(bvec(dim, N1, 22), device="cuda"), precision="fp64", rel_tol=1e-13)
+    g = torch.tensor(np.random.default_rng(23).uniform(-1, 1, N1 ** dim), device="cuda")  # boundary rows too
+    g0 = g.clone()
+    df, dk, rep = MG.adjoint(u, g, precision="fp64", rel_tol=1e-13)
+    assert rep.converged and torch.equal(g, g0)
+    gz = torch.tensor(bvec(dim, N1, 23), device="cuda")  # the same draws, Dirichlet rows zero
+    lam, rep2 = MG.solve_cg(gz, precision="fp64", rel_tol=1e-13, max_iter=400)
+    assert rep2.iterations == rep.iterations
+    df_ref = torch.empty_like(lam)
+    P.mass_vmult(df_ref, lam)
+    dk_ref = -P.cell_energy(u, lam)
+    assert torch.equal(df, df_ref) and torch.equal(dk, dk_ref)
+    df2, dk2, _ = MG.adjoint(u, g, precision="fp64", rel_tol=1e-13, kappa_gradient=False)
+    assert dk2 is None and torch.equal(df2, df)
+    P.close()
+
+
+def test_adjoint_abi_rejects_bad_requests(cuda):
+    from gputensorproductsmoother_b200 import _lib as L
+    import ctypes
+    P = tps.PoissonProblem(3, 2, 4)  # no kappa
+    u = P.new_vector()
+    g = P.new_vector()
+    o = L.TpsSolveOpts(L.DRIVER_CG, 0, 1, 50, 1e-10, 1e-300, 1)
+    rep = L.TpsReport()
+    dk = torch.empty(64, dtype=torch.float64, device="cuda")
+    st = L.lib().tps_adjoint(P.handle, ctypes.byref(o), u.data_ptr(), g.data_ptr(), g.data_ptr(), None,
+                             ctypes.byref(rep), None)
+    assert st == 1  # TPS_ERR_INVALID: dJ/df aliases g
+    df = P.new_vector()
+    st = L.lib().tps_adjoint(P.handle, ctypes.byref(o), u.data_ptr(), g.data_ptr(), df.data_ptr(),
+                             dk.data_ptr(), ctypes.byref(rep), None)
+    assert st == 1  # dJ/dkappa without kappa
+    o.driver = L.DRIVER_GMRES
+    st = L.lib().tps_adjoint(P.handle, ctypes.byref(o), u.data_ptr(), g.data_ptr(), df.data_ptr(), None,
+                             ctypes.byref(rep), None)
+    assert st == 1
+    # the handle stays usable: a zero g gives zero gradients
+    o.driver = L.DRIVER_CG
+    st = L.lib().tps_adjoint(P.handle, ctypes.byref(o), u.data_ptr(), g.data_ptr(), df.data_ptr(), None,
+                             ctypes.byref(rep), None)
+    torch.cuda.synchronize()
+    assert st == L.TPS_OK and df.abs().max().item() == 0.0
     P.close()
