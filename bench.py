@@ -246,12 +246,36 @@ def launches_per_solve(dim: int, n_levels: int, iterations: int) -> int:
     colours = 1 << dim
     per_level = 2 * colours + 1 + (2 if dim == 3 else 1) * 2
     vcycle = per_level * (n_levels - 1) + 1  # coarse: the single patch (colour 0)
-    init = 1 + 1 + 2 + vcycle + 2 + 1 + 2 + 1 + 1
-    per_it = vcycle + 2 + 1 + 1 + 2 + 1 + 1
+    # q = A p and alpha: the operator, then the p.q dot and its finalize; in 3D
+    # the operator forms the dot's partial sums itself (operator + finalize)
+    q_alpha = 2 if dim == 3 else 3
+    init = 1 + 1 + 2 + vcycle + 2 + q_alpha + 1 + 1
+    per_it = vcycle + 2 + 1 + q_alpha + 1 + 1
     # one small copy kernel per host readback: the CG scalars after the set-up
     # and at each iteration's check, and the bounded-wait flag at the end
     readbacks = iterations + 2
     return init + per_it * max(iterations - 1, 0) + readbacks
+
+
+def cg_iteration_bytes(dim: int, k: int, n_fine: int, n_levels: int, s: int) -> dict:
+    """Algorithmic bytes of one MG-CG iteration (V-cycle in s-byte precision,
+    FP64 outer CG), the sum the roofline of a whole solve is measured
+    against.  Per level l >= 1 (N_l DoFs): two coloured sweeps (s (|U_c| +
+    2 |I_c|) per colour), the residual s 3 N_l, the restriction s (N_l +
+    N_l-1) and the prolongation-add s (2 N_l + N_l-1); the coarse level's
+    single-patch solve is left out.  Outer CG on the fine level (N): q = A p
+    8 2N; the beta dots r.z, q.z (z in the V-cycle precision) 16N + sN;
+    p = z + beta p 16N + sN; x, r update and the V-cycle input 8 6N + sN."""
+    n0 = n_fine >> (n_levels - 1)
+    nd = [(n0 << l) * k + 1 for l in range(n_levels)]
+    N = [v ** dim for v in nd]
+    vc = 0
+    for l in range(1, n_levels):
+        vc += 2 * smoother_bytes(dim, k, n0 << l, s)[0]
+        vc += s * 3 * N[l] + s * (N[l] + N[l - 1]) + s * (2 * N[l] + N[l - 1])
+    nf = N[-1]
+    cg = 8 * 2 * nf + (16 * nf + s * nf) + (16 * nf + s * nf) + (8 * 6 * nf + s * nf)
+    return {"vcycle": vc, "outer_cg": cg, "total": vc + cg}
 
 
 # DRAM traffic of the roofline kernel: ncu captures of its colour-0 launch
@@ -804,6 +828,16 @@ def main():
         "gpu_launches": args.steps * launches_per_solve(dim, P.n_levels, rep.iterations),
         "clocks": clocks,
     }
+    # the whole solve against HBM: algorithmic bytes of its CG iterations (the
+    # initial residual and the convergence checks left out) / the solve time
+    itb = cg_iteration_bytes(dim, k, n, P.n_levels, 4)
+    solve_gbps = itb["total"] * rep.iterations / (ms * 1e-3) / 1e9
+    line["solve_roofline"] = {"bytes_per_iteration": itb, "iterations": rep.iterations,
+                              "achieved": solve_gbps, "peak": hbm_peak, "unit": "GB/s",
+                              "frac": solve_gbps / hbm_peak,
+                              "model": "sum over levels of 2 sweeps, residual, restriction, "
+                                       "prolongation + outer-CG vector and operator traffic, "
+                                       "per iteration x iterations / solve time"}
     if rank == 0 and world == 1 and not args.no_configs:
         # every other configuration, measured after the headline's timed region
         subs = {}
