@@ -89,6 +89,7 @@ SIGNATURES = [
     ("tps_fmg", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_VP), ctypes.POINTER(_VP), _VP,
                                ctypes.POINTER(TpsReport), _VP]),
     ("tps_autotune", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("tps_set_operator_layers", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("tps_get_operator_layers", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_smoother_variants", ctypes.c_int, [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
     ("tps_set_smoother_variant", ctypes.c_int, [_VP, ctypes.c_int, ctypes.c_int, ctypes.c_int]),

@@ -122,6 +122,13 @@ class PoissonProblem:
                                                 ctypes.byref(out)), self.handle)
         return out.value
 
+    def set_operator_layers(self, layers: int, dtype: str = "fp32", level: int | None = None) -> None:
+        """Cell layers per CTA of the 3D operator on one level (all if None);
+        0 = the library's rule."""
+        code = {"fp64": L.TPS_F64, "fp32": L.TPS_F32}[dtype]
+        for lv in range(self.n_levels) if level is None else [level]:
+            L.check(L.lib().tps_set_operator_layers(self.handle, code, lv, layers), self.handle)
+
     def smoother_variants(self, dtype: str = "fp32") -> list[int]:
         """Patches per batch of each compiled 3D smoother variant (index =
         variant; -1: one warp per patch; -2: two patches per warp in packed

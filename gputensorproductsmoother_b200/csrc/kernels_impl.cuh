@@ -267,8 +267,8 @@ void smoother3d_launch(Sm3Args a, const SmootherMaps *maps, void *x, const void 
   }
 }
 
-// one colour with one warp per patch (TMA views required): a persistent grid
-// of the CTAs resident per SM x SMs, capped by the patch count
+// one colour with one patch per team of warps (TMA views required): a
+// persistent grid of the CTAs resident per SM x SMs, capped by the patch count
 template <typename T>
 void smoother3d_warp_launch(const Sm3Args &a, const SmootherMaps *maps, void *x, T scale, T fd, int *err,
                             cudaStream_t s)
@@ -277,7 +277,7 @@ void smoother3d_warp_launch(const Sm3Args &a, const SmootherMaps *maps, void *x,
     constexpr int WA = wp3_warps<K, T>();
     using S = Wp3<K, T, WA>;
     static const Residency r = residency(smoother3d_warp_kernel<K, T, WA>, S::NT, S::BYTES);
-    const int need = static_cast<int>(ceil_div(a.n_patches, WA));
+    const int need = a.n_patches;  // one patch at a time per CTA
     const int grid = need < r.per_sm * r.n_sm ? need : r.per_sm * r.n_sm;
     TPS_LAUNCH((smoother3d_warp_kernel<K, T, WA>), grid, S::NT, S::BYTES, s,
         *reinterpret_cast<const CUtensorMap *>(maps->x), *reinterpret_cast<const CUtensorMap *>(maps->b),

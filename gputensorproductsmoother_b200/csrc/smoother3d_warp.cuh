@@ -9,14 +9,17 @@
 // arithmetic of a patch is the same operation for operation, so both
 // kernels give bit-identical sweeps.
 //
-// Execution model: every warp owns its patches, its shared-memory stage and
-// its mbarrier.  The seven contraction stages of a patch are separated by
-// __syncwarp only, so warps never wait for one another (the CTA-wide version
-// loses about half of its issue slots at the barriers between stages).  The
-// next patch's x box and b slab are fetched by TMA as soon as the x stage has
-// consumed the current ones, so the load overlaps the four
-// fast-diagonalisation stages of the same warp and the work of the other
-// warps on the SM.
+// Execution model: a team of warps -- one CTA; two warps in FP64 from degree
+// 4 on, where every stage has at least two 32-lane passes -- owns its patches, one
+// shared-memory stage and one mbarrier; warp w of the team takes passes w,
+// w + TEAM, ... of every stage, so twice the warps per SM share the stage's
+// shared memory.  The seven contraction stages of a patch are separated by
+// the team's barrier (the warp's own __syncwarp for a one-warp team); teams
+// never wait for one another (a CTA-wide batch of patches loses about half
+// of its issue slots at the barriers between stages).  The next patch's x box
+// and b slab are fetched by TMA as soon as the x stage has consumed the
+// current ones, so the load overlaps the four fast-diagonalisation stages of
+// the same team and the work of the other teams on the SM.
 //
 // Shared-memory strides: each staged array is written by one stage and read
 // by the next with a fixed lane -> line mapping (y stage: zi = t % M,
@@ -94,7 +97,7 @@ constexpr bool wp3_enabled()
 constexpr int wp_max(int a, int b) { return a > b ? a : b; }
 constexpr int wp_rup(int a, int m) { return (a + m - 1) / m * m; }
 
-template <int K, typename T, int WARPS>
+template <int K, typename T, int TEAM>
 struct Wp3 {
   using L = WpLayout<K, static_cast<int>(sizeof(T))>;
   static constexpr int N1 = 2 * K + 1, M = 2 * K - 1;
@@ -105,48 +108,44 @@ struct Wp3 {
   static constexpr int VEXT = (M - 1) * L::PV + (M - 1) * L::RV + N1;
   static constexpr int ext(Str3 s) { return (M - 1) * (s.p + s.r + s.c) + 1; }
   static constexpr int QBUF1 = wp_max(ext(L::QA), ext(L::QC)), QBUF2 = wp_max(ext(L::QB), ext(L::QD));
-  // per warp: [x box, later V1 | V2] [b slab] [Z1 | Z2, later QA/QC | QB/QD]
+  // per team: [x box, later V1 | V2] [b slab] [Z1 | Z2, later QA/QC | QB/QD]
   static constexpr int BOFF = wp_rup(wp_max(XBOX, 2 * VEXT), ALIGN);
   static constexpr int ZOFF = BOFF + BBOX;
   static constexpr int WARP_ELEMS = wp_rup(ZOFF + wp_max(2 * ZEXT, QBUF1 + QBUF2), ALIGN);
   static constexpr int QSZ = M * M * M;
-  static constexpr int NT = 32 * WARPS;
-  static constexpr size_t OFF_RL = sizeof(T) * static_cast<size_t>(WARPS) * WARP_ELEMS;
+  static constexpr int NT = 32 * TEAM;  // one team = one CTA, one patch at a time
+  static constexpr size_t OFF_RL = sizeof(T) * static_cast<size_t>(WARP_ELEMS);
   static constexpr size_t OFF_BAR = (OFF_RL + sizeof(T) * QSZ + 7) / 8 * 8;
-  static constexpr size_t BYTES = OFF_BAR + 8 * WARPS;
-  static constexpr size_t bytes_for(int w)
-  {
-    return (sizeof(T) * (static_cast<size_t>(w) * WARP_ELEMS + QSZ) + 7) / 8 * 8 + 8 * static_cast<size_t>(w);
-  }
-  // line tasks of the stages
+  static constexpr size_t BYTES = OFF_BAR + 8;
+  // line tasks of the stages and their 32-lane passes per warp of the team
   static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
   static constexpr int NZT = RING + IPAIR, NYT = M * N1, NQT = M * M;
+  static constexpr int NZP = (NZT + 31) / 32, NYP = (NYT + 31) / 32, NQP = (NQT + 31) / 32;
+  static constexpr int NZPW = (NZP + TEAM - 1) / TEAM, NYPW = (NYP + TEAM - 1) / TEAM;
+  static constexpr int NQPW = (NQP + TEAM - 1) / TEAM;
 };
 
-// warps per CTA: the count that fits the most warps on an SM (228 KB of
-// shared memory, 1 KB reserved per CTA, at most 32 CTAs), fewer warps per CTA
-// on ties
+// warps per patch (the team, one CTA): two in FP64 from degree 4 on, one
+// otherwise (measured at 3D Q4, ms per sweep, one warp vs two: FP64 64^3
+// 1.053 vs 0.998, 32^3 0.152 vs 0.148; FP32 64^3 0.564 vs 0.604, where the
+// pair kernel is the default anyway)
 template <int K, typename T>
 constexpr int wp3_warps()
 {
-  int best = 1, best_w = 0;
-  for (int w = 1; w <= 8; ++w) {
-    const size_t bytes = Wp3<K, T, 1>::bytes_for(w);
-    int ctas = static_cast<int>(233472 / (bytes + 1024));
-    if (ctas > 32) ctas = 32;
-    if (ctas * w > best_w) {
-      best_w = ctas * w;
-      best = w;
-    }
-  }
-  return best;
+  return K >= 4 && sizeof(T) == 8 ? 2 : 1;
 }
 
-// CTAs per SM at that size (the register budget of __launch_bounds__)
+// CTAs per SM (the register budget of __launch_bounds__): as many as shared
+// memory holds (228 KB, 1 KB reserved per CTA, at most 32 CTAs), at most 32
+// warps per SM for the FP64 degree-4 teams (a thread then keeps 64 registers,
+// it needs 62) and 18 otherwise
 template <int K, typename T>
 constexpr int wp3_ctas()
 {
-  const int c = static_cast<int>(233472 / (Wp3<K, T, 1>::bytes_for(wp3_warps<K, T>()) + 1024));
+  constexpr int w = wp3_warps<K, T>();
+  constexpr int max_warps = w == 2 && K <= 4 ? 32 : 18;
+  int c = static_cast<int>(233472 / (Wp3<K, T, w>::BYTES + 1024));
+  if (c * w > max_warps) c = max_warps / w;
   return c > 32 ? 32 : c < 1 ? 1 : c;
 }
 
@@ -161,23 +160,30 @@ __device__ __forceinline__ void wp_patch_xyz(const Sm3Args &a, int j, int k, int
   fz = (a.cz + 2 * jz) * k;
 }
 
-template <int K, typename T, int WARPS>
-__global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
+template <int K, typename T, int TEAM>
+__global__ void __launch_bounds__(32 * TEAM, wp3_ctas<K, T>())
     smoother3d_warp_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
                            T *__restrict__ x, const Sm3Args a, T scale, T fd_scale, int *__restrict__ err)
 {
   griddep_wait();  // programmatic launch: the previous kernel's writes are visible
-  using S = Wp3<K, T, WARPS>;
+  using S = Wp3<K, T, TEAM>;
   using Lo = typename S::L;
   using P2 = typename Pair<T>::type;
   constexpr int N1 = S::N1, M = S::M, W = S::W, AL = S::A;
   constexpr Str3 QA = Lo::QA, QB = Lo::QB, QC = Lo::QC, QD = Lo::QD;
   const DegreeTables<K, T> &tb = c_tables<K, T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+  const int tid = threadIdx.x, lane = tid & 31, wt = tid >> 5;  // wt: warp within the team
   T *RL = reinterpret_cast<T *>(smem_raw + S::OFF_RL);
-  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + S::OFF_BAR) + wid;
-  T *stage = reinterpret_cast<T *>(smem_raw) + static_cast<size_t>(wid) * S::WARP_ELEMS;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + S::OFF_BAR);
+  T *stage = reinterpret_cast<T *>(smem_raw);
+  // the team's barrier between stages (one warp: the warp's own)
+  auto team_sync = [&]() {
+    if constexpr (TEAM == 1)
+      __syncwarp();
+    else
+      __syncthreads();
+  };
   T *Z1 = stage + S::ZOFF, *Z2 = Z1 + S::ZEXT;
   T *V1 = stage, *V2 = stage + S::VEXT;
   T *QAb = Z1, *QBb = Z1 + S::QBUF1;  // QA and QC share one buffer, QB and QD the other
@@ -186,15 +192,15 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
   // fd_scale / (lambda_x + lambda_y + lambda_z), index (z mode, y mode, x mode)
   for (int e = tid; e < S::QSZ; e += S::NT)
     RL[e] = fd_scale / (tb.eval[e % M] + tb.eval[(e / M) % M] + tb.eval[e / (M * M)]);
-  if (lane == 0) {
+  if (tid == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
   }
-  __syncthreads();  // the only CTA-wide barrier: RL and the mbarriers are ready
+  __syncthreads();  // RL and the mbarrier are ready
 
-  const int G = gridDim.x * WARPS;
-  int j = blockIdx.x * WARPS + wid;
-  auto issue = [&](int fx, int fy, int fz) {  // lane 0: the x box and b slab of the patch at (fx, fy, fz)
+  const int G = gridDim.x;
+  int j = blockIdx.x;
+  auto issue = [&](int fx, int fy, int fz) {  // thread 0: the x box and b slab of the patch at (fx, fy, fz)
     const int x0 = fx & ~(AL - 1);
     mbar_arrive_expect_tx(bar, static_cast<uint32_t>(sizeof(T) * (S::BBOX + (a.zero_x ? 0 : S::XBOX))));
     if (!a.zero_x) tma_load_3d(stage, &map_x, bar, x0, fy, fz);
@@ -203,15 +209,16 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
   int fx = 0, fy = 0, fz = 0;
   if (j < a.n_patches) {
     wp_patch_xyz(a, j, K, fx, fy, fz);
-    if (lane == 0) issue(fx, fy, fz);
+    if (tid == 0) issue(fx, fy, fz);
   }
 
   for (int it = 0; j < a.n_patches; j += G, ++it) {
     const int xo = fx & (AL - 1);
-    int nfx = 0, nfy = 0, nfz = 0;  // the next patch of this warp
+    int nfx = 0, nfy = 0, nfz = 0;  // the next patch of this team
     if (j + G < a.n_patches) wp_patch_xyz(a, j + G, K, nfx, nfy, nfz);
-    if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar, it & 1))) {
-      if (lane == 0) atomicExch(err, 1);
+    const bool ok = mbar_wait_bounded(bar, it & 1);
+    if (TEAM == 1 ? !__all_sync(0xffffffffu, ok) : !__syncthreads_and(ok)) {
+      if (tid == 0) atomicExch(err, 1);
       return;  // the only copy in flight was the one waited for
     }
 
@@ -219,8 +226,8 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
       // ---- z: Z1 = M_z x~, Z2 = L_z x~ (ring lines, then pairs of interior lines) ----
       const T *box = stage + xo;
 #pragma unroll
-      for (int p = 0; p < (S::NZT + 31) / 32; ++p) {
-        const int t = lane + 32 * p;
+      for (int jp = 0; jp < S::NZPW; ++jp) {
+        const int t = lane + 32 * (wt + TEAM * jp);
         if (t < S::RING) {
           int y, xx;
           if (t < N1) {
@@ -267,11 +274,11 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
           }
         }
       }
-      __syncwarp();
+      team_sync();
       // ---- y: V1 = M_y Z2 + L_y Z1, V2 = M_y Z1 (V overwrites the dead x box) ----
 #pragma unroll
-      for (int p = 0; p < (S::NYT + 31) / 32; ++p) {
-        const int t = lane + 32 * p;
+      for (int jp = 0; jp < S::NYPW; ++jp) {
+        const int t = lane + 32 * (wt + TEAM * jp);
         if (t < S::NYT) {
           const int zi = t % M, xx = t / M;
           const T *s1 = Z1 + zi * Lo::PZ + xx, *s2 = Z2 + zi * Lo::PZ + xx;
@@ -294,12 +301,12 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
           }
         }
       }
-      __syncwarp();
+      team_sync();
     }
     // ---- x: r = b - s (M_x V1 + L_x V2), then S^T along x -> QA ----
 #pragma unroll
-    for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
-      const int t = lane + 32 * p;
+    for (int jp = 0; jp < S::NQPW; ++jp) {
+      const int t = lane + 32 * (wt + TEAM * jp);
       if (t < S::NQT) {
         const int zi = t / M, yi = t % M;
         const T *bb = bsl + (zi * M + yi) * W + xo + 1;
@@ -329,16 +336,16 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
         for (int i = 0; i < M; ++i) d[i * QA.c] = q[i];
       }
     }
-    __syncwarp();
+    team_sync();
     // the staged box and slab are consumed: fetch the next patch now
-    if (lane == 0 && j + G < a.n_patches) {
+    if (tid == 0 && j + G < a.n_patches) {
       fence_proxy_async_smem();
       issue(nfx, nfy, nfz);
     }
     // ---- S^T along y: QA -> QB ----
 #pragma unroll
-    for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
-      const int t = lane + 32 * p;
+    for (int jp = 0; jp < S::NQPW; ++jp) {
+      const int t = lane + 32 * (wt + TEAM * jp);
       if (t < S::NQT) {
         const int zi = t / M, qx = t % M;
         const T *s = QAb + zi * QA.p + qx * QA.c;
@@ -351,11 +358,11 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
         for (int jj = 0; jj < M; ++jj) d[jj * QB.r] = q[jj];
       }
     }
-    __syncwarp();
+    team_sync();
     // ---- S^T along z, eigenvalue scaling, S along z: QB -> QC ----
 #pragma unroll
-    for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
-      const int t = lane + 32 * p;
+    for (int jp = 0; jp < S::NQPW; ++jp) {
+      const int t = lane + 32 * (wt + TEAM * jp);
       if (t < S::NQT) {
         const int yi = t / M, xi = t % M;
         const T *s = QBb + yi * QB.r + xi * QB.c;
@@ -371,11 +378,11 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
         for (int jj = 0; jj < M; ++jj) d[jj * QC.p] = v[jj];
       }
     }
-    __syncwarp();
+    team_sync();
     // ---- S along x: QC -> QD ----
 #pragma unroll
-    for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
-      const int t = lane + 32 * p;
+    for (int jp = 0; jp < S::NQPW; ++jp) {
+      const int t = lane + 32 * (wt + TEAM * jp);
       if (t < S::NQT) {
         const int zi = t / M, yi = t % M;
         const T *s = QAb + zi * QC.p + yi * QC.r;
@@ -388,15 +395,15 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
         for (int i = 0; i < M; ++i) d[i * QD.c] = q[i];
       }
     }
-    __syncwarp();
+    team_sync();
     // ---- S along y and store x_I ----
     // 64-bit patch base once; 32-bit offsets within the patch (a patch spans
     // less than 2 planes of a level of < 2^31 entries)
     T *const xp = x + (fx + 1 + (fy + 1) * a.sy + (fz + 1) * a.sz);
     const int sy32 = static_cast<int>(a.sy), sz32 = static_cast<int>(a.sz);
 #pragma unroll
-    for (int p = 0; p < (S::NQT + 31) / 32; ++p) {
-      const int t = lane + 32 * p;
+    for (int jp = 0; jp < S::NQPW; ++jp) {
+      const int t = lane + 32 * (wt + TEAM * jp);
       if (t < S::NQT) {
         const int z = t / M, xx = t % M;
         const T *s = QBb + z * QD.p + xx * QD.c;
@@ -409,7 +416,7 @@ __global__ void __launch_bounds__(32 * WARPS, wp3_ctas<K, T>())
         for (int jj = 0; jj < M; ++jj) xp[o + jj * sy32] = q[jj];
       }
     }
-    __syncwarp();  // the Q buffers (inside the Z region) are read before the next z stage
+    team_sync();  // the Q buffers (inside the Z region) are read before the next z stage
     fx = nfx;
     fy = nfy;
     fz = nfz;

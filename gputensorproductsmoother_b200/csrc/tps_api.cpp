@@ -1613,6 +1613,22 @@ int tps_get_smoother_variant(tps_handle *h, int dtype, int level, int *variant)
   });
 }
 
+int tps_set_operator_layers(tps_handle *h, int dtype, int level, int layers)
+{
+  return guarded(h, [&] {
+    const int p = dt_index(dtype);
+    check_level(h, level);
+    if (layers != 0 && layers != 1 && layers != 2 && layers != 4 && layers != 8)
+      throw ApiError(TPS_ERR_INVALID, "operator layers must be 0 (default), 1, 2, 4 or 8");
+    if (static_cast<int>(h->op_layers[p].size()) != h->n_levels) h->op_layers[p].assign(h->n_levels, 0);
+    h->op_layers[p][level] = layers;
+    if (h->graph) {  // later solves re-capture with the chosen tile depth
+      cudaGraphExecDestroy(h->graph);
+      h->graph = nullptr;
+    }
+  });
+}
+
 int tps_get_operator_layers(tps_handle *h, int dtype, int level, int *layers)
 {
   return guarded(h, [&] {

@@ -284,6 +284,11 @@ int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
  * per CTA that tps_autotune chose, or 0 for the library's rule (8 layers, fewer
  * where a level would have fewer than 148 CTAs). */
 int tps_get_operator_layers(tps_handle *h, int dtype, int level, int *layers);
+/* Set the operator tile depth of a level explicitly (1, 2, 4 or 8 cell layers
+ * per CTA; 0 restores the library's rule).  The mat-vec is bit-identical for
+ * every depth; the fused p.q of the outer CG is summed per CTA, so a solve's
+ * rounding follows the depth of the finest level. */
+int tps_set_operator_layers(tps_handle *h, int dtype, int level, int layers);
 /* The compiled variants of the 3D smoother, TPS_SMOOTHER_VARIANTS entries:
  * patches per CTA batch 0 default, 1 half, 2 quarter, 3 one warp per patch
  * (reported as -1 where it is compiled) and 4 two patches per warp in packed

@@ -81,13 +81,19 @@ def test_autotune_keeps_results(cuda):
 
 def test_autotune_operator_tile_depth_keeps_results(cuda):
     """The autotuner also picks the operator's cell layers per CTA (1, 2, 4 or
-    8, at most the level's cells); every output is formed by the same
-    arithmetic whatever the tile depth, so mixed and FP64 solves after tuning
-    are bit-identical to the untuned ones."""
+    8, at most the level's cells).  Every output of the operator is formed by
+    the same arithmetic whatever the tile depth, so the mat-vec is
+    bit-identical; the CG's fused p.q is summed per CTA, so its rounding
+    follows the tile depth: solves after tuning take the same iterations and
+    agree to rounding (each configuration is itself deterministic)."""
     P = tps.PoissonProblem(3, 4, 16)
     N1 = 65
     bb = interior_random(3, N1, 4)
     MG = tps.MultigridSolvers(P)
+    A = tps.LaplaceOperator(P)
+    src = interior_random(3, N1, 5)
+    y_ref = torch.empty_like(src)
+    A.vmult(y_ref, src)
     ref = {p: MG.solve_cg(bb, precision=p, rel_tol=1e-10) for p in ("fp32", "fp64")}
     assert all(P.operator_layers(lv, dt) == 0 for lv in range(P.n_levels) for dt in ("fp32", "fp64"))
     P.autotune("fp32")
@@ -96,7 +102,18 @@ def test_autotune_operator_tile_depth_keeps_results(cuda):
         for lv in range(P.n_levels):
             cz = P.operator_layers(lv, dt)
             assert cz in (1, 2, 4, 8) and cz <= P.cells(lv), (dt, lv, cz)
+    for cz in (1, 2, 4, 8):  # every tile depth of the finest level: the same mat-vec
+        P.set_operator_layers(cz, "fp64", P.n_levels - 1)
+        y = torch.empty_like(src)
+        A.vmult(y, src)
+        assert torch.equal(y, y_ref), cz
+    with pytest.raises(tps.TpsError):
+        P.set_operator_layers(3, "fp64", 0)
+    P.autotune("fp64")
     for p in ("fp32", "fp64"):
         x, rep = MG.solve_cg(bb, precision=p, rel_tol=1e-10)
         assert rep.iterations == ref[p][1].iterations
-        assert torch.equal(x, ref[p][0]), p
+        d = ((x - ref[p][0]).norm() / ref[p][0].norm()).item()
+        assert d <= 1e-12, (p, d)
+        x2, _ = MG.solve_cg(bb, precision=p, rel_tol=1e-10)
+        assert torch.equal(x2, x), p
