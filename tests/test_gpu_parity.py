@@ -193,8 +193,12 @@ def _rhs(dim, N1, seed):
     return b
 
 
-@pytest.mark.parametrize("dim,k,n", [(2, 2, 32), (3, 2, 8), (3, 4, 8)])
+@pytest.mark.parametrize("dim,k,n", [(2, 2, 32), (3, 2, 8), (3, 4, 8), (3, 4, 6), (3, 4, 12), (3, 3, 6), (3, 7, 8)])
 def test_cg_fp64_matches_oracle(cuda, oracle, dim, k, n):
+    """FP64 CG through the C ABI against the oracle: identical iteration
+    counts and residual histories.  The 3D cases include meshes of 3 * 2^L
+    cells (dense coarse solve), whose finest level does not fill the
+    operator's xy tiles (the fused q = A p and its partial p.q sums)."""
     P = tps.PoissonProblem(dim, k, n)
     H = oracle.Hierarchy(dim, k, P.n_coarse, P.n_levels)
     b = _rhs(dim, n * k + 1, 7)
