@@ -134,7 +134,10 @@ cudaError_t set_attributes()
   TPS_SET((patch_solve_kernel<3, K, T>), (sizeof(T) * PVar<3, K>::SOLVE_ELEMS));
   TPS_SET((kappa_smoother_kernel<3, K, T>), (sizeof(T) * KSm<3, K, T>::ELEMS));
 #if TPS_DEGREE >= 2
+#if TPS_DEGREE >= 5
+  // degrees 5..7: the per-patch kernel; 2..4: the patch GEMM below
   if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_tc_kernel<K>), (Tc3<K>::BYTES));
+#endif
 #if TPS_DEGREE <= 4
   if constexpr (sizeof(T) == 4) TPS_SET((smoother3d_gemm_kernel<K>), (Pg3<K>::BYTES));
 #if TPS_DEGREE == 4
@@ -367,8 +370,9 @@ cudaError_t smoother(const LevelGeomH &g, const VecLayout &l, void *x, const voi
 }
 
 #if TPS_DEGREE >= 2
-// persistent grid of the tensor-core smoother: CTAs resident per SM x SMs,
-// capped so that every CTA's TMEM allocation fits at once
+#if TPS_DEGREE >= 5
+// persistent grid of the per-patch tensor-core smoother: CTAs resident per SM
+// x SMs, capped so that every CTA's TMEM allocation fits at once
 int tc_grid(int n_units)
 {
   {
@@ -382,6 +386,7 @@ int tc_grid(int n_units)
     return n_units < g ? n_units : g;
   }
 }
+#endif
 
 cudaError_t smoother_tc(const LevelGeomH &g, const VecLayout &l, void *x, const void *b, int colour,
                         double omega, int zero_x, const SmootherMaps *maps, int passes, int *err, cudaStream_t s)
