@@ -190,11 +190,12 @@ cudaError_t laplace(const LevelGeomH &g, const VecLayout &l, void *dst, const vo
   const T scale = static_cast<T>(stiffness_scale(DIM, g.h));
   if constexpr (DIM == 3) {
     using Sz = OpMarch<K, T>;
-    // at least one CTA per SM of a 148-SM part: 8 layers per CTA on 32^3 and
-    // larger Q4 levels, 1 on 16^3 and smaller (measured with the earlier
-    // streaming kernel, us per FP64 apply with 8 layers vs 1: 16^3 24.7 vs
-    // 19.5, 8^3 23.0 vs 19.6; with 2 layers on 32^3 the recomputed leading
-    // layers made it 33.0 -> 39.6)
+    // at least one CTA per SM of a 148-SM part: 16 layers per CTA on 64^3
+    // Q4 (8 on 32^3), 1 on 16^3 and smaller (each CTA recomputes one leading
+    // layer; measured, ms per FP64 apply with 4 / 8 / 16 layers: Q4 64^3
+    // 0.155 / 0.144 / 0.139, Q7 32^3 0.223 / 0.220 / 0.210; with the earlier
+    // streaming kernel, us per apply with 8 layers vs 1: 16^3 24.7 vs 19.5,
+    // 8^3 23.0 vs 19.6)
     const int cz = layers > 0 ? layers : opmarch_layers<K, T>(g.n, 148);
     const dim3 grid(ceil_div(g.n, Sz::TX), ceil_div(g.n, Sz::TY), ceil_div(g.n, cz));
     const size_t smem = sizeof(T) * Sz::ELEMS;

@@ -66,7 +66,7 @@ struct OpMarch {
   static constexpr int NZT = OY * HX;                 // z-stage column pairs
   static constexpr int NT = ((NYT > NZT ? NYT : NZT) + 31) / 32 * 32;
   static constexpr int EPT = (WY * WX + NT - 1) / NT;  // staged entries per thread and plane
-  static constexpr int CZ = 8;                         // cell layers per CTA (at most)
+  static constexpr int CZ = 16;                        // cell layers per CTA (the default's most)
   // shared memory (elements): IN[K][PL] | X1[K][XS] | X2[K][XS] | T1[K][TS] | T2[K][TS]
   static constexpr int OFF_X1 = march_align4(K * PL);
   static constexpr int OFF_X2 = march_align4(OFF_X1 + K * XS);

@@ -957,7 +957,7 @@ void autotune_levels(tps_handle *h, int p, cudaStream_t s)
   for (int l = 0; l < h->n_levels; ++l) {
     float best_op = 1e30f;
     int bz = 0;
-    for (int cz = 1; cz <= 8 && cz <= h->lv[l].n; cz *= 2) {
+    for (int cz = 1; cz <= 16 && cz <= h->lv[l].n; cz *= 2) {
       h->op_layers[p][l] = cz;
       const float t = best_of_three(h, s, [&] {
         level_laplace(h, l, p, V.layout[l], V.t[l]->p, V.su[l]->p, V.d[l]->p, 1, s);
@@ -1618,8 +1618,8 @@ int tps_set_operator_layers(tps_handle *h, int dtype, int level, int layers)
   return guarded(h, [&] {
     const int p = dt_index(dtype);
     check_level(h, level);
-    if (layers != 0 && layers != 1 && layers != 2 && layers != 4 && layers != 8)
-      throw ApiError(TPS_ERR_INVALID, "operator layers must be 0 (default), 1, 2, 4 or 8");
+    if (layers != 0 && layers != 1 && layers != 2 && layers != 4 && layers != 8 && layers != 16)
+      throw ApiError(TPS_ERR_INVALID, "operator layers must be 0 (default), 1, 2, 4, 8 or 16");
     if (static_cast<int>(h->op_layers[p].size()) != h->n_levels) h->op_layers[p].assign(h->n_levels, 0);
     h->op_layers[p][level] = layers;
     if (h->graph) {  // later solves re-capture with the chosen tile depth

@@ -273,19 +273,19 @@ int tps_solve_host_many(tps_handle *h, const tps_solve_opts *opts, int n, const 
  * AdditionalData::patch_per_block, include/patch_smoother.cuh:101-118, fixed
  * there, chosen here by timing): on every level of the dtype's V-cycle it times
  * each compiled smoother variant (patches per CTA batch, one warp per patch,
- * two patches per warp) and each tile depth of the operator (1, 2, 4 or 8
- * cell layers per CTA of the z-marching kernel), and keeps the fastest of each
+ * two patches per warp) and each tile depth of the operator (1, 2, 4, 8 or
+ * 16 cell layers per CTA of the z-marching kernel), and keeps the fastest of each
  * for later sweeps, operator applications and V-cycles of this handle.
  * ppb_per_level (n_levels entries, may be null) receives the chosen smoother
  * values (0 in 2D, -1 for one warp per patch, -2 for two patches per warp).
  * Batched solves tune their systems automatically. */
 int tps_autotune(tps_handle *h, int dtype, int *ppb_per_level);
 /* The operator tile depth a level of the dtype's V-cycle uses: the cell layers
- * per CTA that tps_autotune chose, or 0 for the library's rule (8 layers, fewer
+ * per CTA that tps_autotune chose, or 0 for the library's rule (16 layers, fewer
  * where a level would have fewer than 148 CTAs). */
 int tps_get_operator_layers(tps_handle *h, int dtype, int level, int *layers);
-/* Set the operator tile depth of a level explicitly (1, 2, 4 or 8 cell layers
- * per CTA; 0 restores the library's rule).  The mat-vec is bit-identical for
+/* Set the operator tile depth of a level explicitly (1, 2, 4, 8 or 16 cell
+ * layers per CTA; 0 restores the library's rule).  The mat-vec is bit-identical for
  * every depth; the fused p.q of the outer CG is summed per CTA, so a solve's
  * rounding follows the depth of the finest level. */
 int tps_set_operator_layers(tps_handle *h, int dtype, int level, int layers);

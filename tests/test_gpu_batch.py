@@ -80,8 +80,8 @@ def test_autotune_keeps_results(cuda):
 
 
 def test_autotune_operator_tile_depth_keeps_results(cuda):
-    """The autotuner also picks the operator's cell layers per CTA (1, 2, 4 or
-    8, at most the level's cells).  Every output of the operator is formed by
+    """The autotuner also picks the operator's cell layers per CTA (1, 2, 4, 8
+    or 16, at most the level's cells).  Every output of the operator is formed by
     the same arithmetic whatever the tile depth, so the mat-vec is
     bit-identical; the CG's fused p.q is summed per CTA, so its rounding
     follows the tile depth: solves after tuning take the same iterations and
@@ -101,8 +101,8 @@ def test_autotune_operator_tile_depth_keeps_results(cuda):
     for dt in ("fp32", "fp64"):
         for lv in range(P.n_levels):
             cz = P.operator_layers(lv, dt)
-            assert cz in (1, 2, 4, 8) and cz <= P.cells(lv), (dt, lv, cz)
-    for cz in (1, 2, 4, 8):  # every tile depth of the finest level: the same mat-vec
+            assert cz in (1, 2, 4, 8, 16) and cz <= P.cells(lv), (dt, lv, cz)
+    for cz in (1, 2, 4, 8, 16):  # every tile depth of the finest level: the same mat-vec
         P.set_operator_layers(cz, "fp64", P.n_levels - 1)
         y = torch.empty_like(src)
         A.vmult(y, src)
