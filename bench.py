@@ -583,7 +583,10 @@ def measure_solves(workload: str, precisions, warmup: int = 1, reps: int = 3) ->
     """Solves of one configuration from x = 0 to 1e-10 with each V-cycle
     precision (the first must be "fp64": the FP64 GPU solution the others'
     errors refer to): best time of `reps` (CUDA events on the solving
-    stream), iterations, final residual, DoF/s."""
+    stream), iterations, final residual, DoF/s.  With both "fp32" and "tf32":
+    whether the TF32 V-cycle used the tensor cores on any level, and at
+    degrees 5..7 the finest level's sweep time on the FP32 SIMT and the
+    tensor-core (TF32) smoothers."""
     import torch
     import gputensorproductsmoother_b200 as tps
     from gputensorproductsmoother_b200 import problems
@@ -596,6 +599,7 @@ def measure_solves(workload: str, precisions, warmup: int = 1, reps: int = 3) ->
     out = {"dofs": P.n_dofs(), "interior_dofs": nint}
     stream = torch.cuda.Stream()
     x64 = None
+    histories = {}
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         for prec in precisions:
@@ -616,10 +620,24 @@ def measure_solves(workload: str, precisions, warmup: int = 1, reps: int = 3) ->
                 x64 = x.clone()
             else:
                 rec["error_vs_fp64_solve"] = (torch.linalg.norm(x - x64) / torch.linalg.norm(x64)).item()
+            histories[prec] = list(rep.history)
             out[prec] = rec
     if "fp64" in out:
         for prec in precisions[1:]:
             out[prec]["speedup_vs_fp64"] = out["fp64"]["ms"] / out[prec]["ms"]
+    if "tf32" in out and "fp32" in out:
+        # the TF32 V-cycle runs the tensor-core smoother only on the levels
+        # where it is faster; a residual history identical to the FP32
+        # V-cycle's shows that it ran on none
+        out["tf32"]["tensor_core_levels_used"] = histories["tf32"] != histories["fp32"]
+        if dim == 3 and k >= 5:
+            lf = P.n_levels - 1
+            sweep = {}
+            for d in ("fp32", "tf32"):
+                P.time_smoother(lf, d, 2)
+                sweep[d] = min(P.time_smoother(lf, d, 10) for _ in range(3))
+            out["finest_level_sweep_ms"] = {"fp32_simt": sweep["fp32"], "tf32_tensor_cores": sweep["tf32"],
+                                            "kernel": f"smoother3d_tc_kernel<{k}>"}
     P.close()
     return out
 
