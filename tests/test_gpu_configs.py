@@ -25,7 +25,9 @@ def test_config_2d_q2_64(cuda, oracle):
     H = oracle.Hierarchy(2, 2, P.n_coarse, P.n_levels)
     xr, itr, _ = H.solve_cg(b.cpu().numpy(), precision=0, symmetric=True, rel_tol=1e-10)
     assert rep.converged and rep.iterations == itr
-    assert np.abs(x.cpu().numpy() - xr).max() <= 1e-11 * np.abs(xr).max()
+    xg = x.cpu().numpy()
+    assert np.linalg.norm(xg - xr) <= 1e-12 * np.linalg.norm(xr)
+    assert np.abs(xg - xr).max() <= 1e-11 * np.abs(xr).max()
 
 
 def test_config_3d_q4_64_mixed_vs_fp64(cuda):
