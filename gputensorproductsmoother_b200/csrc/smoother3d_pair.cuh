@@ -213,10 +213,10 @@ struct Pp3 {
   static constexpr int BOFF = wp_rup(wp_max(2 * XBOX_A, 4 * VEXT), ALIGN);
   static constexpr int ZOFF = BOFF + 2 * BBOX_A;
   static constexpr int WARP_ELEMS = wp_rup(ZOFF + wp_max(4 * ZEXT, 2 * (QBUF1 + QBUF2)), ALIGN);
-  static constexpr int QSZ = M * M * M;
   static constexpr int NT = 32 * TEAM;  // one team = one CTA, one pair of patches at a time
-  static constexpr size_t OFF_RL = sizeof(float) * static_cast<size_t>(WARP_ELEMS);
-  static constexpr size_t OFF_BAR = (OFF_RL + sizeof(float) * QSZ + 7) / 8 * 8;
+  // the eigenvalue scalings live in registers (no shared table), so that the
+  // stage alone sets the CTAs per SM
+  static constexpr size_t OFF_BAR = sizeof(float) * static_cast<size_t>(WARP_ELEMS);
   static constexpr size_t BYTES = OFF_BAR + 8;
   static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
   static constexpr int NZT = RING + IPAIR, NYT = M * N1, NQT = M * M;
@@ -287,9 +287,11 @@ __device__ __forceinline__ PairZTask pair_ztask(int lane, int p)
 // Warps per pair of patches (the team, one CTA): two from degree 4 on, where
 // every stage has at least two 32-lane passes, so the warps split a pair's
 // passes and twice the warps per SM share the staged boxes' shared memory;
-// one below.  CTAs per SM: as many as shared memory holds, at most 16 warps
-// per SM so that a thread keeps 128 registers (the pair contractions hold
-// about 120 live values at degree 4).
+// one below.  The launch bound asks for as many CTAs per SM as shared memory
+// holds, but at most 16 warps' worth, so that a thread may keep 128 registers
+// (the pair contractions hold about 120 live values at degree 4).  The grid
+// is sized by the occupancy the compiled kernel reaches: 10 CTAs (20 warps)
+// per SM at degree 4 with 82 registers.
 constexpr int kPairMaxWarpsPerSm = 16;
 template <int K>
 constexpr int pp3_warps()
@@ -320,7 +322,6 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
   const DegreeTables<K, float> &tb = c_tables<K, float>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, wt = tid >> 5;  // wt: warp within the team
-  float *RL = reinterpret_cast<float *>(smem_raw + S::OFF_RL);
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + S::OFF_BAR);
   float *stage = reinterpret_cast<float *>(smem_raw);
   // the team's barrier between stages (one warp: the warp's own)
@@ -336,23 +337,23 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
   const float *boxA = stage, *boxB = stage + S::XBOX_A;
   const float *bslA = stage + S::BOFF, *bslB = bslA + S::BBOX_A;
 
-  for (int e = tid; e < S::QSZ; e += S::NT)
-    RL[e] = fd_scale / (tb.eval[e % M] + tb.eval[(e / M) % M] + tb.eval[e / (M * M)]);
   if (tid == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
   }
-  __syncthreads();  // RL and the mbarrier are ready
+  __syncthreads();  // the mbarrier is ready
   // this lane's eigenvalue scalings of the z stage of the solve (the tasks of
-  // this warp's passes, modes 0..M-1), kept in registers
+  // this warp's passes, modes 0..M-1), kept in registers: line t = (qy, qx) =
+  // (t / M, t % M), mode qz = jj, omega / (s (lambda_qx + lambda_qy + lambda_qz))
   constexpr int NPW = S::NPW;
   float rl[NPW][M];
 #pragma unroll
   for (int j = 0; j < NPW; ++j) {
     const int t0 = lane + 32 * (wt + TEAM * j);
     const int t = t0 < S::NQT ? t0 : lane % S::NQT;
+    const float exy = tb.eval[t % M], eyy = tb.eval[t / M];
 #pragma unroll
-    for (int jj = 0; jj < M; ++jj) rl[j][jj] = RL[jj * M * M + t];
+    for (int jj = 0; jj < M; ++jj) rl[j][jj] = fd_scale / (exy + eyy + tb.eval[jj]);
   }
 
   const int n_pairs = (a.n_patches + 1) >> 1;

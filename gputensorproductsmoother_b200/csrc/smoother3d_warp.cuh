@@ -112,10 +112,10 @@ struct Wp3 {
   static constexpr int BOFF = wp_rup(wp_max(XBOX, 2 * VEXT), ALIGN);
   static constexpr int ZOFF = BOFF + BBOX;
   static constexpr int WARP_ELEMS = wp_rup(ZOFF + wp_max(2 * ZEXT, QBUF1 + QBUF2), ALIGN);
-  static constexpr int QSZ = M * M * M;
   static constexpr int NT = 32 * TEAM;  // one team = one CTA, one patch at a time
-  static constexpr size_t OFF_RL = sizeof(T) * static_cast<size_t>(WARP_ELEMS);
-  static constexpr size_t OFF_BAR = (OFF_RL + sizeof(T) * QSZ + 7) / 8 * 8;
+  // the eigenvalue scalings live in registers (no shared table), so that the
+  // stage alone sets the CTAs per SM
+  static constexpr size_t OFF_BAR = sizeof(T) * static_cast<size_t>(WARP_ELEMS);
   static constexpr size_t BYTES = OFF_BAR + 8;
   // line tasks of the stages and their 32-lane passes per warp of the team
   static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
@@ -137,8 +137,8 @@ constexpr int wp3_warps()
 
 // CTAs per SM (the register budget of __launch_bounds__): as many as shared
 // memory holds (228 KB, 1 KB reserved per CTA, at most 32 CTAs), at most 32
-// warps per SM for the FP64 degree-4 teams (a thread then keeps 64 registers,
-// it needs 62) and 18 otherwise
+// warps per SM for the FP64 degree-4 teams and 18 otherwise (10 CTAs of the
+// FP64 degree-4 team fit, about 76 registers a thread)
 template <int K, typename T>
 constexpr int wp3_ctas()
 {
@@ -174,7 +174,6 @@ __global__ void __launch_bounds__(32 * TEAM, wp3_ctas<K, T>())
   const DegreeTables<K, T> &tb = c_tables<K, T>;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   const int tid = threadIdx.x, lane = tid & 31, wt = tid >> 5;  // wt: warp within the team
-  T *RL = reinterpret_cast<T *>(smem_raw + S::OFF_RL);
   uint64_t *bar = reinterpret_cast<uint64_t *>(smem_raw + S::OFF_BAR);
   T *stage = reinterpret_cast<T *>(smem_raw);
   // the team's barrier between stages (one warp: the warp's own)
@@ -189,14 +188,23 @@ __global__ void __launch_bounds__(32 * TEAM, wp3_ctas<K, T>())
   T *QAb = Z1, *QBb = Z1 + S::QBUF1;  // QA and QC share one buffer, QB and QD the other
   const T *bsl = stage + S::BOFF;
 
-  // fd_scale / (lambda_x + lambda_y + lambda_z), index (z mode, y mode, x mode)
-  for (int e = tid; e < S::QSZ; e += S::NT)
-    RL[e] = fd_scale / (tb.eval[e % M] + tb.eval[(e / M) % M] + tb.eval[e / (M * M)]);
+  // fd_scale / (lambda_x + lambda_y + lambda_z) for this lane's lines of the
+  // z stage of the solve (t = (y mode, x mode) = (t / M, t % M), one per
+  // pass of this warp) and every z mode, kept in registers
+  T rl[S::NQPW][M];
+#pragma unroll
+  for (int jp = 0; jp < S::NQPW; ++jp) {
+    const int t0 = lane + 32 * (wt + TEAM * jp);
+    const int t = t0 < S::NQT ? t0 : 0;  // lanes without a line compute an unused value
+    const T exy = tb.eval[t % M], eyy = tb.eval[t / M];
+#pragma unroll
+    for (int jj = 0; jj < M; ++jj) rl[jp][jj] = fd_scale / (exy + eyy + tb.eval[jj]);
+  }
   if (tid == 0) {
     mbar_init(bar, 1);
     fence_mbar_init();
   }
-  __syncthreads();  // RL and the mbarrier are ready
+  __syncthreads();  // the mbarrier is ready
 
   const int G = gridDim.x;
   int j = blockIdx.x;
@@ -371,7 +379,7 @@ __global__ void __launch_bounds__(32 * TEAM, wp3_ctas<K, T>())
         for (int jj = 0; jj < M; ++jj) v[jj] = s[jj * QB.p];
         evec_apply<K, T, true>(v, q);
 #pragma unroll
-        for (int jj = 0; jj < M; ++jj) q[jj] *= RL[jj * M * M + t];
+        for (int jj = 0; jj < M; ++jj) q[jj] *= rl[jp][jj];
         evec_apply<K, T, false>(q, v);
         T *d = QAb + yi * QC.r + xi * QC.c;
 #pragma unroll
