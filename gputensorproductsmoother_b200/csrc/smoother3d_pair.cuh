@@ -31,11 +31,14 @@
 // has consumed the current ones.  An odd last patch is paired with itself
 // and stored once.  Every wait is bounded.
 //
-// Shared memory (8-byte pair elements): the z- and y-stage outputs Z and V
-// are stored task-major for the stage that reads them (conflict-free
-// consecutive reads), with strides and, at degree 4, a z-stage lane
-// assignment chosen so that the writes are conflict-free as well; the four
-// fast-diagonalisation arrays use the 8-byte layouts WpLayout<K, 8>.  Every
+// Shared memory (8-byte pair elements): the z-stage outputs are kept only
+// for the 8k ring lines of the box face.  On the interior lines x~ is zero
+// except on the two z faces, so the z stage stores just those two values
+// and the y stage forms the z products itself, with the same rounding.  That
+// is 4.7 KB less per team at degree 4 (Q3 64^3 sweep 0.253 -> 0.228 ms).
+// The z- and y-stage outputs are stored task-major for the stage that reads
+// them (consecutive or shared words); the four fast-diagonalisation arrays
+// use the 8-byte layouts WpLayout<K, 8>.  Every
 // stage runs its passes as straight-line code: lanes past the last task redo
 // a valid task and skip the stores, so the loads of one pass can be issued
 // while the previous pass computes (lanes past the last task take task
@@ -196,52 +199,49 @@ struct Pp3 {
   static constexpr int XBOX = N1 * N1 * W, BBOX = M * M * W;        // floats per patch
   static constexpr int ALIGN = 32;                                   // floats (128 B: TMA destinations)
   static constexpr int XBOX_A = wp_rup(XBOX, ALIGN), BBOX_A = wp_rup(BBOX, ALIGN);
-  // Z [zi][y][x] = M_z / L_z x~ and V [zi][yi][x] in "task-major" layouts:
-  // the next stage's task t (its line) is the fastest index, so its reads of
-  // element q are the consecutive words t + q * stride (conflict-free); the
-  // strides ZY (y of Z) and M * M (x of V) were chosen by a bank-conflict
-  // search over the writing stage's lane mappings
-  static constexpr int ZY = K == 2 ? 15 : K == 3 ? 36 : K == 4 ? 63 : 108;
-  static constexpr Str3 ZL{1, ZY, M}, VL{M, 1, M * M};  // {zi, y or yi, x} strides
-  static constexpr int ZEXT = (M - 1) * ZL.p + (N1 - 1) * ZL.r + (N1 - 1) * ZL.c + 1;
+  // The z stage's output for the box face lines, in "task-major" layouts
+  // (the reading stage's task is the fastest index, so its reads are
+  // consecutive or shared words):
+  // * ring lines (the RING = 8K lines with y or x on the box face), ring
+  //   index q: top row q = x, bottom row N1 + x, left column 2 N1 + y - 1,
+  //   right column 2 N1 + M + y - 1; ZR1 = M_z x~ and ZR2 = L_z x~ as
+  //   [q][zi] (zi fastest);
+  // * interior lines (y, x both interior): x~ is zero there except on the
+  //   z faces, so M_z x~ = m_0 x(0) + m_N x(N1 - 1) per output; only the two
+  //   face values are kept, F0 and F8 as [y - 1][x - 1], and the y stage
+  //   forms the products itself, with the same rounding as the z stage's
+  //   ring lines.
+  // V [zi][yi][x] with strides VL (x stride M * M chosen by a bank-conflict
+  // search over the y stage's lane mapping).
+  static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
+  static constexpr int ZR = RING * M, ZI = M * M;  // pair elements of ZR1 / ZR2 and of F0 / F8
+  static constexpr Str3 VL{M, 1, M * M};           // {zi, yi, x} strides of V
   static constexpr int VEXT = (M - 1) * VL.p + (M - 1) * VL.r + (N1 - 1) * VL.c + 1;
-  static constexpr int NZP = (N1 * N1 - M * M + (M * M + 1) / 2 + 31) / 32;  // passes of the z stage
+  static constexpr int NZP = (RING + IPAIR + 31) / 32;  // passes of the z stage
   static constexpr int ext(Str3 s) { return (M - 1) * (s.p + s.r + s.c) + 1; }
   static constexpr int QBUF1 = wp_max(ext(L::QA), ext(L::QC)), QBUF2 = wp_max(ext(L::QB), ext(L::QD));
   // per team (floats): [x box A | x box B, later V1 | V2] [b slab A | b slab B]
-  // [Z1 | Z2, later QA/QC | QB/QD]; pair arrays take 2 floats per element
+  // [ZR1 | ZR2 | F0 | F8, later QA/QC | QB/QD]; pair arrays take 2 floats per element
   static constexpr int BOFF = wp_rup(wp_max(2 * XBOX_A, 4 * VEXT), ALIGN);
   static constexpr int ZOFF = BOFF + 2 * BBOX_A;
-  static constexpr int WARP_ELEMS = wp_rup(ZOFF + wp_max(4 * ZEXT, 2 * (QBUF1 + QBUF2)), ALIGN);
+  static constexpr int ZSPAN = wp_max(4 * (ZR + ZI), 2 * (QBUF1 + QBUF2));
+  static constexpr int WARP_ELEMS = wp_rup(ZOFF + ZSPAN, ALIGN);
   static constexpr int NT = 32 * TEAM;  // one team = one CTA, one pair of patches at a time
   // the eigenvalue scalings live in registers (no shared table), so that the
-  // stage alone sets the CTAs per SM
-  static constexpr size_t OFF_BAR = sizeof(float) * static_cast<size_t>(WARP_ELEMS);
+  // stage alone sets the CTAs per SM; the mbarrier sits right after the stage
+  static constexpr size_t OFF_BAR = (sizeof(float) * static_cast<size_t>(ZOFF + ZSPAN) + 7) / 8 * 8;
   static constexpr size_t BYTES = OFF_BAR + 8;
-  static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
   static constexpr int NZT = RING + IPAIR, NYT = M * N1, NQT = M * M;
   // 32-lane passes of each stage; warp w of the team takes passes w, w + TEAM, ...
   static constexpr int NYP = (NYT + 31) / 32, NP = (NQT + 31) / 32;
   static constexpr int NZPW = (NZP + TEAM - 1) / TEAM, NYPW = (NYP + TEAM - 1) / TEAM, NPW = (NP + TEAM - 1) / TEAM;
 };
 
-// Lane assignment of the z stage at degree 4 (positions y * 9 + x of the box
-// face, 255: idle): pass 0 the 32 ring lines, pass 1 two interior lines per
-// lane.  With the Z layout above (y stride 63, x stride 7, 8-byte words) every
-// half-warp's 16 stores of one instruction fall on 16 distinct bank pairs;
-// the assignment was found by a greedy search over the lines' residues
-// (y * 63 + 7 x) mod 16.
-static __device__ const unsigned char kPairRing4[32] = {0,  7,  78, 5,  76, 3,  74, 1,  8,  79, 6,  77, 4,  75, 2,  73,
-                                          80, 71, 62, 53, 44, 35, 26, 17, 72, 63, 54, 45, 36, 27, 18, 9};
-static __device__ const unsigned char kPairIn4[2][32] = {
-    {16, 10, 11, 12, 13, 14, 15, 19, 20, 21, 22, 23, 24, 25, 33, 34,
-     48, 58, 59, 61, 47, 68, 70, 56, 65, 255, 255, 255, 255, 255, 255, 255},
-    {32, 42, 43, 28, 29, 30, 31, 51, 52, 37, 38, 39, 40, 41, 49, 50,
-     64, 60, 46, 67, 69, 55, 57, 66, 255, 255, 255, 255, 255, 255, 255, 255}};
-
-// z-stage task of a lane in one pass: ring = one full z-line, else up to
-// two interior z-lines (their x box rows read at z = 0 and z = N1-1 only);
-// positions y * N1 + x, -1 = none
+// z-stage task of a lane in one pass: ring = one full z-line (its ring
+// index q is the task index t, so lane t's stores of ZR1 / ZR2 are the words
+// t * M + zi: an odd stride, conflict-free), else up to two interior z-lines
+// (interior indices i and i + IPAIR, consecutive across lanes); positions
+// y * N1 + x, -1 = none
 struct PairZTask {
   int ring, in0, in1;
 };
@@ -249,37 +249,30 @@ struct PairZTask {
 template <int K>
 __device__ __forceinline__ PairZTask pair_ztask(int lane, int p)
 {
-  constexpr int N1 = 2 * K + 1, M = 2 * K - 1, RING = N1 * N1 - M * M, NZT = RING + (M * M + 1) / 2;
+  constexpr int N1 = 2 * K + 1, M = 2 * K - 1, RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
+  constexpr int NZT = RING + IPAIR;
   PairZTask r{-1, -1, -1};
-  if constexpr (K == 4) {
-    if (p == 0) {
-      r.ring = kPairRing4[lane];
+  const int t = lane + 32 * p;
+  if (t < RING) {
+    int y, xx;
+    if (t < N1) {
+      y = 0;
+      xx = t;
+    } else if (t < 2 * N1) {
+      y = N1 - 1;
+      xx = t - N1;
+    } else if (t < 2 * N1 + M) {
+      y = 1 + t - 2 * N1;
+      xx = 0;
     } else {
-      const int a = kPairIn4[0][lane], b = kPairIn4[1][lane];
-      r.in0 = a == 255 ? -1 : a;
-      r.in1 = b == 255 ? -1 : b;
+      y = 1 + t - 2 * N1 - M;
+      xx = N1 - 1;
     }
-  } else {
-    const int t = lane + 32 * p;
-    if (t < RING) {
-      int y, xx;
-      if (t < N1) {
-        y = 0;
-        xx = t;
-      } else if (t < 2 * N1) {
-        y = N1 - 1;
-        xx = t - N1;
-      } else {
-        const int q = t - 2 * N1;
-        y = 1 + (q >> 1);
-        xx = (q & 1) ? N1 - 1 : 0;
-      }
-      r.ring = y * N1 + xx;
-    } else if (t < NZT) {
-      const int r0 = 2 * (t - RING);
-      r.in0 = (1 + r0 / M) * N1 + 1 + r0 % M;
-      if (r0 + 1 < M * M) r.in1 = (1 + (r0 + 1) / M) * N1 + 1 + (r0 + 1) % M;
-    }
+    r.ring = y * N1 + xx;
+  } else if (t < NZT) {
+    const int e0 = t - RING, e1 = e0 + IPAIR;
+    r.in0 = (1 + e0 / M) * N1 + 1 + e0 % M;
+    if (e1 < M * M) r.in1 = (1 + e1 / M) * N1 + 1 + e1 % M;
   }
   return r;
 }
@@ -289,9 +282,9 @@ __device__ __forceinline__ PairZTask pair_ztask(int lane, int p)
 // passes and twice the warps per SM share the staged boxes' shared memory;
 // one below.  The launch bound asks for as many CTAs per SM as shared memory
 // holds, but at most 16 warps' worth, so that a thread may keep 128 registers
-// (the pair contractions hold about 120 live values at degree 4).  The grid
-// is sized by the occupancy the compiled kernel reaches: 10 CTAs (20 warps)
-// per SM at degree 4 with 82 registers.
+// (90 at degree 4, so the registers allow 10 CTAs of two warps; a bound of 11
+// CTAs forced 78 registers and measured 0.476 against 0.459 ms per Q4 64^3
+// sweep).  The grid is sized by the occupancy the compiled kernel reaches.
 constexpr int kPairMaxWarpsPerSm = 16;
 template <int K>
 constexpr int pp3_warps()
@@ -331,9 +324,10 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
     else
       __syncthreads();
   };
-  float2 *Z1 = reinterpret_cast<float2 *>(stage + S::ZOFF), *Z2 = Z1 + S::ZEXT;
+  float2 *ZR1 = reinterpret_cast<float2 *>(stage + S::ZOFF), *ZR2 = ZR1 + S::ZR;
+  float2 *F0 = ZR2 + S::ZR, *F8 = F0 + S::ZI;
   float2 *V1 = reinterpret_cast<float2 *>(stage), *V2 = V1 + S::VEXT;
-  float2 *QAb = Z1, *QBb = Z1 + S::QBUF1;  // QA and QC share one buffer, QB and QD the other
+  float2 *QAb = ZR1, *QBb = ZR1 + S::QBUF1;  // QA and QC share one buffer, QB and QD the other
   const float *boxA = stage, *boxB = stage + S::XBOX_A;
   const float *bslA = stage + S::BOFF, *bslB = bslA + S::BBOX_A;
 
@@ -354,6 +348,28 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
     const float exy = tb.eval[t % M], eyy = tb.eval[t / M];
 #pragma unroll
     for (int jj = 0; jj < M; ++jj) rl[j][jj] = fd_scale / (exy + eyy + tb.eval[jj]);
+  }
+
+  // this lane's y-stage lines (task t = (zi, xx) = (t % M, t / M), one per
+  // pass of this warp): rows 1..M of a side column (xx = 0 or N1 - 1) are ring
+  // lines, read from ZR1 / ZR2; those of an interior column are formed from
+  // the face values F0 / F8 as c_0 x(0) + c_N x(N1 - 1) of row zi + 1 of the
+  // patch mass and stiffness.  Side lanes take coefficients (1, 0) and (0, 1),
+  // which pass the ring values through (up to the sign of a zero).
+  float yc[S::NYPW][4];  // c_0 and c_N of the mass, then of the stiffness
+  int yb[S::NYPW][2];    // offsets (pair elements from ZR1) of rows y = 1 of the two arrays
+#pragma unroll
+  for (int j = 0; j < S::NYPW; ++j) {
+    const int t0 = lane + 32 * (wt + TEAM * j);
+    const int t = t0 < S::NYT ? t0 : lane % S::NYT;
+    const int zi = t % M, xx = t / M;
+    const bool side = xx == 0 || xx == N1 - 1;
+    yc[j][0] = side ? 1.f : tb.pmass[(zi + 1) * N1];
+    yc[j][1] = side ? 0.f : tb.pmass[(zi + 1) * N1 + N1 - 1];
+    yc[j][2] = side ? 0.f : tb.plap[(zi + 1) * N1];
+    yc[j][3] = side ? 1.f : tb.plap[(zi + 1) * N1 + N1 - 1];
+    yb[j][0] = side ? (2 * N1 + (xx == 0 ? 0 : M)) * M + zi : 2 * S::ZR + xx - 1;
+    yb[j][1] = yb[j][0] + (side ? S::ZR : S::ZI);
   }
 
   const int n_pairs = (a.n_patches + 1) >> 1;
@@ -399,12 +415,14 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
     }
 
     if (!a.zero_x) {
-      // ---- z: Z1 = M_z x~, Z2 = L_z x~ (ring lines, then interior lines) ----
+      // ---- z: ZR1 = M_z x~, ZR2 = L_z x~ on the ring lines; the face values
+      // x(0), x(N1 - 1) of the interior lines into F0, F8 ----
       const float *ba = boxA + xoa, *bb = boxB + xob;
 #pragma unroll
       for (int j = 0; j < S::NZPW; ++j) {
         const PairZTask tk = ztk[j];
         if (tk.ring >= 0) {
+          const int q = lane + 32 * (wt + TEAM * j);  // ring index = task index
           const int y = tk.ring / N1, xx = tk.ring % N1;
           const int o = y * W + xx;
           float2 v[N1], E[K], O[K], ec, r1[M], r2[M];
@@ -413,11 +431,11 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
           pr_fold<K>(v, E, O, ec);
           pr_rows<K>(tb.pmass_fe, tb.pmass_fo, E, O, ec, r1);
           pr_rows<K>(tb.plap_fe, tb.plap_fo, E, O, ec, r2);
-          float2 *d1 = Z1 + y * S::ZL.r + xx * S::ZL.c, *d2 = Z2 + y * S::ZL.r + xx * S::ZL.c;
+          float2 *d1 = ZR1 + q * M, *d2 = ZR2 + q * M;
 #pragma unroll
           for (int i = 0; i < M; ++i) {
-            d1[i * S::ZL.p] = r1[i];
-            d2[i * S::ZL.p] = r2[i];
+            d1[i] = r1[i];
+            d2[i] = r2[i];
           }
         }
 #pragma unroll
@@ -425,15 +443,9 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
           const int pos = h == 0 ? tk.in0 : tk.in1;
           if (pos >= 0) {
             const int y = pos / N1, xx = pos % N1;
-            const int o = y * W + xx;
-            const float2 v0 = make_float2(ba[o], bb[o]);
-            const float2 vn = make_float2(ba[o + (N1 - 1) * N1 * W], bb[o + (N1 - 1) * N1 * W]);
-            float2 *d1 = Z1 + y * S::ZL.r + xx * S::ZL.c, *d2 = Z2 + y * S::ZL.r + xx * S::ZL.c;
-#pragma unroll
-            for (int i = 0; i < M; ++i) {
-              d1[i * S::ZL.p] = pr_fma(tb.pmass[(i + 1) * N1 + N1 - 1], vn, pr_mul(tb.pmass[(i + 1) * N1], v0));
-              d2[i * S::ZL.p] = pr_fma(tb.plap[(i + 1) * N1 + N1 - 1], vn, pr_mul(tb.plap[(i + 1) * N1], v0));
-            }
+            const int o = y * W + xx, e = (y - 1) * M + xx - 1;
+            F0[e] = make_float2(ba[o], bb[o]);
+            F8[e] = make_float2(ba[o + (N1 - 1) * N1 * W], bb[o + (N1 - 1) * N1 * W]);
           }
         }
       }
@@ -441,21 +453,43 @@ __global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
       // ---- y: V1 = M_y Z2 + L_y Z1, V2 = M_y Z1 (V overwrites the dead x boxes) ----
       // task t = (zi, xx) = (t % M, t / M); lanes past the last task redo a
       // valid task (lane mod the task count) and skip the stores, so every pass
-      // is straight-line code
+      // is straight-line code.  Z1, Z2 on the lane's line: rows 0 and N1 - 1
+      // from the ring arrays (ring index xx and N1 + xx, so word t and
+      // N1 M + t), rows 1..M as set up above; folded in pairs of rows as
+      // pr_fold does.
 #pragma unroll
       for (int j = 0; j < S::NYPW; ++j) {
         const int t0 = lane + 32 * (wt + TEAM * j);
         const bool act = t0 < S::NYT;
         const int t = act ? t0 : lane % S::NYT;
         const int zi = t % M, xx = t / M;
-        const float2 *s1 = Z1 + t, *s2 = Z2 + t;  // = zi * ZL.p + xx * ZL.c
-        float2 v[N1], E1[K], O1[K], ec1, E2[K], O2[K], ec2;
+        const float2 *s1 = ZR1 + yb[j][0], *s2 = ZR1 + yb[j][1];
+        const float cm0 = yc[j][0], cmn = yc[j][1], cl0 = yc[j][2], cln = yc[j][3];
+        // Z1, Z2 of row y = 1 + r of the line
+        auto zrow = [&](int r, float2 &z1, float2 &z2) {
+          const float2 f0 = s1[r * M], f8 = s2[r * M];
+          z1 = pr_fma(cmn, f8, pr_mul(cm0, f0));
+          z2 = pr_fma(cln, f8, pr_mul(cl0, f0));
+        };
+        float2 E1[K], O1[K], ec1, E2[K], O2[K], ec2;
+        {
+          const float2 a1 = ZR1[t], b1 = ZR1[N1 * M + t], a2 = ZR2[t], b2 = ZR2[N1 * M + t];
+          E1[0] = pr_add(a1, b1);
+          O1[0] = pr_sub(a1, b1);
+          E2[0] = pr_add(a2, b2);
+          O2[0] = pr_sub(a2, b2);
+        }
 #pragma unroll
-        for (int qq = 0; qq < N1; ++qq) v[qq] = s1[qq * S::ZL.r];
-        pr_fold<K>(v, E1, O1, ec1);
-#pragma unroll
-        for (int qq = 0; qq < N1; ++qq) v[qq] = s2[qq * S::ZL.r];
-        pr_fold<K>(v, E2, O2, ec2);
+        for (int jj = 1; jj < K; ++jj) {
+          float2 a1, a2, b1, b2;
+          zrow(jj - 1, a1, a2);          // row jj
+          zrow(N1 - 2 - jj, b1, b2);     // row N1 - 1 - jj
+          E1[jj] = pr_add(a1, b1);
+          O1[jj] = pr_sub(a1, b1);
+          E2[jj] = pr_add(a2, b2);
+          O2[jj] = pr_sub(a2, b2);
+        }
+        zrow(K - 1, ec1, ec2);  // the centre row K
         float2 ra[M], rc[M];
         pr_rows_sum<K>(tb.pmass_fe, tb.pmass_fo, E2, O2, ec2, tb.plap_fe, tb.plap_fo, E1, O1, ec1, ra);
         pr_rows<K>(tb.pmass_fe, tb.pmass_fo, E1, O1, ec1, rc);
