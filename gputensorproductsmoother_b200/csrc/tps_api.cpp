@@ -431,17 +431,30 @@ int default_variant(const tps_handle *h, int level, int p)
 {
   if (h->dim != 3) return 0;
   const int64_t c = h->lv[level].n / 2;  // patches per direction of colour 0
-  const bool large = c * c * c >= 4096;
-  // levels whose colours hold fewer patches are latency-bound: half CTA
-  // batches in FP32 and, at degree 3, quarter batches in FP64 (measured on
-  // B200, us per sweep, default / half / quarter batch / warp per patch:
-  // Q4 FP32 16^3 37.0 / 36.9 / 39.3 / 40.5, 8^3 35.3 / 31.2 / 33.7 / 37.4,
-  // 4^3 33.6 / 29.6 / 31.8 / 35.4; Q3 FP64 16^3 33.0 / 32.1 / 31.8 / 34.9)
-  if (!large) return p == 1 ? 1 : (h->k == 3 ? 2 : 0);
-  if (p == 1 && h->k >= 2 && h->k <= 4 && h->kt->smoother_ppb(3, 1, 4) == -2 && h->kt->smoother_ppb(3, 1, 3) == -1)
-    return 4;
-  if ((h->k != 3 && h->k != 4) || h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 3) != -1) return 0;
-  return 3;
+  const int64_t c3 = c * c * c;
+  const bool large = c3 >= 4096, medium = c3 >= 512;
+  const bool warp = h->kt->smoother_ppb(3, p == 0 ? 0 : 1, 3) == -1;  // one warp per patch compiled
+  const bool pair = p == 1 && h->kt->smoother_ppb(3, 1, 4) == -2;     // two patches per warp compiled
+  // The fastest variant per level size, measured on B200 (us per sweep,
+  // variants 0..4 = CTA batch P, P/2, P/4, warp per patch, pair of patches):
+  //   FP32 Q4 32^3 118 / 116 / 116 / 92 / 87, 16^3 37.2 / 37.5 / 39.4 / 38.9 / 35.4,
+  //        8^3 36.3 / 31.4 / 33.8 / 36.4 / 31.4, 4^3 35.9 / 32.0 / 33.9 / 36.8 / 32.4;
+  //   FP32 Q3 32^3 72 / 63 / 65 / 57 / 58, 16^3 34.6 / 27.1 / 27.5 / 29.8 / 32.0;
+  //   FP32 Q2 16^3 34.4 / 27.9 / 25.2 / 21.9 / 23.0;
+  //   FP64 Q4 32^3 165 / 171 / 165 / 135, 16^3 45.8 / 49.4 / 45.8 / 40.7,
+  //        8^3 38.3 / 42.6 / 38.4 / 33.6, 4^3 38.8 / 42.7 / 38.8 / 33.1;
+  //   FP64 Q3 32^3 98 / 96 / 101 / 80, 16^3 33.3 / 32.2 / 32.1 / 35.2, 8^3 32.2 / 28.8 / 27.4 / 31.5;
+  //   FP64 Q2 32^3 41.4 / 41.2 / 40.8 / 42.6, 16^3 31.4 / 27.9 / 24.3 / 24.7.
+  // Levels whose colours hold few patches are latency-bound; there the
+  // smaller CTA batches win.
+  if (p == 1) {
+    if (pair && h->k >= 2 && h->k <= 4 && (large || (medium && h->k == 4))) return 4;
+    if (warp && h->k == 2 && medium) return 3;
+    return large ? 0 : 1;
+  }
+  if (warp && (h->k == 4 || (h->k == 3 && large))) return 3;
+  if (h->k == 2 || h->k == 3) return 2;
+  return 0;
 }
 
 // one coloured sweep; x_zero declares x == 0 on entry (the first colour then

@@ -301,10 +301,18 @@ int tps_set_operator_layers(tps_handle *h, int dtype, int level, int layers);
 int tps_smoother_variants(tps_handle *h, int dtype, int *ppb);
 int tps_set_smoother_variant(tps_handle *h, int dtype, int level, int variant);
 /* The variant a level's sweeps use now: the one set or autotuned, else the
- * library default: where a colour holds at least 4096 patches, two patches
- * per warp (FP32, degrees 2..4) or one warp per patch (FP64, degrees 3 and
- * 4), else the default CTA batch; on smaller levels half CTA batches in FP32
- * and, at degree 3, quarter batches in FP64. */
+ * library default, the fastest measured per level size.
+ * FP32:
+ *   - two patches per warp where a colour holds at least 4096 patches
+ *     (degrees 2..4), and at degree 4 from 512 patches;
+ *   - one warp per patch at degree 2 from 512 patches;
+ *   - otherwise the default CTA batch on large levels and half batches on
+ *     smaller ones.
+ * FP64:
+ *   - one warp per patch at degree 4, and at degree 3 where a colour holds
+ *     at least 4096 patches;
+ *   - otherwise quarter CTA batches at degrees 2 and 3, and the default batch
+ *     at other degrees. */
 int tps_get_smoother_variant(tps_handle *h, int dtype, int level, int *variant);
 
 /* ---- batched solves (no reference counterpart) ----------------------------
