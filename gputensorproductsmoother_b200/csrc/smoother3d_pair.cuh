@@ -280,11 +280,10 @@ __device__ __forceinline__ PairZTask pair_ztask(int lane, int p)
 // Warps per pair of patches (the team, one CTA): two from degree 4 on, where
 // every stage has at least two 32-lane passes, so the warps split a pair's
 // passes and twice the warps per SM share the staged boxes' shared memory;
-// one below.  The launch bound asks for as many CTAs per SM as shared memory
-// holds, but at most 16 warps' worth, so that a thread may keep 128 registers
-// (90 at degree 4, so the registers allow 10 CTAs of two warps; a bound of 11
-// CTAs forced 78 registers and measured 0.476 against 0.459 ms per Q4 64^3
-// sweep).  The grid is sized by the occupancy the compiled kernel reaches.
+// one below.  The register bound (pp3_regs) follows from as many CTAs per
+// SM as shared memory holds, but at most 16 warps' worth (a thread may then
+// keep 128 registers), except at degree 4 (below).  The grid is sized by the
+// occupancy the compiled kernel reaches.
 constexpr int kPairMaxWarpsPerSm = 16;
 template <int K>
 constexpr int pp3_warps()
@@ -301,8 +300,19 @@ constexpr int pp3_ctas()
   return ctas < 1 ? 1 : ctas;
 }
 
+// registers a thread may keep: what pp3_ctas CTAs per SM leave, except at
+// degree 4, where 88 (84 used) let 11 CTAs of two warps share an SM (ms per
+// Q4 64^3 sweep: 0.4507 against 0.4587 with 90 registers and 10 CTAs)
+template <int K>
+constexpr int pp3_regs()
+{
+  if (K == 4) return 88;
+  const int r = 65536 / (pp3_ctas<K>() * 32 * pp3_warps<K>()) / 8 * 8;
+  return r > 255 ? 255 : r;
+}
+
 template <int K, int TEAM>
-__global__ void __launch_bounds__(32 * TEAM, pp3_ctas<K>())
+__global__ void __launch_bounds__(32 * TEAM) __maxnreg__(pp3_regs<K>())
     smoother3d_pair_kernel(const __grid_constant__ CUtensorMap map_x, const __grid_constant__ CUtensorMap map_b,
                            float *__restrict__ x, const Sm3Args a, float scale, float fd_scale,
                            int *__restrict__ err)
