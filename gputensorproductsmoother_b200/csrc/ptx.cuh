@@ -258,5 +258,7 @@ __device__ __forceinline__ void cp_async_zfill_s(uint32_t saddr, const void *gme
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 // this thread's copies of all committed groups have landed in shared memory
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+// all but this thread's most recently committed group have landed
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 }  // namespace tps

@@ -18,6 +18,7 @@
 // lives in a per-level scratch buffer.
 #pragma once
 
+#include "ptx.cuh"
 #include "tps_common.cuh"
 
 namespace tps {
@@ -104,6 +105,13 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
   // the extra registers cost more than the overlap gained, 0.050 -> 0.068 ms,
   // so FP32 adds at the end)
   constexpr bool PREFETCH = OUT == XYOut::AddInterior && WO * C <= NT;
+  // The other add-mode tiles (FP32) stage the current fine values of the
+  // tile in shared memory by asynchronous copies, issued right after the
+  // coarse tile's, so that the read-modify-write of the fine level waits on
+  // no load at the end (3D Q4 64^3 mixed solve 12.35 -> 12.23 ms; the
+  // coarse tile by asynchronous copies as well, 12.37 -> 12.35)
+  constexpr bool STAGE_CUR = OUT == XYOut::AddInterior && !PREFETCH;
+  __shared__ T sCur[STAGE_CUR ? WO * WO : 1];
   T cur[1][2 * K];
   if constexpr (PREFETCH) {
     const int t = threadIdx.x;
@@ -116,15 +124,31 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
       cur[0][f] = interior ? outp[gx + gy * out_sy] : T(0);
     }
   }
-  for (int e = threadIdx.x; e < WI * WI; e += NT) {
-    const int lx = e % WI, ly = e / WI;
-    const int gx = cx0 * K + lx, gy = cy0 * K + ly;
-    T v = T(0);
-    if (gx < N1c && gy < N1c) {
+  {
+    const uint32_t s_in = smem_u32(sIn);
+    for (int e = threadIdx.x; e < WI * WI; e += NT) {
+      const int lx = e % WI, ly = e / WI;
+      const int gx = cx0 * K + lx, gy = cy0 * K + ly;
       const bool bnd = gx == 0 || gx == N1c - 1 || gy == 0 || gy == N1c - 1;
-      if (!(mask_in && bnd)) v = inp[gx + gy * in_sy];
+      const bool ok = gx < N1c && gy < N1c && !(mask_in && bnd);
+      cp_async_zfill_s<sizeof(T)>(s_in + static_cast<uint32_t>(sizeof(T) * e), ok ? inp + gx + gy * in_sy : inp,
+                                  ok ? static_cast<uint32_t>(sizeof(T)) : 0u);
     }
-    sIn[e] = v;
+    cp_async_commit();
+  }
+  if constexpr (STAGE_CUR) {
+    const uint32_t s_cur = smem_u32(sCur);
+    for (int e = threadIdx.x; e < WO * WO; e += NT) {
+      const int xx = e % WO, yy = e / WO;
+      const int gx = 2 * K * cx0 + xx, gy = 2 * K * cy0 + yy;
+      const bool ok = gx < N1f && gy < N1f;
+      cp_async_zfill_s<sizeof(T)>(s_cur + static_cast<uint32_t>(sizeof(T) * e), ok ? outp + gx + gy * out_sy : outp,
+                                  ok ? static_cast<uint32_t>(sizeof(T)) : 0u);
+    }
+    cp_async_commit();
+    cp_async_wait_1();  // the coarse tile has landed; the fine one may be in flight
+  } else {
+    cp_async_wait_all();
   }
   __syncthreads();
   for (int t = threadIdx.x; t < WI * C; t += NT) {
@@ -136,6 +160,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
 #pragma unroll
     for (int f = 0; f < 2 * K; ++f) sX[y * WO + c * 2 * K + f] = o[f];
   }
+  if constexpr (STAGE_CUR) cp_async_wait_all();  // this thread's share of the fine tile
   __syncthreads();
   // y stage: fine rows of the tile, added to (or stored into) the fine plane
   auto y_task = [&](int t, const T (&add)[2 * K]) {
@@ -154,6 +179,8 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
       const bool interior = gx > 0 && gx < N1f - 1 && gy > 0 && gy < N1f - 1;
       if constexpr (PREFETCH) {
         if (interior) outp[gi] = add[f] + o[f];
+      } else if constexpr (STAGE_CUR) {
+        if (interior) outp[gi] = sCur[(2 * K * c + f) * WO + xx] + o[f];
       } else if constexpr (OUT == XYOut::AddInterior) {
         if (interior) outp[gi] += o[f];
       } else if constexpr (OUT == XYOut::SetInterior) {
@@ -192,14 +219,21 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
   T *outp = out + plane * out_plane;
   const int cx0 = blockIdx.x * C, cy0 = blockIdx.y * C;
   const int fx0 = 2 * K * (cx0 - 1), fy0 = 2 * K * (cy0 - 1);
+  // the fine tile (with its halo) by asynchronous copies, all in flight at
+  // once; a loop of plain loads waited on each (measured at 3D 64^3, us per
+  // restriction, plain / asynchronous: Q4 FP32 69.9 / 56.9, Q4 FP64 112.8 /
+  // 92.3, Q3 FP64 37.7 / 33.1; Q7 32^3 FP64 101.5 / 65.9, FP32 51.3 / 56.0);
+  // entries outside the interior are zero-filled
+  const uint32_t s_in = smem_u32(sIn);
   for (int e = threadIdx.x; e < WI * WI; e += NT) {
     const int lx = e % WI, ly = e / WI;
     const int gx = fx0 + lx, gy = fy0 + ly;
-    T v = T(0);
-    if (!zero_plane && gx > 0 && gx < N1f - 1 && gy > 0 && gy < N1f - 1)
-      v = __ldg(&inp[gx + gy * in_sy]);
-    sIn[e] = v;
+    const bool ok = !zero_plane && gx > 0 && gx < N1f - 1 && gy > 0 && gy < N1f - 1;
+    cp_async_zfill_s<sizeof(T)>(s_in + static_cast<uint32_t>(sizeof(T) * e), ok ? inp + gx + gy * in_sy : inp,
+                                ok ? static_cast<uint32_t>(sizeof(T)) : 0u);
   }
+  cp_async_commit();
+  cp_async_wait_all();
   __syncthreads();
   for (int t = threadIdx.x; t < WI * C; t += NT) {
     const int c = t % C, y = t / C;
