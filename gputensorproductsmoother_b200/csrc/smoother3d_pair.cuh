@@ -301,8 +301,11 @@ constexpr int pp3_ctas()
 }
 
 // registers a thread may keep: what pp3_ctas CTAs per SM leave, except at
-// degree 4, where 88 (84 used) let 11 CTAs of two warps share an SM (ms per
-// Q4 64^3 sweep: 0.4507 against 0.4587 with 90 registers and 10 CTAs)
+// degree 4, where the bound is 88.  The kernel then uses 84 (ms per Q4 64^3
+// sweep: 0.451, against 0.459 with 90).  Registers are allocated per SM
+// sub-partition, 5 warps of 88 each, so 10 CTAs of two warps fit either way.
+// A bound of 80 (6 warps per sub-partition, 11 CTAs with shared memory)
+// measured 0.467.
 template <int K>
 constexpr int pp3_regs()
 {
