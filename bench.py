@@ -286,7 +286,7 @@ TRAFFIC_CAPTURES = {
     ("smoother3d_warp_kernel<4,float>", "poisson3d_q4_64"):
         (136.6e6, 167.5e6, "profiles/smoother3d_warp_k4_f32_poisson3d_q4_64.md"),
     ("smoother3d_pair_kernel<4>", "poisson3d_q4_64"):
-        (136.52e6, 167.5e6, "profiles/smoother3d_pair_k4_f32_poisson3d_q4_64.md"),
+        (136.58e6, 167.5e6, "profiles/smoother3d_pair_k4_f32_poisson3d_q4_64.md"),
 }
 
 
