@@ -215,6 +215,11 @@ struct Pp3 {
   // search over the y stage's lane mapping).
   static constexpr int RING = N1 * N1 - M * M, IPAIR = (M * M + 1) / 2;
   static constexpr int ZR = RING * M, ZI = M * M;  // pair elements of ZR1 / ZR2 and of F0 / F8
+  // F0 starts PADF pair elements after ZR2: at degree 4 that puts the y
+  // stage's reads of F0 and F8 (interior columns) on other bank pairs than
+  // its reads of ZR1 and ZR2 (side columns) in the same instruction
+  // (F0 and F8 at words 5 and 6 mod 16; by a wavefront model of both passes)
+  static constexpr int PADF = K == 4 ? 5 : 0;
   static constexpr Str3 VL{M, 1, M * M};           // {zi, yi, x} strides of V
   static constexpr int VEXT = (M - 1) * VL.p + (M - 1) * VL.r + (N1 - 1) * VL.c + 1;
   static constexpr int NZP = (RING + IPAIR + 31) / 32;  // passes of the z stage
@@ -224,7 +229,7 @@ struct Pp3 {
   // [ZR1 | ZR2 | F0 | F8, later QA/QC | QB/QD]; pair arrays take 2 floats per element
   static constexpr int BOFF = wp_rup(wp_max(2 * XBOX_A, 4 * VEXT), ALIGN);
   static constexpr int ZOFF = BOFF + 2 * BBOX_A;
-  static constexpr int ZSPAN = wp_max(4 * (ZR + ZI), 2 * (QBUF1 + QBUF2));
+  static constexpr int ZSPAN = wp_max(4 * (ZR + ZI) + 2 * PADF, 2 * (QBUF1 + QBUF2));
   static constexpr int WARP_ELEMS = wp_rup(ZOFF + ZSPAN, ALIGN);
   static constexpr int NT = 32 * TEAM;  // one team = one CTA, one pair of patches at a time
   // the eigenvalue scalings live in registers (no shared table), so that the
@@ -338,7 +343,7 @@ __global__ void __launch_bounds__(32 * TEAM) __maxnreg__(pp3_regs<K>())
       __syncthreads();
   };
   float2 *ZR1 = reinterpret_cast<float2 *>(stage + S::ZOFF), *ZR2 = ZR1 + S::ZR;
-  float2 *F0 = ZR2 + S::ZR, *F8 = F0 + S::ZI;
+  float2 *F0 = ZR2 + S::ZR + S::PADF, *F8 = F0 + S::ZI;
   float2 *V1 = reinterpret_cast<float2 *>(stage), *V2 = V1 + S::VEXT;
   float2 *QAb = ZR1, *QBb = ZR1 + S::QBUF1;  // QA and QC share one buffer, QB and QD the other
   const float *boxA = stage, *boxB = stage + S::XBOX_A;
@@ -381,7 +386,7 @@ __global__ void __launch_bounds__(32 * TEAM) __maxnreg__(pp3_regs<K>())
     yc[j][1] = side ? 0.f : tb.pmass[(zi + 1) * N1 + N1 - 1];
     yc[j][2] = side ? 0.f : tb.plap[(zi + 1) * N1];
     yc[j][3] = side ? 1.f : tb.plap[(zi + 1) * N1 + N1 - 1];
-    yb[j][0] = side ? (2 * N1 + (xx == 0 ? 0 : M)) * M + zi : 2 * S::ZR + xx - 1;
+    yb[j][0] = side ? (2 * N1 + (xx == 0 ? 0 : M)) * M + zi : 2 * S::ZR + S::PADF + xx - 1;
     yb[j][1] = yb[j][0] + (side ? S::ZR : S::ZI);
   }
 
