@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(XYTile<K>::NT)
   // overlaps the coarse tile load and the x stage (measured at 3D Q4 64^3:
   // FP64 prolongation 0.094 -> 0.085 ms; with the two tasks of the FP32 tiles
   // the extra registers cost more than the overlap gained, 0.050 -> 0.068 ms,
-  // so FP32 adds at the end)
+  // so those tiles stage the values in shared memory instead, below)
   constexpr bool PREFETCH = OUT == XYOut::AddInterior && WO * C <= NT;
   // The other add-mode tiles (FP32) stage the current fine values of the
   // tile in shared memory by asynchronous copies, issued right after the
